@@ -1,0 +1,142 @@
+/*
+ * grid_gpu.h — C ABI of the B200 (sm_100a) ring-arithmetic hot path for
+ * Gridland (mrain/lattica): R_q = Z_q[X]/(X^d + 1), q an odd prime < 2^32.
+ *
+ * Data convention (zero-copy with the reference's types):
+ *   - A coefficient of R_q is one uint32_t PrimeField<Q, u32> Montgomery word,
+ *     value * 2^32 mod q, canonical in [0, q) (algebra/src/arith/prime.rs:24-29,
+ *     repr(transparent) over u32).
+ *   - A polynomial is d consecutive words (CyclotomicPolyRing / TwistedNttPoly
+ *     are inline [R; N], algebra/src/poly/ring.rs:140-145,
+ *     algebra/src/poly/twisted_ntt.rs:22-27).
+ *   - A ring matrix is row-major rows x cols polynomials (RingMat,
+ *     algebra/src/lattice/types.rs:230-265); a batch of vectors is
+ *     batch x len polynomials.
+ *   - "Evaluations" means the reference's twisted NTT domain: slot k holds
+ *     a(psi^(2k+1)) with psi = g^((q-1)/2d), g the smallest generator.
+ *
+ * Entry points come in two flavours:
+ *   - *_dev: device pointers, asynchronous on the caller's cudaStream_t
+ *     (passed as void*; NULL = legacy default stream). 16-byte aligned
+ *     buffers are required.
+ *   - host-buffer calls (no suffix): host pointers, synchronous; they copy in,
+ *     compute, copy out. Pinned buffers (grid_gpu_host_register) overlap copies
+ *     with compute.
+ *
+ * Every call returns a grid_status; none aborts. Plans are bound to the CUDA
+ * device current at creation. Host-buffer calls on one plan are serialised
+ * internally; *_dev calls are safe from several threads with distinct streams.
+ */
+#ifndef GRID_GPU_H
+#define GRID_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum grid_status {
+  GRID_OK = 0,
+  /* NttError (algebra/src/arith/ntt.rs:386-395) */
+  GRID_ERR_LENGTH_MISMATCH = 1,
+  GRID_ERR_LENGTH_NOT_POW2 = 2,
+  GRID_ERR_UNSUPPORTED_SIZE = 3,
+  GRID_ERR_UNSUPPORTED_TWIST = 4,
+  /* CommitmentError (commit/src/error.rs:7-18) */
+  GRID_ERR_INVALID_PARAMETERS = 5,
+  GRID_ERR_DIMENSION_MISMATCH = 6,
+  /* PrimeField const checks (algebra/src/arith/prime.rs:31-46) */
+  GRID_ERR_INVALID_MODULUS = 7,
+  /* ABI-level */
+  GRID_ERR_NULL_POINTER = 8,
+  GRID_ERR_OUT_OF_MEMORY = 9,
+  GRID_ERR_CUDA = 10,
+  GRID_ERR_TIMEOUT = 11,           /* a bounded device-side wait gave up */
+  GRID_ERR_UNSUPPORTED_DEGREE = 12, /* valid plan, but no kernel compiled for this d */
+  GRID_ERR_MISALIGNED = 13,
+  GRID_ERR_NO_DEVICE = 14
+} grid_status;
+
+typedef struct grid_gpu_plan grid_gpu_plan;
+typedef struct grid_gpu_matrix grid_gpu_matrix;
+
+typedef struct grid_gpu_plan_info {
+  uint32_t q;
+  uint32_t d;
+  uint32_t generator; /* Montgomery word of the smallest generator of Z_q^* */
+  uint32_t psi;       /* Montgomery word of root_of_unity(2d) */
+  uint32_t omega;     /* Montgomery word of root_of_unity(d) = psi^2 */
+  uint32_t n_inv;     /* Montgomery word of d^-1 */
+  uint32_t r_mod_q;   /* 2^32 mod q (the Montgomery one) */
+  uint32_t r2_mod_q;  /* 2^64 mod q */
+  uint64_t max_ntt_size;
+} grid_gpu_plan_info;
+
+/* ---- library ---------------------------------------------------------- */
+
+/* Human-readable name of a status code (static string). */
+const char* grid_gpu_status_string(int status);
+/* ABI version: (major << 16) | minor. */
+uint32_t grid_gpu_abi_version(void);
+/* Largest ring degree with compiled kernels (256). */
+uint32_t grid_gpu_max_degree(void);
+
+/* ---- plans: replace NttPlan::build / TwistedNttPlan::build ------------- */
+
+/* Mirrors TwistedNttPlan::build (algebra/src/poly/ntt.rs:139-154) over
+ * NttPlan::build (algebra/src/arith/ntt.rs:469-500): validates q, then
+ * LengthNotPowerOfTwo, UnsupportedSize, UnsupportedTwist in that order. */
+int grid_gpu_plan_create(uint64_t q, uint64_t d, grid_gpu_plan** out);
+int grid_gpu_plan_destroy(grid_gpu_plan* plan);
+/* Host-only: validate (q, d) exactly like grid_gpu_plan_create and return the
+ * plan's parameters and merged twiddles without touching a device. Any output
+ * pointer may be NULL (zeta/izeta: d words each). */
+int grid_gpu_plan_describe(uint64_t q, uint64_t d, grid_gpu_plan_info* info, uint32_t* zeta,
+                           uint32_t* izeta);
+int grid_gpu_plan_get_info(const grid_gpu_plan* plan, grid_gpu_plan_info* out);
+/* Host copy of the merged-NTT twiddle tables (d words each, index 0 unused):
+ * zeta[k] = psi^brv(k), izeta[k] = zeta[k]^-1 (Montgomery words). */
+int grid_gpu_plan_get_twiddles(const grid_gpu_plan* plan, uint32_t* zeta, uint32_t* izeta);
+/* Reads and clears the plan's device error word (GRID_ERR_TIMEOUT if a
+ * bounded device wait gave up since the last check). Synchronises `stream`. */
+int grid_gpu_plan_check(grid_gpu_plan* plan, void* stream);
+
+/* ---- NTT: replace NTTRing::ntt_{forward,inverse}_with_plan for twisted plans
+ *      (algebra/src/poly/ntt.rs:75-104, arith/prime.rs:617-637) ------------- */
+
+int grid_gpu_ntt_forward_dev(const grid_gpu_plan* plan, uint32_t* polys, size_t npolys,
+                             void* stream);
+int grid_gpu_ntt_inverse_dev(const grid_gpu_plan* plan, uint32_t* polys, size_t npolys,
+                             void* stream);
+/* out = INTT(NTT(a) (.) b_evals): forward twisted NTT, Montgomery pointwise
+ * product with evaluations b, inverse twisted NTT. out may alias a. */
+int grid_gpu_ntt_mul_inverse_dev(const grid_gpu_plan* plan, const uint32_t* a,
+                                 const uint32_t* b_evals, uint32_t* out, size_t npolys,
+                                 void* stream);
+/* Negacyclic product out = a * b mod (X^d + 1), poly_mul_ntt
+ * (algebra/src/poly/ntt.rs:305-319). Uses b_scratch (npolys*d words) for NTT(b). */
+int grid_gpu_poly_mul_dev(const grid_gpu_plan* plan, const uint32_t* a, const uint32_t* b,
+                          uint32_t* out, uint32_t* b_scratch, size_t npolys, void* stream);
+/* Ring::pointwise_mul_assign_slice (algebra/src/arith/prime.rs:433-447): dst *= rhs. */
+int grid_gpu_pointwise_mul_dev(const grid_gpu_plan* plan, uint32_t* dst, const uint32_t* rhs,
+                               size_t nwords, void* stream);
+
+int grid_gpu_ntt_forward(grid_gpu_plan* plan, uint32_t* polys, size_t npolys);
+int grid_gpu_ntt_inverse(grid_gpu_plan* plan, uint32_t* polys, size_t npolys);
+int grid_gpu_ntt_mul_inverse(grid_gpu_plan* plan, const uint32_t* a, const uint32_t* b_evals,
+                             uint32_t* out, size_t npolys);
+int grid_gpu_poly_mul(grid_gpu_plan* plan, const uint32_t* a, const uint32_t* b, uint32_t* out,
+                      size_t npolys);
+
+/* ---- host memory ------------------------------------------------------ */
+
+/* Page-lock a caller buffer so host-buffer calls can DMA it asynchronously. */
+int grid_gpu_host_register(void* ptr, size_t bytes);
+int grid_gpu_host_unregister(void* ptr);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GRID_GPU_H */

@@ -1,0 +1,92 @@
+"""ctypes binding of the C ABI in include/grid_gpu.h (libgridgpu.so).
+
+The product path has no CPU fallback: if the shared library is missing or a
+GPU is absent, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libgridgpu.so")
+
+GRID_OK = 0
+STATUS_NAMES = {
+    0: "OK", 1: "LengthMismatch", 2: "LengthNotPowerOfTwo", 3: "UnsupportedSize",
+    4: "UnsupportedTwist", 5: "InvalidParameters", 6: "DimensionMismatch",
+    7: "InvalidModulus", 8: "NullPointer", 9: "OutOfMemory", 10: "Cuda", 11: "Timeout",
+    12: "UnsupportedDegree", 13: "Misaligned", 14: "NoDevice",
+}
+
+_u32p = C.POINTER(C.c_uint32)
+_vp = C.c_void_p
+
+
+class PlanInfo(C.Structure):
+    _fields_ = [("q", C.c_uint32), ("d", C.c_uint32), ("generator", C.c_uint32),
+                ("psi", C.c_uint32), ("omega", C.c_uint32), ("n_inv", C.c_uint32),
+                ("r_mod_q", C.c_uint32), ("r2_mod_q", C.c_uint32), ("max_ntt_size", C.c_uint64)]
+
+
+# name -> (restype, argtypes); every symbol declared in include/grid_gpu.h.
+SIGNATURES = {
+    "grid_gpu_status_string": (C.c_char_p, [C.c_int]),
+    "grid_gpu_abi_version": (C.c_uint32, []),
+    "grid_gpu_max_degree": (C.c_uint32, []),
+    "grid_gpu_plan_create": (C.c_int, [C.c_uint64, C.c_uint64, C.POINTER(_vp)]),
+    "grid_gpu_plan_destroy": (C.c_int, [_vp]),
+    "grid_gpu_plan_describe": (C.c_int, [C.c_uint64, C.c_uint64, C.POINTER(PlanInfo), _vp, _vp]),
+    "grid_gpu_plan_get_info": (C.c_int, [_vp, C.POINTER(PlanInfo)]),
+    "grid_gpu_plan_get_twiddles": (C.c_int, [_vp, _vp, _vp]),
+    "grid_gpu_plan_check": (C.c_int, [_vp, _vp]),
+    "grid_gpu_ntt_forward_dev": (C.c_int, [_vp, _vp, C.c_size_t, _vp]),
+    "grid_gpu_ntt_inverse_dev": (C.c_int, [_vp, _vp, C.c_size_t, _vp]),
+    "grid_gpu_ntt_mul_inverse_dev": (C.c_int, [_vp, _vp, _vp, _vp, C.c_size_t, _vp]),
+    "grid_gpu_poly_mul_dev": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_size_t, _vp]),
+    "grid_gpu_pointwise_mul_dev": (C.c_int, [_vp, _vp, _vp, C.c_size_t, _vp]),
+    "grid_gpu_ntt_forward": (C.c_int, [_vp, _vp, C.c_size_t]),
+    "grid_gpu_ntt_inverse": (C.c_int, [_vp, _vp, C.c_size_t]),
+    "grid_gpu_ntt_mul_inverse": (C.c_int, [_vp, _vp, _vp, _vp, C.c_size_t]),
+    "grid_gpu_poly_mul": (C.c_int, [_vp, _vp, _vp, _vp, C.c_size_t]),
+    "grid_gpu_host_register": (C.c_int, [_vp, C.c_size_t]),
+    "grid_gpu_host_unregister": (C.c_int, [_vp]),
+}
+
+_lib = None
+_lock = threading.Lock()
+
+
+class GridGpuError(RuntimeError):
+    """A non-OK grid_status returned by the C ABI."""
+
+    def __init__(self, code: int, where: str = ""):
+        self.code = code
+        self.name = STATUS_NAMES.get(code, f"status{code}")
+        super().__init__(f"{where}: {self.name} ({code})" if where else f"{self.name} ({code})")
+
+
+def load():
+    """Load libgridgpu.so (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise ImportError(
+                    f"{LIB_PATH} is missing: build it with `python -m lattica_b200.build` "
+                    "(there is no CPU fallback)")
+            lib = C.CDLL(LIB_PATH)
+            for name, (res, args) in SIGNATURES.items():
+                fn = getattr(lib, name)
+                fn.restype = res
+                fn.argtypes = args
+            _lib = lib
+    return _lib
+
+
+def check(code: int, where: str = "") -> None:
+    if code != GRID_OK:
+        raise GridGpuError(code, where)

@@ -1,0 +1,130 @@
+// Internal host-side declarations shared by the CUDA translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include <mutex>
+#include <vector>
+
+#include "../../include/grid_gpu.h"
+#include "grid_field.cuh"
+
+namespace grid {
+
+// Merged (twist-folded) negacyclic NTT twiddles for one (q, d).
+// zeta[k] = psi^brv(k) for k in [1, d), psi the primitive 2d-th root used by
+// the reference (smallest generator g, psi = g^((q-1)/2d)); izeta[k] is its
+// inverse. Each entry is a Montgomery word plus its Shoup companion
+// w * q^-1 mod 2^32.
+struct TwiddleTable {
+  std::vector<uint32_t> zeta, zeta_q, izeta, izeta_q;  // index 0 unused
+  uint32_t ninv = 0, ninv_q = 0;                       // d^-1
+  uint32_t izeta1_ninv = 0, izeta1_ninv_q = 0;         // izeta[1] * d^-1
+};
+
+// Largest d for which kernels are compiled.
+constexpr uint32_t kMaxDegree = 256;
+
+// Kernel-parameter copy of the twiddles for thread-per-poly kernels (d <= 64).
+template <int D>
+struct Tw1 {
+  FieldParams f;
+  uint32_t fw[D][2];
+  uint32_t iw[D][2];
+  uint32_t ninv[2];
+  uint32_t iw1n[2];
+};
+
+enum NttMode : int {
+  MODE_FWD = 0,     // coefficients -> twisted evaluations (natural order)
+  MODE_INV = 1,     // twisted evaluations -> coefficients
+  MODE_MULINV = 2,  // out = INTT(NTT(a) (.) b_evals)
+  MODE_POLYMUL = 3, // out = INTT(NTT(a) (.) NTT(b))  (negacyclic product)
+};
+
+struct DeviceScratch {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace grid
+
+struct grid_gpu_plan {
+  uint32_t q = 0, d = 0, log_d = 0;
+  int device = 0;
+  grid::FieldParams f{};
+  uint32_t generator = 0, psi = 0, omega = 0, n_inv = 0;  // Montgomery words
+  grid::TwiddleTable tw;
+  // Device copy of the twiddle table as uint2 {w, wq}: fw[d], iw[d], {ninv}, {izeta1*ninv}.
+  uint2* d_tw = nullptr;
+  int* d_err = nullptr;
+  cudaStream_t stream = nullptr;   // host-buffer entry points: first pipeline stream
+  cudaStream_t stream2 = nullptr;  // second pipeline stream
+  std::mutex mu;                   // serialises host-buffer calls and scratch growth
+  grid::DeviceScratch scratch[16];
+  int num_sms = 0;
+};
+
+struct grid_gpu_matrix {
+  grid_gpu_plan* plan = nullptr;
+  size_t rows = 0, cols = 0;
+  uint32_t* d_evals = nullptr;  // rows x cols polys in the twisted evaluation domain
+};
+
+namespace grid {
+
+// ntt.cu
+int launch_ntt(const grid_gpu_plan* p, int mode, const uint32_t* a, const uint32_t* b,
+               uint32_t* out, size_t npolys, cudaStream_t s);
+int ntt_max_degree();
+
+// commit.cu
+int launch_matvec(const grid_gpu_plan* p, const uint32_t* a_evals, size_t rows, size_t cols,
+                  const uint32_t* s_evals, size_t batch, uint32_t* t_evals, int accumulate,
+                  cudaStream_t s);
+int launch_gram(const grid_gpu_plan* p, const uint32_t* s_evals, size_t r, size_t n,
+                uint32_t* g_evals, cudaStream_t s);
+int launch_pointwise(const grid_gpu_plan* p, uint32_t* dst, const uint32_t* rhs, size_t words,
+                     cudaStream_t s);
+int launch_add(const grid_gpu_plan* p, uint32_t* dst, const uint32_t* rhs, size_t words,
+               cudaStream_t s);
+
+// decompose.cu
+int launch_decompose_balanced(const grid_gpu_plan* p, const uint32_t* polys, size_t npolys,
+                              uint64_t base, size_t num_limbs, uint32_t* out, cudaStream_t s);
+int launch_gadget_decompose(const grid_gpu_plan* p, const uint32_t* x, size_t len,
+                            uint64_t base, size_t digits, uint32_t* out, cudaStream_t s);
+
+// jl.cu
+int launch_jl_project(const FieldParams& f, const uint8_t seed[32], size_t rows,
+                      const uint32_t* parts, size_t num_parts, size_t cols, size_t d,
+                      uint32_t* p_out, int8_t* flat_out, void* scratch, size_t scratch_bytes,
+                      int num_sms, int* d_err, cudaStream_t s);
+size_t jl_scratch_bytes(size_t rows, size_t num_parts, int num_sms);
+
+// helpers
+int cuda_status(cudaError_t e);
+int ensure_scratch(grid_gpu_plan* p, int slot, size_t bytes);
+
+constexpr int kMaxDevices = 64;
+
+// Sets the dynamic shared-memory limit of `kernel` once per device and caches
+// its resident blocks per SM (idempotent; benign if two threads race).
+template <typename K>
+int prepare_kernel(K kernel, size_t smem, int threads, int dev, int* cache, int* bps_out) {
+  if (dev < 0 || dev >= kMaxDevices) return GRID_ERR_INVALID_PARAMETERS;
+  if (cache[dev] == 0) {
+    cudaError_t e =
+        cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_status(e);
+    int bps = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kernel, threads, smem);
+    if (e != cudaSuccess) return cuda_status(e);
+    cache[dev] = bps < 1 ? 1 : bps;
+  }
+  *bps_out = cache[dev];
+  return GRID_OK;
+}
+
+}  // namespace grid

@@ -1,0 +1,543 @@
+// Batched twisted negacyclic NTT / INTT kernels for R_q = Z_q[X]/(X^d + 1).
+//
+// Reference path replaced: TwistedNttPlan::{forward,inverse}_in_place_trusted
+// (algebra/src/poly/ntt.rs:75-104) over the bit-reverse + DIT forward and
+// GS + n^-1 + bit-reverse inverse (algebra/src/arith/ntt.rs:620-681), and the
+// config-style "NTT -> Montgomery pointwise -> INTT" chain.
+//
+// Design (sm_100a):
+//  * The twist by psi^i, the bit-reversal and the n^-1 scale are folded into
+//    a merged Cooley-Tukey / Gentleman-Sande pair with twiddles psi^brv(k).
+//    The forward transform leaves evaluation x(psi^(2*brv(j)+1)) in register
+//    j; the reference's natural-order slot k is register brv(k), so output
+//    ordering is pure register renaming at the store.
+//  * One warp streams tiles of 32 (d <= 64) or 32/T (d = 128, 256) polys.
+//    Tiles move HBM <-> shared memory with TMA bulk copies (one 256-byte piece
+//    per lane) into 16-byte-padded slots, so per-thread 128-bit shared loads
+//    are bank-conflict free; mbarriers track arrival, bulk-group waits track
+//    store completion, and the next tile's input is prefetched into the other
+//    buffer while the current tile computes.
+//  * d <= 64: one thread holds a whole polynomial in registers; every twiddle
+//    index is a compile-time constant, so twiddles come from the kernel
+//    parameter block (constant bank operands).
+//  * d = 128 / 256: T = 2 / 4 threads per polynomial, 64 coefficients each;
+//    log2(T) stages cross threads through warp shuffles; twiddles are staged
+//    once per block into shared memory.
+#include <cuda_runtime.h>
+
+#include "grid_async.cuh"
+#include "grid_field.cuh"
+#include "grid_internal.h"
+
+namespace grid {
+namespace {
+
+constexpr int kWarpsPerBlock = 4;
+constexpr int kThreads = kWarpsPerBlock * 32;
+
+__host__ __device__ constexpr int ilog2(int x) { return x <= 1 ? 0 : 1 + ilog2(x >> 1); }
+
+__host__ __device__ constexpr int brv(int x, int bits) {
+  int r = 0;
+  for (int i = 0; i < bits; ++i) r |= ((x >> i) & 1) << (bits - 1 - i);
+  return r;
+}
+
+__device__ __forceinline__ void ct_bfly(uint32_t& u, uint32_t& v, uint32_t w, uint32_t wq,
+                                        uint32_t q) {
+  const uint32_t t = mont_mul_c(v, w, wq, q);
+  v = sub_mod(u, t, q);
+  u = add_mod(u, t, q);
+}
+
+__device__ __forceinline__ void gs_bfly(uint32_t& u, uint32_t& v, uint32_t w, uint32_t wq,
+                                        uint32_t q) {
+  const uint32_t s = add_mod(u, v, q);
+  const uint32_t d = sub_mod(u, v, q);
+  u = s;
+  v = mont_mul_c(d, w, wq, q);
+}
+
+// ---------------------------------------------------------------------------
+// Thread-per-polynomial transforms (d <= 64). x holds positions 0..D-1.
+// ---------------------------------------------------------------------------
+template <int D, int LEN>
+__device__ __forceinline__ void fwd1_stages(uint32_t (&x)[D], const Tw1<D>& tw) {
+  const uint32_t q = tw.f.q;
+#pragma unroll
+  for (int g = 0; g < D / (2 * LEN); ++g) {
+    const int k = D / (2 * LEN) + g;
+#pragma unroll
+    for (int j = g * 2 * LEN; j < g * 2 * LEN + LEN; ++j)
+      ct_bfly(x[j], x[j + LEN], tw.fw[k][0], tw.fw[k][1], q);
+  }
+  if constexpr (LEN > 1) fwd1_stages<D, LEN / 2>(x, tw);
+}
+
+template <int D, int LEN>
+__device__ __forceinline__ void inv1_stages(uint32_t (&x)[D], const Tw1<D>& tw) {
+  const uint32_t q = tw.f.q;
+  if constexpr (LEN == D / 2) {
+    // Last GS stage (single group, k = 1) with d^-1 folded in.
+#pragma unroll
+    for (int j = 0; j < LEN; ++j) {
+      const uint32_t s = add_mod(x[j], x[j + LEN], q);
+      const uint32_t d = sub_mod(x[j], x[j + LEN], q);
+      x[j] = mont_mul_c(s, tw.ninv[0], tw.ninv[1], q);
+      x[j + LEN] = mont_mul_c(d, tw.iw1n[0], tw.iw1n[1], q);
+    }
+  } else {
+#pragma unroll
+    for (int g = 0; g < D / (2 * LEN); ++g) {
+      const int k = D / (2 * LEN) + g;
+#pragma unroll
+      for (int j = g * 2 * LEN; j < g * 2 * LEN + LEN; ++j)
+        gs_bfly(x[j], x[j + LEN], tw.iw[k][0], tw.iw[k][1], q);
+    }
+    inv1_stages<D, LEN * 2>(x, tw);
+  }
+}
+
+template <int D, int MODE>
+__global__ void __launch_bounds__(kThreads) ntt1_kernel(const uint32_t* __restrict__ a,
+                                                        const uint32_t* __restrict__ b,
+                                                        uint32_t* out, unsigned long long npolys,
+                                                        const __grid_constant__ Tw1<D> tw,
+                                                        int* __restrict__ err) {
+  constexpr int LOGD = ilog2(D);
+  constexpr int PS = D + 4;                 // padded slot stride (words)
+  constexpr uint32_t PIECE = D * 4;         // bytes each lane moves per tile
+  constexpr int BUF = 32 * PS;              // words per tile buffer
+  extern __shared__ __align__(128) uint32_t smem[];
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  uint32_t* wbase = smem + warp * 2 * BUF;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kWarpsPerBlock * 2 * BUF) + warp * 4;
+  if (lane == 0) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) mbar_init(&bars[i], 1);
+    fence_mbar_init();
+  }
+  __syncwarp();
+
+  const unsigned long long ntiles = (npolys + 31) >> 5;
+  const unsigned long long stride = (unsigned long long)gridDim.x * kWarpsPerBlock;
+  unsigned long long tile = (unsigned long long)blockIdx.x * kWarpsPerBlock + warp;
+  uint32_t parity = 0, pending = 0;
+
+  auto issue = [&](uint32_t* buf, const uint32_t* src, unsigned long long t, int bar) {
+    const unsigned long long p0 = t << 5;
+    const unsigned long long left = npolys - p0;
+    const uint32_t np = left < 32 ? (uint32_t)left : 32u;
+    if (lane == 0) mbar_arrive_expect_tx(&bars[bar], np * PIECE);
+    __syncwarp();
+    if ((uint32_t)lane < np) bulk_load(buf + lane * PS, src + (p0 + lane) * D, PIECE, &bars[bar]);
+    pending |= 1u << bar;
+  };
+  auto wait = [&](int bar) -> bool {
+    const bool ok = mbar_wait(&bars[bar], (parity >> bar) & 1u, err);
+    parity ^= 1u << bar;
+    pending &= ~(1u << bar);
+    return __all_sync(0xffffffffu, ok);  // keep the warp's control flow uniform
+  };
+
+  bool ok = true;
+  int buf = 0;
+  if (tile < ntiles) issue(wbase, a, tile, 0);
+  for (; tile < ntiles; tile += stride, buf ^= 1) {
+    uint32_t* s = wbase + buf * BUF;
+    uint32_t* slot = s + lane * PS;
+    const unsigned long long p0 = tile << 5;
+    const unsigned long long left = npolys - p0;
+    const uint32_t np = left < 32 ? (uint32_t)left : 32u;
+
+    if (!wait(buf * 2)) { ok = false; break; }
+    uint32_t x[D];
+    const uint4* sv = reinterpret_cast<const uint4*>(slot);
+#pragma unroll
+    for (int c = 0; c < D / 4; ++c) {
+      const uint4 v = sv[c];
+      if constexpr (MODE == MODE_INV) {
+        x[brv(4 * c + 0, LOGD)] = v.x;
+        x[brv(4 * c + 1, LOGD)] = v.y;
+        x[brv(4 * c + 2, LOGD)] = v.z;
+        x[brv(4 * c + 3, LOGD)] = v.w;
+      } else {
+        x[4 * c + 0] = v.x;
+        x[4 * c + 1] = v.y;
+        x[4 * c + 2] = v.z;
+        x[4 * c + 3] = v.w;
+      }
+    }
+    fence_proxy_async_smem();
+    __syncwarp();
+    const unsigned long long next = tile + stride;
+    if (next < ntiles) {
+      bulk_wait_read_all();
+      __syncwarp();
+      issue(wbase + (buf ^ 1) * BUF, a, next, (buf ^ 1) * 2);
+    }
+    if constexpr (MODE == MODE_MULINV) issue(s, b, tile, buf * 2 + 1);
+
+    if constexpr (MODE != MODE_INV) fwd1_stages<D, D / 2>(x, tw);
+    if constexpr (MODE == MODE_MULINV) {
+      if (!wait(buf * 2 + 1)) { ok = false; break; }
+      const uint32_t q = tw.f.q, qinv = tw.f.qinv;
+#pragma unroll
+      for (int c = 0; c < D / 4; ++c) {
+        const uint4 v = sv[c];
+        x[brv(4 * c + 0, LOGD)] = mont_mul(x[brv(4 * c + 0, LOGD)], v.x, q, qinv);
+        x[brv(4 * c + 1, LOGD)] = mont_mul(x[brv(4 * c + 1, LOGD)], v.y, q, qinv);
+        x[brv(4 * c + 2, LOGD)] = mont_mul(x[brv(4 * c + 2, LOGD)], v.z, q, qinv);
+        x[brv(4 * c + 3, LOGD)] = mont_mul(x[brv(4 * c + 3, LOGD)], v.w, q, qinv);
+      }
+    }
+    if constexpr (MODE != MODE_FWD) inv1_stages<D, 1>(x, tw);
+
+    uint4* so = reinterpret_cast<uint4*>(slot);
+#pragma unroll
+    for (int c = 0; c < D / 4; ++c) {
+      if constexpr (MODE == MODE_FWD) {
+        so[c] = make_uint4(x[brv(4 * c + 0, LOGD)], x[brv(4 * c + 1, LOGD)],
+                           x[brv(4 * c + 2, LOGD)], x[brv(4 * c + 3, LOGD)]);
+      } else {
+        so[c] = make_uint4(x[4 * c + 0], x[4 * c + 1], x[4 * c + 2], x[4 * c + 3]);
+      }
+    }
+    fence_proxy_async_smem();
+    if ((uint32_t)lane < np) {
+      bulk_store(out + (p0 + lane) * D, slot, PIECE);
+      bulk_commit();
+    }
+  }
+  if (!ok) {
+    // Let copies already in flight land before the block's shared memory goes away.
+    for (int bar = 0; bar < 4; ++bar)
+      if (pending & (1u << bar)) mbar_wait(&bars[bar], (parity >> bar) & 1u, err);
+  }
+  bulk_wait_all();
+}
+
+// ---------------------------------------------------------------------------
+// T threads per polynomial (d = 128, 256). Thread t of a polynomial holds the
+// 4-word chunks c = T*m + t (m = 0 .. D/(4T)-1): local element e = 4m + s is
+// global position i = 4T*m + 4t + s.
+// ---------------------------------------------------------------------------
+template <int D, int T, int LEN>
+__device__ __forceinline__ void fwdT_stages(uint32_t (&x)[D / T], const uint2* __restrict__ tws,
+                                            int t, uint32_t q) {
+  constexpr int E = D / T;
+  constexpr int LOG2LEN = ilog2(2 * LEN);
+  if constexpr (LEN >= 4 * T) {
+    constexpr int STEP = LEN / T;
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      if ((e & STEP) == 0) {
+        const int k = D / (2 * LEN) + ((4 * T * (e >> 2)) >> LOG2LEN);
+        const uint2 w = tws[k];
+        ct_bfly(x[e], x[e + STEP], w.x, w.y, q);
+      }
+    }
+  } else if constexpr (LEN >= 4) {
+    constexpr int M = LEN / 4;
+    const bool upper = (t & M) != 0;
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const int k = D / (2 * LEN) + ((4 * T * (e >> 2) + 4 * t) >> LOG2LEN);
+      const uint2 w = tws[k];
+      const uint32_t prod = mont_mul_c(x[e], w.x, w.y, q);
+      const uint32_t mine = upper ? prod : x[e];
+      const uint32_t other = __shfl_xor_sync(0xffffffffu, mine, M);
+      x[e] = upper ? sub_mod(other, mine, q) : add_mod(mine, other, q);
+    }
+  } else {
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      if ((e & LEN) == 0) {
+        const int k = D / (2 * LEN) + ((4 * T * (e >> 2) + 4 * t + (e & 3)) >> LOG2LEN);
+        const uint2 w = tws[k];
+        ct_bfly(x[e], x[e + LEN], w.x, w.y, q);
+      }
+    }
+  }
+  if constexpr (LEN > 1) fwdT_stages<D, T, LEN / 2>(x, tws, t, q);
+}
+
+template <int D, int T, int LEN>
+__device__ __forceinline__ void invT_stages(uint32_t (&x)[D / T], const uint2* __restrict__ tws,
+                                            int t, uint32_t q) {
+  constexpr int E = D / T;
+  constexpr int LOG2LEN = ilog2(2 * LEN);
+  const uint2* iw = tws + D;
+  if constexpr (LEN == D / 2) {
+    static_assert(LEN >= 4 * T, "last stage must be thread-local");
+    constexpr int STEP = LEN / T;
+    const uint2 n0 = tws[2 * D], n1 = tws[2 * D + 1];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      if ((e & STEP) == 0) {
+        const uint32_t s = add_mod(x[e], x[e + STEP], q);
+        const uint32_t d = sub_mod(x[e], x[e + STEP], q);
+        x[e] = mont_mul_c(s, n0.x, n0.y, q);
+        x[e + STEP] = mont_mul_c(d, n1.x, n1.y, q);
+      }
+    }
+  } else {
+    if constexpr (LEN >= 4 * T) {
+      constexpr int STEP = LEN / T;
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        if ((e & STEP) == 0) {
+          const int k = D / (2 * LEN) + ((4 * T * (e >> 2)) >> LOG2LEN);
+          const uint2 w = iw[k];
+          gs_bfly(x[e], x[e + STEP], w.x, w.y, q);
+        }
+      }
+    } else if constexpr (LEN >= 4) {
+      constexpr int M = LEN / 4;
+      const bool upper = (t & M) != 0;
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const int k = D / (2 * LEN) + ((4 * T * (e >> 2) + 4 * t) >> LOG2LEN);
+        const uint2 w = iw[k];
+        const uint32_t other = __shfl_xor_sync(0xffffffffu, x[e], M);
+        // lower keeps u + v; upper gets (u - v) * w with u = other, v = x[e]
+        const uint32_t s = upper ? sub_mod(other, x[e], q) : add_mod(x[e], other, q);
+        const uint32_t prod = mont_mul_c(s, w.x, w.y, q);
+        x[e] = upper ? prod : s;
+      }
+    } else {
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        if ((e & LEN) == 0) {
+          const int k = D / (2 * LEN) + ((4 * T * (e >> 2) + 4 * t + (e & 3)) >> LOG2LEN);
+          const uint2 w = iw[k];
+          gs_bfly(x[e], x[e + LEN], w.x, w.y, q);
+        }
+      }
+    }
+    invT_stages<D, T, LEN * 2>(x, tws, t, q);
+  }
+}
+
+template <int D, int T, int MODE>
+__global__ void __launch_bounds__(kThreads) nttT_kernel(const uint32_t* __restrict__ a,
+                                                        const uint32_t* __restrict__ b,
+                                                        uint32_t* out, unsigned long long npolys,
+                                                        const uint2* __restrict__ gtw,
+                                                        FieldParams f, int* __restrict__ err) {
+  constexpr int LOGD = ilog2(D);
+  constexpr int E = D / T;                   // words per thread
+  constexpr int PW = 32 / T;                 // polys per warp tile
+  constexpr int PS = D + 4 * T;              // padded slot stride (words)
+  constexpr uint32_t PIECE = E * 4;          // bytes each lane moves
+  constexpr int BUF = PW * PS;
+  constexpr int TWN = 2 * D + 2;             // uint2 twiddle entries
+  extern __shared__ __align__(128) uint32_t smem[];
+  uint2* tws = reinterpret_cast<uint2*>(smem);
+  uint32_t* tiles = smem + 2 * TWN + 4;      // keep 16-byte alignment
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int pl = lane / T;                   // poly within tile
+  const int t = lane % T;
+  for (int i = threadIdx.x; i < TWN; i += blockDim.x) tws[i] = gtw[i];
+  uint32_t* wbase = tiles + warp * 2 * BUF;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(tiles + kWarpsPerBlock * 2 * BUF) + warp * 4;
+  if (lane == 0) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) mbar_init(&bars[i], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+
+  const unsigned long long ntiles = (npolys + PW - 1) / PW;
+  const unsigned long long stride = (unsigned long long)gridDim.x * kWarpsPerBlock;
+  unsigned long long tile = (unsigned long long)blockIdx.x * kWarpsPerBlock + warp;
+  uint32_t parity = 0, pending = 0;
+  const uint32_t q = f.q, qinv = f.qinv;
+  const int bt = brv(4 * t, LOGD);           // bit-reversed contribution of t
+
+  auto issue = [&](uint32_t* buf, const uint32_t* src, unsigned long long tl, int bar) {
+    const unsigned long long p0 = tl * PW;
+    const unsigned long long left = npolys - p0;
+    const uint32_t np = left < (unsigned long long)PW ? (uint32_t)left : (uint32_t)PW;
+    if (lane == 0) mbar_arrive_expect_tx(&bars[bar], np * D * 4);
+    __syncwarp();
+    if ((uint32_t)pl < np)
+      bulk_load(buf + pl * PS + t * E, src + (p0 + pl) * D + t * E, PIECE, &bars[bar]);
+    pending |= 1u << bar;
+  };
+  auto wait = [&](int bar) -> bool {
+    const bool ok = mbar_wait(&bars[bar], (parity >> bar) & 1u, err);
+    parity ^= 1u << bar;
+    pending &= ~(1u << bar);
+    return __all_sync(0xffffffffu, ok);  // keep the warp's control flow uniform
+  };
+
+  bool ok = true;
+  int buf = 0;
+  if (tile < ntiles) issue(wbase, a, tile, 0);
+  for (; tile < ntiles; tile += stride, buf ^= 1) {
+    uint32_t* s = wbase + buf * BUF;
+    uint32_t* slot = s + pl * PS;
+    const unsigned long long p0 = tile * PW;
+    const unsigned long long left = npolys - p0;
+    const uint32_t np = left < (unsigned long long)PW ? (uint32_t)left : (uint32_t)PW;
+
+    if (!wait(buf * 2)) { ok = false; break; }
+    uint32_t x[E];
+    if constexpr (MODE == MODE_INV) {
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const int i = 4 * T * (e >> 2) + (e & 3);
+        x[e] = slot[brv(i, LOGD) | bt];
+      }
+    } else {
+#pragma unroll
+      for (int m = 0; m < E / 4; ++m) {
+        const uint4 v = reinterpret_cast<const uint4*>(slot)[T * m + t];
+        x[4 * m + 0] = v.x;
+        x[4 * m + 1] = v.y;
+        x[4 * m + 2] = v.z;
+        x[4 * m + 3] = v.w;
+      }
+    }
+    fence_proxy_async_smem();
+    __syncwarp();
+    const unsigned long long next = tile + stride;
+    if (next < ntiles) {
+      bulk_wait_read_all();
+      __syncwarp();
+      issue(wbase + (buf ^ 1) * BUF, a, next, (buf ^ 1) * 2);
+    }
+    if constexpr (MODE == MODE_MULINV) issue(s, b, tile, buf * 2 + 1);
+
+    if constexpr (MODE != MODE_INV) fwdT_stages<D, T, D / 2>(x, tws, t, q);
+    if constexpr (MODE == MODE_MULINV) {
+      if (!wait(buf * 2 + 1)) { ok = false; break; }
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const int i = 4 * T * (e >> 2) + (e & 3);
+        x[e] = mont_mul(x[e], slot[brv(i, LOGD) | bt], q, qinv);
+      }
+    }
+    if constexpr (MODE != MODE_FWD) invT_stages<D, T, 1>(x, tws, t, q);
+
+    __syncwarp();  // every lane done reading the slot before it is overwritten
+    if constexpr (MODE == MODE_FWD) {
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const int i = 4 * T * (e >> 2) + (e & 3);
+        slot[brv(i, LOGD) | bt] = x[e];
+      }
+    } else {
+#pragma unroll
+      for (int m = 0; m < E / 4; ++m)
+        reinterpret_cast<uint4*>(slot)[T * m + t] =
+            make_uint4(x[4 * m + 0], x[4 * m + 1], x[4 * m + 2], x[4 * m + 3]);
+    }
+    fence_proxy_async_smem();
+    __syncwarp();  // pieces span other lanes' chunks
+    if ((uint32_t)pl < np) {
+      bulk_store(out + (p0 + pl) * D + t * E, slot + t * E, PIECE);
+      bulk_commit();
+    }
+  }
+  if (!ok) {
+    for (int bar = 0; bar < 4; ++bar)
+      if (pending & (1u << bar)) mbar_wait(&bars[bar], (parity >> bar) & 1u, err);
+  }
+  bulk_wait_all();
+}
+
+// ---------------------------------------------------------------------------
+// Host launchers
+// ---------------------------------------------------------------------------
+template <int D>
+Tw1<D> make_tw1(const grid_gpu_plan* p) {
+  Tw1<D> tw{};
+  tw.f = p->f;
+  for (int k = 0; k < D; ++k) {
+    tw.fw[k][0] = p->tw.zeta[k];
+    tw.fw[k][1] = p->tw.zeta_q[k];
+    tw.iw[k][0] = p->tw.izeta[k];
+    tw.iw[k][1] = p->tw.izeta_q[k];
+  }
+  tw.ninv[0] = p->tw.ninv;
+  tw.ninv[1] = p->tw.ninv_q;
+  tw.iw1n[0] = p->tw.izeta1_ninv;
+  tw.iw1n[1] = p->tw.izeta1_ninv_q;
+  return tw;
+}
+
+int grid_size(const grid_gpu_plan* p, unsigned long long tiles, int blocks_per_sm) {
+  const unsigned long long want = (tiles + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  const unsigned long long cap = (unsigned long long)p->num_sms * blocks_per_sm;
+  unsigned long long g = want < cap ? want : cap;
+  return g < 1 ? 1 : (int)g;
+}
+
+template <int D, int MODE>
+int run1(const grid_gpu_plan* p, const uint32_t* a, const uint32_t* b, uint32_t* out,
+         size_t npolys, cudaStream_t s) {
+  constexpr int PS = D + 4;
+  constexpr size_t smem = (size_t)kWarpsPerBlock * 2 * 32 * PS * 4 + kWarpsPerBlock * 4 * 8;
+  static int bps_cache[kMaxDevices] = {};
+  int bps = 0;
+  const int st = prepare_kernel(ntt1_kernel<D, MODE>, smem, kThreads, p->device, bps_cache, &bps);
+  if (st) return st;
+  const unsigned long long tiles = (npolys + 31) / 32;
+  const Tw1<D> tw = make_tw1<D>(p);
+  ntt1_kernel<D, MODE><<<grid_size(p, tiles, bps), kThreads, smem, s>>>(
+      a, b, out, (unsigned long long)npolys, tw, p->d_err);
+  return cuda_status(cudaGetLastError());
+}
+
+template <int D, int T, int MODE>
+int runT(const grid_gpu_plan* p, const uint32_t* a, const uint32_t* b, uint32_t* out,
+         size_t npolys, cudaStream_t s) {
+  constexpr int PW = 32 / T;
+  constexpr int PS = D + 4 * T;
+  constexpr size_t smem =
+      (size_t)(2 * (2 * D + 2) + 4) * 4 + (size_t)kWarpsPerBlock * 2 * PW * PS * 4 +
+      kWarpsPerBlock * 4 * 8;
+  static int bps_cache[kMaxDevices] = {};
+  int bps = 0;
+  const int st = prepare_kernel(nttT_kernel<D, T, MODE>, smem, kThreads, p->device, bps_cache, &bps);
+  if (st) return st;
+  const unsigned long long tiles = (npolys + PW - 1) / PW;
+  nttT_kernel<D, T, MODE><<<grid_size(p, tiles, bps), kThreads, smem, s>>>(
+      a, b, out, (unsigned long long)npolys, p->d_tw, p->f, p->d_err);
+  return cuda_status(cudaGetLastError());
+}
+
+template <int MODE>
+int dispatch(const grid_gpu_plan* p, const uint32_t* a, const uint32_t* b, uint32_t* out,
+             size_t n, cudaStream_t s) {
+  switch (p->d) {
+    case 8: return run1<8, MODE>(p, a, b, out, n, s);
+    case 16: return run1<16, MODE>(p, a, b, out, n, s);
+    case 32: return run1<32, MODE>(p, a, b, out, n, s);
+    case 64: return run1<64, MODE>(p, a, b, out, n, s);
+    case 128: return runT<128, 2, MODE>(p, a, b, out, n, s);
+    case 256: return runT<256, 4, MODE>(p, a, b, out, n, s);
+    default: return GRID_ERR_UNSUPPORTED_DEGREE;
+  }
+}
+
+}  // namespace
+
+int ntt_max_degree() { return (int)kMaxDegree; }
+
+int launch_ntt(const grid_gpu_plan* p, int mode, const uint32_t* a, const uint32_t* b,
+               uint32_t* out, size_t npolys, cudaStream_t s) {
+  if (npolys == 0) return GRID_OK;
+  switch (mode) {
+    case MODE_FWD: return dispatch<MODE_FWD>(p, a, nullptr, out, npolys, s);
+    case MODE_INV: return dispatch<MODE_INV>(p, a, nullptr, out, npolys, s);
+    case MODE_MULINV: return dispatch<MODE_MULINV>(p, a, b, out, npolys, s);
+    default: return GRID_ERR_INVALID_PARAMETERS;
+  }
+}
+
+}  // namespace grid

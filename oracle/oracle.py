@@ -1,0 +1,339 @@
+"""ctypes wrapper around the C oracle (test infrastructure only).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this module. Arrays are numpy uint32 Montgomery words (PrimeField<Q, u32>).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import build as _build
+
+_u32p = C.POINTER(C.c_uint32)
+_i64p = C.POINTER(C.c_int64)
+_i8p = C.POINTER(C.c_int8)
+_u8p = C.POINTER(C.c_uint8)
+
+_LIB = None
+
+
+class OracleError(RuntimeError):
+    def __init__(self, code: int, what: str = ""):
+        super().__init__(f"oracle error {code} {what}")
+        self.code = code
+
+
+class _Field(C.Structure):
+    _fields_ = [("q", C.c_uint32), ("r_mod_q", C.c_uint32), ("r2_mod_q", C.c_uint32),
+                ("q_inv", C.c_uint32)]
+
+
+class _Plan(C.Structure):
+    _fields_ = [("f", _Field), ("n", C.c_uint32), ("generator", C.c_uint32),
+                ("omega", C.c_uint32), ("psi", C.c_uint32), ("inv_scale", C.c_uint32),
+                ("fwd_tw", _u32p), ("inv_tw", _u32p), ("twists", _u32p), ("untwists", _u32p)]
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = _build.build()
+        L = C.CDLL(path)
+        fp = C.POINTER(_Field)
+        pp = C.POINTER(_Plan)
+        sig = {
+            "orc_field_init": (C.c_int, [fp, C.c_uint64]),
+            "orc_to_mont": (C.c_uint32, [fp, C.c_uint64]),
+            "orc_from_mont": (C.c_uint32, [fp, C.c_uint32]),
+            "orc_add": (C.c_uint32, [fp, C.c_uint32, C.c_uint32]),
+            "orc_sub": (C.c_uint32, [fp, C.c_uint32, C.c_uint32]),
+            "orc_mul": (C.c_uint32, [fp, C.c_uint32, C.c_uint32]),
+            "orc_pow": (C.c_uint32, [fp, C.c_uint32, C.c_uint64]),
+            "orc_inv": (C.c_uint32, [fp, C.c_uint32]),
+            "orc_is_prime_u64": (C.c_int, [C.c_uint64]),
+            "orc_plan_create": (C.c_int, [pp, C.c_uint64, C.c_uint64]),
+            "orc_plan_destroy": (None, [pp]),
+            "orc_max_ntt_size": (C.c_uint64, [C.c_uint64]),
+            "orc_find_generator": (C.c_uint32, [fp]),
+            "orc_ntt_forward": (None, [pp, _u32p]),
+            "orc_ntt_inverse": (None, [pp, _u32p]),
+            "orc_twisted_forward": (None, [pp, _u32p, C.c_size_t]),
+            "orc_twisted_inverse": (None, [pp, _u32p, C.c_size_t]),
+            "orc_ntt_mul_inverse": (None, [pp, _u32p, _u32p, _u32p, C.c_size_t]),
+            "orc_ntt_mul_inverse_mt": (None, [pp, _u32p, _u32p, _u32p, C.c_size_t, C.c_int]),
+            "orc_poly_mul_ntt": (None, [pp, _u32p, _u32p, _u32p]),
+            "orc_naive_negacyclic": (None, [fp, C.c_uint32, _u32p, _u32p, _u32p]),
+            "orc_pointwise_mul": (None, [fp, _u32p, _u32p, C.c_size_t]),
+            "orc_matvec": (C.c_int, [pp, _u32p, C.c_size_t, C.c_size_t, C.c_int, _u32p,
+                                     C.c_size_t, _u32p]),
+            "orc_matvec_mt": (C.c_int, [pp, _u32p, C.c_size_t, C.c_size_t, C.c_int, _u32p,
+                                        C.c_size_t, _u32p, C.c_int]),
+            "orc_linear_commit": (C.c_int, [pp, _u32p, C.c_size_t, C.c_size_t, _u32p,
+                                            C.c_size_t, _u32p, _u32p, _u32p]),
+            "orc_gram": (C.c_int, [pp, _u32p, C.c_size_t, C.c_size_t, _u32p, C.c_int]),
+            "orc_gram_naive": (C.c_int, [pp, _u32p, C.c_size_t, C.c_size_t, _u32p]),
+            "orc_garbage_index": (C.c_size_t, [C.c_size_t, C.c_size_t, C.c_size_t]),
+            "orc_decompose_coeff_balanced": (None, [C.c_uint64, C.c_uint64, C.c_size_t,
+                                                    C.c_uint64, _i64p]),
+            "orc_centered_mod": (C.c_int64, [C.c_int64, C.c_int64]),
+            "orc_decompose_polys": (C.c_int, [fp, C.c_uint32, _u32p, C.c_size_t, C.c_uint64,
+                                              C.c_size_t, _u32p]),
+            "orc_reconstruct_from_limbs": (C.c_int, [fp, C.c_uint32, _u32p, C.c_size_t,
+                                                     C.c_uint64, _u32p]),
+            "orc_gadget_digits": (C.c_size_t, [C.c_uint64, C.c_uint64]),
+            "orc_gadget_decompose": (C.c_int, [fp, _u32p, C.c_size_t, C.c_uint64, _u32p]),
+            "orc_chacha20_block": (None, [_u8p, C.c_uint32, _u8p, _u8p]),
+            "orc_chacha20_quarter": (None, [_u32p, _u32p, _u32p, _u32p]),
+            "orc_jl_project": (C.c_int, [fp, _u8p, C.c_size_t, C.c_size_t, _u32p, C.c_size_t,
+                                         C.c_size_t, _u32p, _i8p, C.c_int]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _LIB = L
+    return _LIB
+
+
+def _u32(a):
+    a = np.ascontiguousarray(a, dtype=np.uint32)
+    return a, a.ctypes.data_as(_u32p)
+
+
+class Field:
+    def __init__(self, q: int):
+        self.s = _Field()
+        st = lib().orc_field_init(C.byref(self.s), q)
+        if st:
+            raise OracleError(st, f"q={q}")
+        self.q = q
+
+    def to_mont(self, v):
+        v = np.asarray(v, dtype=np.uint64).ravel()
+        out = np.empty(v.shape, dtype=np.uint32)
+        L = lib()
+        for i, x in enumerate(v):
+            out[i] = L.orc_to_mont(C.byref(self.s), int(x))
+        return out
+
+    def from_mont(self, w):
+        w = np.asarray(w, dtype=np.uint32).ravel()
+        L = lib()
+        return np.array([L.orc_from_mont(C.byref(self.s), int(x)) for x in w], dtype=np.uint64)
+
+    def mul(self, a: int, b: int) -> int:
+        return lib().orc_mul(C.byref(self.s), a, b)
+
+    def add(self, a: int, b: int) -> int:
+        return lib().orc_add(C.byref(self.s), a, b)
+
+    def sub(self, a: int, b: int) -> int:
+        return lib().orc_sub(C.byref(self.s), a, b)
+
+    def pow(self, a: int, e: int) -> int:
+        return lib().orc_pow(C.byref(self.s), a, e)
+
+    def one(self) -> int:
+        return self.s.r_mod_q
+
+
+class Plan:
+    """Twisted negacyclic plan of length n (mirrors TwistedNttPlan::build)."""
+
+    def __init__(self, q: int, n: int):
+        self.s = _Plan()
+        st = lib().orc_plan_create(C.byref(self.s), q, n)
+        if st:
+            lib().orc_plan_destroy(C.byref(self.s))
+            raise OracleError(st, f"q={q} n={n}")
+        self.q, self.n = q, n
+        self.field = Field(q)
+
+    def __del__(self):
+        try:
+            lib().orc_plan_destroy(C.byref(self.s))
+        except Exception:
+            pass
+
+    def _ref(self):
+        return C.byref(self.s)
+
+    def tables(self):
+        n = self.n
+        get = lambda p, k: np.ctypeslib.as_array(p, shape=(k,)).copy() if k else np.empty(0, np.uint32)
+        return {
+            "fwd_tw": get(self.s.fwd_tw, n - 1), "inv_tw": get(self.s.inv_tw, n - 1),
+            "twists": get(self.s.twists, n), "untwists": get(self.s.untwists, n),
+            "generator": self.s.generator, "omega": self.s.omega, "psi": self.s.psi,
+            "inv_scale": self.s.inv_scale,
+        }
+
+    def forward(self, polys):
+        a, p = _u32(np.array(polys, dtype=np.uint32, copy=True))
+        lib().orc_twisted_forward(self._ref(), p, a.size // self.n)
+        return a
+
+    def inverse(self, evals):
+        a, p = _u32(np.array(evals, dtype=np.uint32, copy=True))
+        lib().orc_twisted_inverse(self._ref(), p, a.size // self.n)
+        return a
+
+    def ntt_forward_cyclic(self, v):
+        a, p = _u32(np.array(v, dtype=np.uint32, copy=True))
+        lib().orc_ntt_forward(self._ref(), p)
+        return a
+
+    def ntt_inverse_cyclic(self, v):
+        a, p = _u32(np.array(v, dtype=np.uint32, copy=True))
+        lib().orc_ntt_inverse(self._ref(), p)
+        return a
+
+    def ntt_mul_inverse(self, a, b, threads: int = 1):
+        a, pa = _u32(a)
+        b, pb = _u32(b)
+        out = np.empty_like(a)
+        cnt = a.size // self.n
+        if threads == 1:
+            lib().orc_ntt_mul_inverse(self._ref(), pa, pb, out.ctypes.data_as(_u32p), cnt)
+        else:
+            lib().orc_ntt_mul_inverse_mt(self._ref(), pa, pb, out.ctypes.data_as(_u32p), cnt,
+                                         threads)
+        return out
+
+    def poly_mul(self, a, b):
+        a, pa = _u32(a)
+        b, pb = _u32(b)
+        out = np.empty(self.n, dtype=np.uint32)
+        lib().orc_poly_mul_ntt(self._ref(), pa, pb, out.ctypes.data_as(_u32p))
+        return out
+
+    def naive_negacyclic(self, a, b):
+        a, pa = _u32(a)
+        b, pb = _u32(b)
+        out = np.empty(self.n, dtype=np.uint32)
+        lib().orc_naive_negacyclic(C.byref(self.s.f), self.n, pa, pb, out.ctypes.data_as(_u32p))
+        return out
+
+    def matvec(self, A, rows, cols, s, batch, a_is_eval=False, threads=1):
+        A, pA = _u32(A)
+        s, ps = _u32(s)
+        t = np.empty(batch * rows * self.n, dtype=np.uint32)
+        if threads == 1:
+            st = lib().orc_matvec(self._ref(), pA, rows, cols, int(a_is_eval), ps, batch,
+                                  t.ctypes.data_as(_u32p))
+        else:
+            st = lib().orc_matvec_mt(self._ref(), pA, rows, cols, int(a_is_eval), ps, batch,
+                                     t.ctypes.data_as(_u32p), threads)
+        if st:
+            raise OracleError(st)
+        return t
+
+    def linear_commit(self, a_msg, rows, msg_cols, a_open, open_cols, m, r):
+        am, pam = _u32(a_msg)
+        ao, pao = _u32(a_open)
+        mm, pm = _u32(m)
+        rr, pr = _u32(r)
+        t = np.empty(rows * self.n, dtype=np.uint32)
+        st = lib().orc_linear_commit(self._ref(), pam, rows, msg_cols, pao, open_cols, pm, pr,
+                                     t.ctypes.data_as(_u32p))
+        if st:
+            raise OracleError(st)
+        return t
+
+    def gram(self, S, r, n, threads=0, naive=False):
+        S, pS = _u32(S)
+        G = np.empty(r * (r + 1) // 2 * self.n, dtype=np.uint32)
+        if naive:
+            st = lib().orc_gram_naive(self._ref(), pS, r, n, G.ctypes.data_as(_u32p))
+        else:
+            st = lib().orc_gram(self._ref(), pS, r, n, G.ctypes.data_as(_u32p), threads)
+        if st:
+            raise OracleError(st)
+        return G
+
+
+def decompose_coeff_balanced(c: int, base: int, num_limbs: int, q: int):
+    out = (C.c_int64 * num_limbs)()
+    lib().orc_decompose_coeff_balanced(c, base, num_limbs, q, out)
+    return list(out)
+
+
+def centered_mod(v: int, base: int) -> int:
+    return lib().orc_centered_mod(v, base)
+
+
+def garbage_index(r: int, i: int, j: int) -> int:
+    return lib().orc_garbage_index(r, i, j)
+
+
+def max_ntt_size(q: int) -> int:
+    return lib().orc_max_ntt_size(q)
+
+
+def is_prime(q: int) -> bool:
+    return bool(lib().orc_is_prime_u64(q))
+
+
+def decompose_polys(field: Field, d: int, polys, base: int, num_limbs: int):
+    p, pp = _u32(polys)
+    npolys = p.size // d
+    out = np.empty(npolys * num_limbs * d, dtype=np.uint32)
+    st = lib().orc_decompose_polys(C.byref(field.s), d, pp, npolys, base, num_limbs,
+                                   out.ctypes.data_as(_u32p))
+    if st:
+        raise OracleError(st)
+    return out
+
+
+def reconstruct_from_limbs(field: Field, d: int, limbs, base: int):
+    l, pl = _u32(limbs)
+    out = np.empty(d, dtype=np.uint32)
+    lib().orc_reconstruct_from_limbs(C.byref(field.s), d, pl, l.size // d, base,
+                                     out.ctypes.data_as(_u32p))
+    return out
+
+
+def gadget_digits(q: int, base: int) -> int:
+    return lib().orc_gadget_digits(q, base)
+
+
+def gadget_decompose(field: Field, x, base: int):
+    x, px = _u32(x)
+    k = gadget_digits(field.q, base)
+    out = np.empty(k * x.size, dtype=np.uint32)
+    st = lib().orc_gadget_decompose(C.byref(field.s), px, x.size, base, out.ctypes.data_as(_u32p))
+    if st:
+        raise OracleError(st)
+    return out.reshape(k, x.size)
+
+
+def chacha20_block(key: bytes, counter: int, nonce: bytes) -> bytes:
+    k = (C.c_uint8 * 32).from_buffer_copy(key)
+    n = (C.c_uint8 * 12).from_buffer_copy(nonce)
+    out = (C.c_uint8 * 64)()
+    lib().orc_chacha20_block(k, counter, n, out)
+    return bytes(out)
+
+
+def chacha20_quarter(a, b, c, d):
+    v = [C.c_uint32(x) for x in (a, b, c, d)]
+    lib().orc_chacha20_quarter(*[C.byref(x) for x in v])
+    return tuple(x.value for x in v)
+
+
+def jl_project(field: Field, seed: bytes, rows: int, parts, num_parts: int, cols: int, d: int,
+               want_flat: bool = True, threads: int = 0):
+    parts, pp = _u32(parts)
+    assert parts.size == num_parts * cols
+    sd = (C.c_uint8 * 32).from_buffer_copy(seed)
+    p = np.empty(rows, dtype=np.uint32)
+    flat = np.zeros(rows * num_parts * cols, dtype=np.int8) if want_flat else None
+    st = lib().orc_jl_project(C.byref(field.s), sd, rows, cols, pp, num_parts, d,
+                              p.ctypes.data_as(_u32p),
+                              flat.ctypes.data_as(_i8p) if want_flat else None, threads)
+    if st:
+        raise OracleError(st)
+    return p, flat
