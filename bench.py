@@ -181,6 +181,8 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     q, d, n = WORKLOADS[args.workload]
+    if args.polys:
+        n = args.polys
     plan = TwistedNttPlan(q, d)
     lib = _lib.load()
 
@@ -263,6 +265,8 @@ def run_ours(args, rank, world, local_rank):
     bytes_per_launch = 3 * 4 * d * n
     achieved = bytes_per_launch / (kernel_ms / 1e3) / 1e9
     traffic = _traffic(f"{args.workload}_mulinv")
+    if args.polys:
+        traffic = None
     line = {
         "metric": METRIC, "value": value, "unit": "polys/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
@@ -283,7 +287,7 @@ def run_ours(args, rank, world, local_rank):
         "clocks": sampler.summary(),
     }
     if world == 1:
-        line["cpu_baseline"] = cpu_baseline(q, d, n)
+        line["cpu_baseline"] = cpu_baseline(q, d, WORKLOADS[args.workload][2])
     print(json.dumps(line), flush=True)
 
 
@@ -294,6 +298,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="ntt64")
+    ap.add_argument("--polys", type=int, default=0,
+                    help="override the polynomial count (smaller cases for profiling)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 

@@ -130,6 +130,95 @@ int grid_gpu_ntt_mul_inverse(grid_gpu_plan* plan, const uint32_t* a, const uint3
 int grid_gpu_poly_mul(grid_gpu_plan* plan, const uint32_t* a, const uint32_t* b, uint32_t* out,
                       size_t npolys);
 
+/* ---- prepared matrices: the device-resident key cache of
+ *      PreparedLinearOps::build_linear_key_cache / build_matrix_cache
+ *      (commit/src/linear.rs:576-631, 690-715) ---------------------------- */
+
+/* Upload a rows x cols ring matrix (row-major polys) and keep its twisted
+ * evaluations resident on the device. a_is_evals = 1 takes A already in the
+ * evaluation domain (TwistedNttPoly::from_evals, poly/twisted_ntt.rs:47-49). */
+int grid_gpu_matrix_create(grid_gpu_plan* plan, const uint32_t* A, size_t rows, size_t cols,
+                           int a_is_evals, grid_gpu_matrix** out);
+int grid_gpu_matrix_create_dev(grid_gpu_plan* plan, const uint32_t* A, size_t rows, size_t cols,
+                               int a_is_evals, grid_gpu_matrix** out, void* stream);
+int grid_gpu_matrix_destroy(grid_gpu_matrix* m);
+int grid_gpu_matrix_shape(const grid_gpu_matrix* m, size_t* rows, size_t* cols);
+int grid_gpu_matrix_device_evals(const grid_gpu_matrix* m, const uint32_t** evals);
+
+/* ---- commitments: t = A * s, replacing mul_matrix_vector_runtime /
+ *      CommitKey::inner_commit_slice (commit/src/linear.rs:459-473,
+ *      labrador/src/crs.rs:211-216) ---------------------------------------- */
+
+/* s: batch x cols coefficient polys; t: batch x rows coefficient polys. */
+int grid_gpu_commit_workspace(const grid_gpu_matrix* A, size_t batch, size_t* bytes);
+int grid_gpu_commit_dev(const grid_gpu_matrix* A, const uint32_t* s, size_t batch, uint32_t* t,
+                        void* workspace, size_t workspace_bytes, void* stream);
+int grid_gpu_commit(grid_gpu_matrix* A, const uint32_t* s, size_t batch, uint32_t* t);
+/* t = A_msg * m + A_open * r per batch entry: recompute_linear_commitment_parts_trusted
+ * (commit/src/linear.rs:476-506). Ajtai with a zero opening is grid_gpu_commit. */
+int grid_gpu_linear_commit(grid_gpu_matrix* A_msg, grid_gpu_matrix* A_open, const uint32_t* m,
+                           const uint32_t* r, size_t batch, uint32_t* t);
+
+/* ---- Gram matrix: compute_garbage_g (labrador/src/main_protocol/garbage.rs:76-93)
+ *      G[idx(i,j)] = <s_i, s_j> for i <= j, row-major upper triangle
+ *      (garbage_index, main_protocol/mod.rs:664-670). S: r x n polys. ------- */
+
+int grid_gpu_gram_workspace(const grid_gpu_plan* plan, size_t r, size_t n, size_t* bytes);
+int grid_gpu_gram_dev(const grid_gpu_plan* plan, const uint32_t* S, size_t r, size_t n,
+                      uint32_t* G, void* workspace, size_t workspace_bytes, void* stream);
+int grid_gpu_gram(grid_gpu_plan* plan, const uint32_t* S, size_t r, size_t n, uint32_t* G);
+
+/* ---- JL projection: JLMatrix::project_and_extract_jl_rows (labrador/src/jl.rs:267-303)
+ *      seed: 32 bytes; parts: num_parts x cols words; rows <= 256; p_out: rows words;
+ *      flat_out (optional, NULL to skip): rows*num_parts*cols int8 in the
+ *      reference's [row][part][coeff][poly] order, cols = n*d. ---------------- */
+
+int grid_gpu_jl_workspace(size_t rows, size_t* bytes);
+int grid_gpu_jl_project_dev(const grid_gpu_plan* plan, const uint8_t* seed, size_t rows,
+                            const uint32_t* parts, size_t num_parts, size_t cols, size_t d,
+                            uint32_t* p_out, int8_t* flat_out, void* workspace,
+                            size_t workspace_bytes, void* stream);
+int grid_gpu_jl_project(grid_gpu_plan* plan, const uint8_t* seed, size_t rows,
+                        const uint32_t* parts, size_t num_parts, size_t cols, size_t d,
+                        uint32_t* p_out, int8_t* flat_out);
+
+/* ---- decompositions ------------------------------------------------------ */
+
+/* decompose_polys (labrador/src/main_protocol/mod.rs:731-747): out is
+ * npolys x num_limbs x d, limbs centered in [-base/2, base/2] stored mod q. */
+int grid_gpu_decompose_balanced_dev(const grid_gpu_plan* plan, const uint32_t* polys,
+                                    size_t npolys, uint64_t base, size_t num_limbs,
+                                    uint32_t* out, void* stream);
+int grid_gpu_decompose_balanced(grid_gpu_plan* plan, const uint32_t* polys, size_t npolys,
+                                uint64_t base, size_t num_limbs, uint32_t* out);
+/* Number of unsigned base-`base` digits of q - 1 (decomposition.rs:9-22). */
+int grid_gpu_gadget_digits(uint64_t q, uint64_t base, size_t* digits);
+/* gadget_decompose (algebra/src/poly/decomposition.rs:47-61): digit_major = 1
+ * gives out[digit][len]; 0 gives GadgetRing::decompose_element order
+ * out[poly][digit][coeff] (commit/src/gadget/mod.rs:151-162, len % d == 0). */
+int grid_gpu_gadget_decompose_dev(const grid_gpu_plan* plan, const uint32_t* x, size_t len,
+                                  uint64_t base, int digit_major, uint32_t* out, void* stream);
+int grid_gpu_gadget_decompose(grid_gpu_plan* plan, const uint32_t* x, size_t len, uint64_t base,
+                              int digit_major, uint32_t* out);
+
+/* ---- fused LaBRADOR prover round: the hot calls of prove_step
+ *      (labrador/src/main_protocol/step_prover.rs:118-170) on one witness ----
+ * A: kappa x n (CommitKey::a), S: r x n coefficient polys. Outputs:
+ *   t_limbs  r*kappa*t1 polys  inner_commit_decomposed (crs.rs:225-256)
+ *   g        r(r+1)/2 polys    compute_garbage_g
+ *   g_limbs  r(r+1)/2*t2 polys decompose_polys(g, b2, t2)       (NULL: skip)
+ *   p_out    jl_rows words     JL projection with jl_seed        (NULL: skip)
+ *   jl_flat  jl_rows*r*n*d i8  extracted JL entries              (NULL: skip)
+ * The witness is moved to the evaluation domain once and shared by the
+ * commitment and the Gram matrix. */
+int grid_gpu_prover_round_workspace(const grid_gpu_matrix* A, size_t r, size_t jl_rows,
+                                    size_t* bytes);
+int grid_gpu_prover_round_dev(const grid_gpu_matrix* A, const uint32_t* S, size_t r,
+                              uint64_t b1, size_t t1, uint64_t b2, size_t t2,
+                              const uint8_t* jl_seed, size_t jl_rows, uint32_t* t_limbs,
+                              uint32_t* g, uint32_t* g_limbs, uint32_t* p_out, int8_t* jl_flat,
+                              void* workspace, size_t workspace_bytes, void* stream);
+
 /* ---- host memory ------------------------------------------------------ */
 
 /* Page-lock a caller buffer so host-buffer calls can DMA it asynchronously. */

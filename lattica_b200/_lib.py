@@ -50,6 +50,36 @@ SIGNATURES = {
     "grid_gpu_ntt_inverse": (C.c_int, [_vp, _vp, C.c_size_t]),
     "grid_gpu_ntt_mul_inverse": (C.c_int, [_vp, _vp, _vp, _vp, C.c_size_t]),
     "grid_gpu_poly_mul": (C.c_int, [_vp, _vp, _vp, _vp, C.c_size_t]),
+    "grid_gpu_matrix_create": (C.c_int, [_vp, _vp, C.c_size_t, C.c_size_t, C.c_int, C.POINTER(_vp)]),
+    "grid_gpu_matrix_create_dev": (C.c_int, [_vp, _vp, C.c_size_t, C.c_size_t, C.c_int,
+                                             C.POINTER(_vp), _vp]),
+    "grid_gpu_matrix_destroy": (C.c_int, [_vp]),
+    "grid_gpu_matrix_shape": (C.c_int, [_vp, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
+    "grid_gpu_matrix_device_evals": (C.c_int, [_vp, C.POINTER(_vp)]),
+    "grid_gpu_commit_workspace": (C.c_int, [_vp, C.c_size_t, C.POINTER(C.c_size_t)]),
+    "grid_gpu_commit_dev": (C.c_int, [_vp, _vp, C.c_size_t, _vp, _vp, C.c_size_t, _vp]),
+    "grid_gpu_commit": (C.c_int, [_vp, _vp, C.c_size_t, _vp]),
+    "grid_gpu_linear_commit": (C.c_int, [_vp, _vp, _vp, _vp, C.c_size_t, _vp]),
+    "grid_gpu_gram_workspace": (C.c_int, [_vp, C.c_size_t, C.c_size_t, C.POINTER(C.c_size_t)]),
+    "grid_gpu_gram_dev": (C.c_int, [_vp, _vp, C.c_size_t, C.c_size_t, _vp, _vp, C.c_size_t, _vp]),
+    "grid_gpu_gram": (C.c_int, [_vp, _vp, C.c_size_t, C.c_size_t, _vp]),
+    "grid_gpu_jl_workspace": (C.c_int, [C.c_size_t, C.POINTER(C.c_size_t)]),
+    "grid_gpu_jl_project_dev": (C.c_int, [_vp, _vp, C.c_size_t, _vp, C.c_size_t, C.c_size_t,
+                                          C.c_size_t, _vp, _vp, _vp, C.c_size_t, _vp]),
+    "grid_gpu_jl_project": (C.c_int, [_vp, _vp, C.c_size_t, _vp, C.c_size_t, C.c_size_t,
+                                      C.c_size_t, _vp, _vp]),
+    "grid_gpu_decompose_balanced_dev": (C.c_int, [_vp, _vp, C.c_size_t, C.c_uint64, C.c_size_t,
+                                                  _vp, _vp]),
+    "grid_gpu_decompose_balanced": (C.c_int, [_vp, _vp, C.c_size_t, C.c_uint64, C.c_size_t, _vp]),
+    "grid_gpu_gadget_digits": (C.c_int, [C.c_uint64, C.c_uint64, C.POINTER(C.c_size_t)]),
+    "grid_gpu_gadget_decompose_dev": (C.c_int, [_vp, _vp, C.c_size_t, C.c_uint64, C.c_int, _vp,
+                                                _vp]),
+    "grid_gpu_gadget_decompose": (C.c_int, [_vp, _vp, C.c_size_t, C.c_uint64, C.c_int, _vp]),
+    "grid_gpu_prover_round_workspace": (C.c_int, [_vp, C.c_size_t, C.c_size_t,
+                                                  C.POINTER(C.c_size_t)]),
+    "grid_gpu_prover_round_dev": (C.c_int, [_vp, _vp, C.c_size_t, C.c_uint64, C.c_size_t,
+                                            C.c_uint64, C.c_size_t, _vp, C.c_size_t, _vp, _vp,
+                                            _vp, _vp, _vp, _vp, C.c_size_t, _vp]),
     "grid_gpu_host_register": (C.c_int, [_vp, C.c_size_t]),
     "grid_gpu_host_unregister": (C.c_int, [_vp]),
 }

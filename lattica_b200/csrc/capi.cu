@@ -1,0 +1,446 @@
+// C ABI for prepared matrices, commitments, the Gram matrix, the JL
+// projection, decompositions and the fused LaBRADOR prover round.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <new>
+
+#include "grid_internal.h"
+
+using namespace grid;
+
+namespace {
+
+bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+
+size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+// Bump allocator over a caller workspace (256-byte aligned sub-buffers).
+struct Carver {
+  char* base;
+  size_t cap, used = 0;
+  bool ok = true;
+  Carver(void* b, size_t c) : base(static_cast<char*>(b)), cap(c) {}
+  template <typename T>
+  T* take(size_t count) {
+    const size_t bytes = round_up(count * sizeof(T), 256);
+    if (used + bytes > cap || !base) {
+      ok = false;
+      used += bytes;
+      return nullptr;
+    }
+    T* p = reinterpret_cast<T*>(base + used);
+    used += bytes;
+    return p;
+  }
+};
+
+size_t words_bytes(size_t words) { return round_up(words * 4, 256); }
+
+size_t commit_ws_bytes(const grid_gpu_plan* p, size_t rows, size_t cols, size_t batch) {
+  return words_bytes(batch * cols * p->d) +
+         words_bytes(emm_workspace_words(p, (int)batch, (int)rows, (int)cols, EMM_DENSE));
+}
+
+size_t gram_ws_bytes(const grid_gpu_plan* p, size_t r, size_t n) {
+  return words_bytes(r * n * p->d) + words_bytes(emm_workspace_words(p, (int)r, (int)r, (int)n,
+                                                                       EMM_UPPER));
+}
+
+bool dims_ok(size_t a, size_t b, size_t c) {
+  // all kernels index rows/cols/K with int
+  return a > 0 && b > 0 && c > 0 && a < (1u << 30) && b < (1u << 30) && c < (1u << 30);
+}
+
+// t = A * s for `batch` vectors, into t (coefficients). ws from a Carver.
+int commit_core(const grid_gpu_matrix* A, const uint32_t* s, size_t batch, uint32_t* t,
+                Carver& cv, cudaStream_t st) {
+  const grid_gpu_plan* p = A->plan;
+  uint32_t* s_hat = cv.take<uint32_t>(batch * A->cols * p->d);
+  const size_t ew = emm_workspace_words(p, (int)batch, (int)A->rows, (int)A->cols, EMM_DENSE);
+  uint32_t* work = ew ? cv.take<uint32_t>(ew) : nullptr;
+  if (!cv.ok) return GRID_ERR_INVALID_PARAMETERS;
+  int rc = launch_ntt(p, MODE_FWD, s, nullptr, s_hat, batch * A->cols, st);
+  if (rc) return rc;
+  rc = launch_emm(p, s_hat, A->d_evals, (int)batch, (int)A->rows, (int)A->cols, EMM_DENSE, t,
+                  work, st);
+  if (rc) return rc;
+  return launch_ntt(p, MODE_INV, t, nullptr, t, batch * A->rows, st);
+}
+
+}  // namespace
+
+extern "C" {
+
+/* ---- prepared matrices ------------------------------------------------- */
+
+int grid_gpu_matrix_create_dev(grid_gpu_plan* p, const uint32_t* A, size_t rows, size_t cols,
+                               int a_is_evals, grid_gpu_matrix** out, void* stream) {
+  if (!p || !out || !A) return GRID_ERR_NULL_POINTER;
+  *out = nullptr;
+  if (!dims_ok(rows, cols, 1)) return GRID_ERR_INVALID_PARAMETERS;
+  if (!aligned16(A)) return GRID_ERR_MISALIGNED;
+  grid_gpu_matrix* m = new (std::nothrow) grid_gpu_matrix();
+  if (!m) return GRID_ERR_OUT_OF_MEMORY;
+  m->plan = p;
+  m->rows = rows;
+  m->cols = cols;
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e = cudaMalloc(&m->d_evals, rows * cols * p->d * 4);
+  if (e != cudaSuccess) {
+    delete m;
+    return cuda_status(e);
+  }
+  int rc;
+  if (a_is_evals) {
+    rc = cuda_status(cudaMemcpyAsync(m->d_evals, A, rows * cols * p->d * 4,
+                                     cudaMemcpyDeviceToDevice, st));
+  } else {
+    rc = launch_ntt(p, MODE_FWD, A, nullptr, m->d_evals, rows * cols, st);
+  }
+  if (rc) {
+    cudaFree(m->d_evals);
+    delete m;
+    return rc;
+  }
+  *out = m;
+  return GRID_OK;
+}
+
+int grid_gpu_matrix_create(grid_gpu_plan* p, const uint32_t* A, size_t rows, size_t cols,
+                           int a_is_evals, grid_gpu_matrix** out) {
+  if (!p || !out || !A) return GRID_ERR_NULL_POINTER;
+  *out = nullptr;
+  if (!dims_ok(rows, cols, 1)) return GRID_ERR_INVALID_PARAMETERS;
+  std::lock_guard<std::mutex> lk(p->mu);
+  const size_t bytes = rows * cols * p->d * 4;
+  int rc = ensure_scratch(p, 6, bytes);
+  if (rc) return rc;
+  rc = cuda_status(cudaMemcpyAsync(p->scratch[6].ptr, A, bytes, cudaMemcpyHostToDevice, p->stream));
+  if (rc) return rc;
+  rc = grid_gpu_matrix_create_dev(p, static_cast<uint32_t*>(p->scratch[6].ptr), rows, cols,
+                                  a_is_evals, out, p->stream);
+  const int fin = finish_host_call(p, p->stream);
+  if (rc) return rc;
+  if (fin && *out) {
+    grid_gpu_matrix_destroy(*out);
+    *out = nullptr;
+  }
+  return fin;
+}
+
+int grid_gpu_matrix_destroy(grid_gpu_matrix* m) {
+  if (!m) return GRID_ERR_NULL_POINTER;
+  if (m->d_evals) cudaFree(m->d_evals);
+  delete m;
+  return GRID_OK;
+}
+
+int grid_gpu_matrix_shape(const grid_gpu_matrix* m, size_t* rows, size_t* cols) {
+  if (!m || !rows || !cols) return GRID_ERR_NULL_POINTER;
+  *rows = m->rows;
+  *cols = m->cols;
+  return GRID_OK;
+}
+
+int grid_gpu_matrix_device_evals(const grid_gpu_matrix* m, const uint32_t** evals) {
+  if (!m || !evals) return GRID_ERR_NULL_POINTER;
+  *evals = m->d_evals;
+  return GRID_OK;
+}
+
+/* ---- commitments ------------------------------------------------------- */
+
+int grid_gpu_commit_workspace(const grid_gpu_matrix* A, size_t batch, size_t* bytes) {
+  if (!A || !bytes) return GRID_ERR_NULL_POINTER;
+  *bytes = commit_ws_bytes(A->plan, A->rows, A->cols, batch);
+  return GRID_OK;
+}
+
+int grid_gpu_commit_dev(const grid_gpu_matrix* A, const uint32_t* s, size_t batch, uint32_t* t,
+                        void* workspace, size_t workspace_bytes, void* stream) {
+  if (!A || ((!s || !t) && batch)) return GRID_ERR_NULL_POINTER;
+  if (batch == 0) return GRID_OK;
+  if (!dims_ok(batch, A->rows, A->cols)) return GRID_ERR_INVALID_PARAMETERS;
+  if (!aligned16(s) || !aligned16(t) || !aligned16(workspace)) return GRID_ERR_MISALIGNED;
+  Carver cv(workspace, workspace_bytes);
+  return commit_core(A, s, batch, t, cv, (cudaStream_t)stream);
+}
+
+int grid_gpu_commit(grid_gpu_matrix* A, const uint32_t* s, size_t batch, uint32_t* t) {
+  if (!A || ((!s || !t) && batch)) return GRID_ERR_NULL_POINTER;
+  if (batch == 0) return GRID_OK;
+  if (!dims_ok(batch, A->rows, A->cols)) return GRID_ERR_INVALID_PARAMETERS;
+  grid_gpu_plan* p = A->plan;
+  std::lock_guard<std::mutex> lk(p->mu);
+  const size_t s_bytes = batch * A->cols * p->d * 4, t_bytes = batch * A->rows * p->d * 4;
+  const size_t ws = commit_ws_bytes(p, A->rows, A->cols, batch);
+  int rc;
+  if ((rc = ensure_scratch(p, 6, s_bytes)) || (rc = ensure_scratch(p, 7, t_bytes)) ||
+      (rc = ensure_scratch(p, 8, ws)))
+    return rc;
+  cudaStream_t st = p->stream;
+  rc = cuda_status(cudaMemcpyAsync(p->scratch[6].ptr, s, s_bytes, cudaMemcpyHostToDevice, st));
+  if (!rc) {
+    Carver cv(p->scratch[8].ptr, ws);
+    rc = commit_core(A, static_cast<uint32_t*>(p->scratch[6].ptr), batch,
+                     static_cast<uint32_t*>(p->scratch[7].ptr), cv, st);
+  }
+  if (!rc)
+    rc = cuda_status(cudaMemcpyAsync(t, p->scratch[7].ptr, t_bytes, cudaMemcpyDeviceToHost, st));
+  const int fin = finish_host_call(p, st);
+  return rc ? rc : fin;
+}
+
+int grid_gpu_linear_commit(grid_gpu_matrix* A_msg, grid_gpu_matrix* A_open, const uint32_t* m,
+                           const uint32_t* r, size_t batch, uint32_t* t) {
+  if (!A_msg || !A_open || ((!m || !r || !t) && batch)) return GRID_ERR_NULL_POINTER;
+  if (A_msg->plan != A_open->plan) return GRID_ERR_INVALID_PARAMETERS;
+  if (A_msg->rows != A_open->rows) return GRID_ERR_DIMENSION_MISMATCH;
+  if (batch == 0) return GRID_OK;
+  grid_gpu_plan* p = A_msg->plan;
+  std::lock_guard<std::mutex> lk(p->mu);
+  const size_t rows = A_msg->rows, d = p->d;
+  const size_t m_bytes = batch * A_msg->cols * d * 4, r_bytes = batch * A_open->cols * d * 4;
+  const size_t t_bytes = batch * rows * d * 4;
+  const size_t ws = commit_ws_bytes(p, rows, A_msg->cols, batch) +
+                    commit_ws_bytes(p, rows, A_open->cols, batch);
+  int rc;
+  if ((rc = ensure_scratch(p, 6, m_bytes)) || (rc = ensure_scratch(p, 7, r_bytes)) ||
+      (rc = ensure_scratch(p, 9, t_bytes)) || (rc = ensure_scratch(p, 10, t_bytes)) ||
+      (rc = ensure_scratch(p, 8, ws)))
+    return rc;
+  cudaStream_t st = p->stream;
+  uint32_t* dm = static_cast<uint32_t*>(p->scratch[6].ptr);
+  uint32_t* dr = static_cast<uint32_t*>(p->scratch[7].ptr);
+  uint32_t* t1 = static_cast<uint32_t*>(p->scratch[9].ptr);
+  uint32_t* t2 = static_cast<uint32_t*>(p->scratch[10].ptr);
+  rc = cuda_status(cudaMemcpyAsync(dm, m, m_bytes, cudaMemcpyHostToDevice, st));
+  if (!rc) rc = cuda_status(cudaMemcpyAsync(dr, r, r_bytes, cudaMemcpyHostToDevice, st));
+  if (!rc) {
+    Carver cv(p->scratch[8].ptr, ws);
+    rc = commit_core(A_msg, dm, batch, t1, cv, st);
+    if (!rc) rc = commit_core(A_open, dr, batch, t2, cv, st);
+  }
+  // A_msg*m + A_open*r: INTT is linear, so adding the coefficient forms is exact.
+  if (!rc) rc = launch_add(p, t1, t2, batch * rows * d, st);
+  if (!rc) rc = cuda_status(cudaMemcpyAsync(t, t1, t_bytes, cudaMemcpyDeviceToHost, st));
+  const int fin = finish_host_call(p, st);
+  return rc ? rc : fin;
+}
+
+/* ---- Gram matrix (garbage g) ------------------------------------------- */
+
+int grid_gpu_gram_workspace(const grid_gpu_plan* p, size_t r, size_t n, size_t* bytes) {
+  if (!p || !bytes) return GRID_ERR_NULL_POINTER;
+  *bytes = gram_ws_bytes(p, r, n);
+  return GRID_OK;
+}
+
+int grid_gpu_gram_dev(const grid_gpu_plan* p, const uint32_t* S, size_t r, size_t n,
+                      uint32_t* G, void* workspace, size_t workspace_bytes, void* stream) {
+  if (!p || !S || !G) return GRID_ERR_NULL_POINTER;
+  if (!dims_ok(r, n, 1)) return GRID_ERR_INVALID_PARAMETERS;
+  if (!aligned16(S) || !aligned16(G) || !aligned16(workspace)) return GRID_ERR_MISALIGNED;
+  cudaStream_t st = (cudaStream_t)stream;
+  Carver cv(workspace, workspace_bytes);
+  uint32_t* s_hat = cv.take<uint32_t>(r * n * p->d);
+  const size_t ew = emm_workspace_words(p, (int)r, (int)r, (int)n, EMM_UPPER);
+  uint32_t* work = ew ? cv.take<uint32_t>(ew) : nullptr;
+  if (!cv.ok) return GRID_ERR_INVALID_PARAMETERS;
+  int rc = launch_ntt(p, MODE_FWD, S, nullptr, s_hat, r * n, st);
+  if (rc) return rc;
+  rc = launch_emm(p, s_hat, s_hat, (int)r, (int)r, (int)n, EMM_UPPER, G, work, st);
+  if (rc) return rc;
+  return launch_ntt(p, MODE_INV, G, nullptr, G, r * (r + 1) / 2, st);
+}
+
+int grid_gpu_gram(grid_gpu_plan* p, const uint32_t* S, size_t r, size_t n, uint32_t* G) {
+  if (!p || !S || !G) return GRID_ERR_NULL_POINTER;
+  if (!dims_ok(r, n, 1)) return GRID_ERR_INVALID_PARAMETERS;
+  std::lock_guard<std::mutex> lk(p->mu);
+  const size_t s_bytes = r * n * p->d * 4, g_bytes = r * (r + 1) / 2 * p->d * 4;
+  const size_t ws = gram_ws_bytes(p, r, n);
+  int rc;
+  if ((rc = ensure_scratch(p, 6, s_bytes)) || (rc = ensure_scratch(p, 7, g_bytes)) ||
+      (rc = ensure_scratch(p, 8, ws)))
+    return rc;
+  cudaStream_t st = p->stream;
+  rc = cuda_status(cudaMemcpyAsync(p->scratch[6].ptr, S, s_bytes, cudaMemcpyHostToDevice, st));
+  if (!rc)
+    rc = grid_gpu_gram_dev(p, static_cast<uint32_t*>(p->scratch[6].ptr), r, n,
+                           static_cast<uint32_t*>(p->scratch[7].ptr), p->scratch[8].ptr, ws, st);
+  if (!rc)
+    rc = cuda_status(cudaMemcpyAsync(G, p->scratch[7].ptr, g_bytes, cudaMemcpyDeviceToHost, st));
+  const int fin = finish_host_call(p, st);
+  return rc ? rc : fin;
+}
+
+/* ---- JL projection ------------------------------------------------------ */
+
+int grid_gpu_jl_workspace(size_t rows, size_t* bytes) {
+  if (!bytes) return GRID_ERR_NULL_POINTER;
+  *bytes = round_up(jl_scratch_bytes(rows, 0, 0), 256);
+  return GRID_OK;
+}
+
+int grid_gpu_jl_project_dev(const grid_gpu_plan* p, const uint8_t* seed, size_t rows,
+                            const uint32_t* parts, size_t num_parts, size_t cols, size_t d,
+                            uint32_t* p_out, int8_t* flat_out, void* workspace,
+                            size_t workspace_bytes, void* stream) {
+  if (!p || !seed || !p_out || (!parts && cols && num_parts)) return GRID_ERR_NULL_POINTER;
+  if (!aligned16(workspace)) return GRID_ERR_MISALIGNED;
+  return launch_jl_project(p->f, seed, rows, parts, num_parts, cols, d, p_out, flat_out,
+                           workspace, workspace_bytes, p->num_sms, p->d_err, (cudaStream_t)stream);
+}
+
+int grid_gpu_jl_project(grid_gpu_plan* p, const uint8_t* seed, size_t rows,
+                        const uint32_t* parts, size_t num_parts, size_t cols, size_t d,
+                        uint32_t* p_out, int8_t* flat_out) {
+  if (!p || !seed || !p_out || (!parts && cols && num_parts)) return GRID_ERR_NULL_POINTER;
+  if (rows == 0 || rows > 256 || d == 0 || cols % d) return GRID_ERR_INVALID_PARAMETERS;
+  std::lock_guard<std::mutex> lk(p->mu);
+  const size_t in_bytes = num_parts * cols * 4, flat_bytes = flat_out ? rows * num_parts * cols : 0;
+  const size_t ws = round_up(jl_scratch_bytes(rows, 0, 0), 256);
+  int rc;
+  if ((rc = ensure_scratch(p, 6, in_bytes ? in_bytes : 16)) ||
+      (rc = ensure_scratch(p, 7, rows * 4)) || (rc = ensure_scratch(p, 8, ws)) ||
+      (flat_bytes && (rc = ensure_scratch(p, 11, flat_bytes))))
+    return rc;
+  cudaStream_t st = p->stream;
+  if (in_bytes)
+    rc = cuda_status(cudaMemcpyAsync(p->scratch[6].ptr, parts, in_bytes, cudaMemcpyHostToDevice, st));
+  if (!rc)
+    rc = launch_jl_project(p->f, seed, rows, static_cast<uint32_t*>(p->scratch[6].ptr), num_parts,
+                           cols, d, static_cast<uint32_t*>(p->scratch[7].ptr),
+                           flat_bytes ? static_cast<int8_t*>(p->scratch[11].ptr) : nullptr,
+                           p->scratch[8].ptr, ws, p->num_sms, p->d_err, st);
+  if (!rc)
+    rc = cuda_status(cudaMemcpyAsync(p_out, p->scratch[7].ptr, rows * 4, cudaMemcpyDeviceToHost, st));
+  if (!rc && flat_bytes)
+    rc = cuda_status(cudaMemcpyAsync(flat_out, p->scratch[11].ptr, flat_bytes,
+                                     cudaMemcpyDeviceToHost, st));
+  const int fin = finish_host_call(p, st);
+  return rc ? rc : fin;
+}
+
+/* ---- decompositions ---------------------------------------------------- */
+
+int grid_gpu_decompose_balanced_dev(const grid_gpu_plan* p, const uint32_t* polys, size_t npolys,
+                                    uint64_t base, size_t num_limbs, uint32_t* out, void* stream) {
+  if (!p || ((!polys || !out) && npolys)) return GRID_ERR_NULL_POINTER;
+  return launch_decompose_balanced(p, polys, npolys, base, num_limbs, out, (cudaStream_t)stream);
+}
+
+int grid_gpu_decompose_balanced(grid_gpu_plan* p, const uint32_t* polys, size_t npolys,
+                                uint64_t base, size_t num_limbs, uint32_t* out) {
+  if (!p || ((!polys || !out) && npolys)) return GRID_ERR_NULL_POINTER;
+  if (base < 2 || num_limbs == 0 || num_limbs > 64) return GRID_ERR_INVALID_PARAMETERS;
+  if (npolys == 0) return GRID_OK;
+  std::lock_guard<std::mutex> lk(p->mu);
+  const size_t in_bytes = npolys * p->d * 4, out_bytes = in_bytes * num_limbs;
+  int rc;
+  if ((rc = ensure_scratch(p, 6, in_bytes)) || (rc = ensure_scratch(p, 7, out_bytes))) return rc;
+  cudaStream_t st = p->stream;
+  rc = cuda_status(cudaMemcpyAsync(p->scratch[6].ptr, polys, in_bytes, cudaMemcpyHostToDevice, st));
+  if (!rc)
+    rc = launch_decompose_balanced(p, static_cast<uint32_t*>(p->scratch[6].ptr), npolys, base,
+                                   num_limbs, static_cast<uint32_t*>(p->scratch[7].ptr), st);
+  if (!rc)
+    rc = cuda_status(cudaMemcpyAsync(out, p->scratch[7].ptr, out_bytes, cudaMemcpyDeviceToHost, st));
+  const int fin = finish_host_call(p, st);
+  return rc ? rc : fin;
+}
+
+int grid_gpu_gadget_digits(uint64_t q, uint64_t base, size_t* digits) {
+  if (!digits) return GRID_ERR_NULL_POINTER;
+  if (base < 2 || q < 3) return GRID_ERR_INVALID_PARAMETERS;
+  *digits = gadget_digit_count(q, base);
+  return GRID_OK;
+}
+
+int grid_gpu_gadget_decompose_dev(const grid_gpu_plan* p, const uint32_t* x, size_t len,
+                                  uint64_t base, int digit_major, uint32_t* out, void* stream) {
+  if (!p || ((!x || !out) && len)) return GRID_ERR_NULL_POINTER;
+  if (base < 2) return GRID_ERR_INVALID_PARAMETERS;
+  if (!digit_major && len % p->d) return GRID_ERR_LENGTH_MISMATCH;
+  return launch_gadget_decompose(p, x, len, base, gadget_digit_count(p->q, base), digit_major,
+                                 out, (cudaStream_t)stream);
+}
+
+int grid_gpu_gadget_decompose(grid_gpu_plan* p, const uint32_t* x, size_t len, uint64_t base,
+                              int digit_major, uint32_t* out) {
+  if (!p || ((!x || !out) && len)) return GRID_ERR_NULL_POINTER;
+  if (base < 2) return GRID_ERR_INVALID_PARAMETERS;
+  if (!digit_major && len % p->d) return GRID_ERR_LENGTH_MISMATCH;
+  if (len == 0) return GRID_OK;
+  std::lock_guard<std::mutex> lk(p->mu);
+  const size_t k = gadget_digit_count(p->q, base);
+  const size_t in_bytes = len * 4, out_bytes = in_bytes * k;
+  int rc;
+  if ((rc = ensure_scratch(p, 6, in_bytes)) || (rc = ensure_scratch(p, 7, out_bytes))) return rc;
+  cudaStream_t st = p->stream;
+  rc = cuda_status(cudaMemcpyAsync(p->scratch[6].ptr, x, in_bytes, cudaMemcpyHostToDevice, st));
+  if (!rc)
+    rc = launch_gadget_decompose(p, static_cast<uint32_t*>(p->scratch[6].ptr), len, base, k,
+                                 digit_major, static_cast<uint32_t*>(p->scratch[7].ptr), st);
+  if (!rc)
+    rc = cuda_status(cudaMemcpyAsync(out, p->scratch[7].ptr, out_bytes, cudaMemcpyDeviceToHost, st));
+  const int fin = finish_host_call(p, st);
+  return rc ? rc : fin;
+}
+
+/* ---- fused LaBRADOR prover round ---------------------------------------- */
+
+int grid_gpu_prover_round_workspace(const grid_gpu_matrix* A, size_t r, size_t jl_rows,
+                                    size_t* bytes) {
+  if (!A || !bytes) return GRID_ERR_NULL_POINTER;
+  const grid_gpu_plan* p = A->plan;
+  const size_t n = A->cols, kappa = A->rows, d = p->d;
+  const size_t emm = emm_workspace_words(p, (int)r, (int)kappa, (int)n, EMM_DENSE) >
+                             emm_workspace_words(p, (int)r, (int)r, (int)n, EMM_UPPER)
+                         ? emm_workspace_words(p, (int)r, (int)kappa, (int)n, EMM_DENSE)
+                         : emm_workspace_words(p, (int)r, (int)r, (int)n, EMM_UPPER);
+  *bytes = words_bytes(r * n * d) + words_bytes(emm) + words_bytes(r * kappa * d) +
+           round_up(jl_scratch_bytes(jl_rows ? jl_rows : 1, 0, 0), 256);
+  return GRID_OK;
+}
+
+int grid_gpu_prover_round_dev(const grid_gpu_matrix* A, const uint32_t* S, size_t r,
+                              uint64_t b1, size_t t1, uint64_t b2, size_t t2,
+                              const uint8_t* jl_seed, size_t jl_rows, uint32_t* t_limbs,
+                              uint32_t* g, uint32_t* g_limbs, uint32_t* p_out, int8_t* jl_flat,
+                              void* workspace, size_t workspace_bytes, void* stream) {
+  if (!A || !S || !t_limbs || !g) return GRID_ERR_NULL_POINTER;
+  const grid_gpu_plan* p = A->plan;
+  const size_t n = A->cols, kappa = A->rows, d = p->d;
+  if (!dims_ok(r, n, kappa)) return GRID_ERR_INVALID_PARAMETERS;
+  if (!aligned16(S) || !aligned16(g) || !aligned16(workspace)) return GRID_ERR_MISALIGNED;
+  cudaStream_t st = (cudaStream_t)stream;
+  Carver cv(workspace, workspace_bytes);
+  uint32_t* s_hat = cv.take<uint32_t>(r * n * d);
+  const size_t e1 = emm_workspace_words(p, (int)r, (int)kappa, (int)n, EMM_DENSE);
+  const size_t e2 = emm_workspace_words(p, (int)r, (int)r, (int)n, EMM_UPPER);
+  const size_t ew = e1 > e2 ? e1 : e2;
+  uint32_t* work = ew ? cv.take<uint32_t>(ew) : nullptr;
+  uint32_t* t = cv.take<uint32_t>(r * kappa * d);
+  void* jl_ws = cv.take<char>(jl_scratch_bytes(jl_rows ? jl_rows : 1, 0, 0));
+  if (!cv.ok) return GRID_ERR_INVALID_PARAMETERS;
+  // Witness to the evaluation domain once; shared by the commitment and the Gram.
+  int rc = launch_ntt(p, MODE_FWD, S, nullptr, s_hat, r * n, st);
+  // 1. inner commitments t_i = A s_i, then balanced limbs (inner_commit_decomposed)
+  if (!rc) rc = launch_emm(p, s_hat, A->d_evals, (int)r, (int)kappa, (int)n, EMM_DENSE, t, work, st);
+  if (!rc) rc = launch_ntt(p, MODE_INV, t, nullptr, t, r * kappa, st);
+  if (!rc) rc = launch_decompose_balanced(p, t, r * kappa, b1, t1, t_limbs, st);
+  // 2. garbage g_ij = <s_i, s_j>, i <= j, then balanced limbs
+  if (!rc) rc = launch_emm(p, s_hat, s_hat, (int)r, (int)r, (int)n, EMM_UPPER, g, work, st);
+  if (!rc) rc = launch_ntt(p, MODE_INV, g, nullptr, g, r * (r + 1) / 2, st);
+  if (!rc && g_limbs) rc = launch_decompose_balanced(p, g, r * (r + 1) / 2, b2, t2, g_limbs, st);
+  // 3. JL projection of the coefficient vectors (one part per witness vector)
+  if (!rc && jl_seed && p_out)
+    rc = launch_jl_project(p->f, jl_seed, jl_rows, S, r, n * d, d, p_out, jl_flat, jl_ws,
+                           jl_scratch_bytes(jl_rows, 0, 0), p->num_sms, p->d_err, st);
+  return rc;
+}
+
+}  // extern "C"

@@ -51,6 +51,51 @@ __device__ __forceinline__ uint32_t sub_mod(uint32_t a, uint32_t b, uint32_t q) 
   return a < b ? r + q : r;
 }
 
+// ---------------------------------------------------------------------------
+// Lazy words: any 32-bit word congruent to the value mod q. r1 = 2^32 mod q.
+//
+// Carries and borrows are taken from unsigned compares. (Taking the borrow
+// from the high word of a 64-bit difference, or from a sub.cc / subc pair,
+// was measured on sm_100a to report a borrow for 0 - 0 when fed by __umulhi
+// results inside the unrolled transforms, so those forms are not used.)
+// ---------------------------------------------------------------------------
+
+// a - t (mod q) for t < q and any word a; result in [0, 2^32).
+// Borrow: a - t + 2^32 + q wraps to a - t + q, which lies in (0, q).
+__device__ __forceinline__ uint32_t sub_lazy(uint32_t a, uint32_t t, uint32_t q) {
+  const uint32_t r = a - t;
+  return a < t ? r + q : r;
+}
+
+// a + t (mod q) for t < q and any word a; result in [0, 2^32).
+// Carry: a + t - 2^32 <= q - 2, plus r1 < q stays below 2^32 for every q < 2^32.
+__device__ __forceinline__ uint32_t add_lazy(uint32_t a, uint32_t t, uint32_t r1) {
+  const uint32_t s = a + t;
+  return s < t ? s + r1 : s;
+}
+
+// (a + b) mod q, canonical, for canonical a, b: a - (q - b), + q on borrow.
+__device__ __forceinline__ uint32_t add_canon(uint32_t a, uint32_t b, uint32_t q) {
+  return sub_lazy(a, q - b, q);
+}
+
+// Montgomery product by a constant w < q (Shoup companion wq): canonical for any word a.
+__device__ __forceinline__ uint32_t mont_c(uint32_t a, uint32_t w, uint32_t wq, uint32_t q) {
+  const uint32_t hi = __umulhi(a, w);
+  const uint32_t m = a * wq;
+  const uint32_t u = __umulhi(m, q);
+  return sub_lazy(hi, u, q);
+}
+
+// Montgomery product a*b*2^-32 for any word a and canonical b: canonical.
+__device__ __forceinline__ uint32_t mont_v(uint32_t a, uint32_t b, uint32_t q, uint32_t qinv) {
+  const uint32_t lo = a * b;
+  const uint32_t hi = __umulhi(a, b);
+  const uint32_t m = lo * qinv;
+  const uint32_t u = __umulhi(m, q);
+  return sub_lazy(hi, u, q);
+}
+
 // Any 32-bit word x -> x mod q, by one Montgomery multiply with 2^32 mod q.
 __device__ __forceinline__ uint32_t reduce_word(uint32_t x, const FieldParams& f) {
   return mont_mul(x, f.r1, f.q, f.qinv);
@@ -68,25 +113,19 @@ __device__ __forceinline__ uint32_t to_mont(uint32_t v, const FieldParams& f) {
 
 // 96-bit accumulator for sums of 64-bit products: acc += a*b.
 struct Acc96 {
-  uint32_t w0, w1, w2;
+  uint64_t lo;   // bits 0..63
+  uint32_t w2;   // bits 64..95
 };
 
-__device__ __forceinline__ void acc96_zero(Acc96& a) { a.w0 = a.w1 = a.w2 = 0; }
-
-__device__ __forceinline__ void acc96_mad(Acc96& acc, uint32_t a, uint32_t b) {
-  asm("mad.lo.cc.u32 %0, %3, %4, %0;\n\t"
-      "madc.hi.cc.u32 %1, %3, %4, %1;\n\t"
-      "addc.u32 %2, %2, 0;"
-      : "+r"(acc.w0), "+r"(acc.w1), "+r"(acc.w2)
-      : "r"(a), "r"(b));
+__device__ __forceinline__ void acc96_zero(Acc96& a) {
+  a.lo = 0;
+  a.w2 = 0;
 }
 
-__device__ __forceinline__ void acc96_add(Acc96& acc, const Acc96& o) {
-  asm("add.cc.u32 %0, %0, %3;\n\t"
-      "addc.cc.u32 %1, %1, %4;\n\t"
-      "addc.u32 %2, %2, %5;"
-      : "+r"(acc.w0), "+r"(acc.w1), "+r"(acc.w2)
-      : "r"(o.w0), "r"(o.w1), "r"(o.w2));
+__device__ __forceinline__ void acc96_mad(Acc96& acc, uint32_t a, uint32_t b) {
+  const uint64_t p = (uint64_t)a * b;
+  acc.lo += p;
+  acc.w2 += acc.lo < p ? 1u : 0u;
 }
 
 // Reduce V = w2*2^64 + w1*2^32 + w0 to V * 2^-32 mod q (canonical).
@@ -94,12 +133,13 @@ __device__ __forceinline__ void acc96_add(Acc96& acc, const Acc96& o) {
 // sum(a_k*b_k) * 2^-32 = sum(mont_mul(a_k, b_k)) mod q.
 // Requires w2 < 2^32 (at most 2^32 products of words < 2^32).
 __device__ __forceinline__ uint32_t acc96_reduce(const Acc96& acc, const FieldParams& f) {
+  const uint32_t w0 = (uint32_t)acc.lo, w1 = (uint32_t)(acc.lo >> 32);
   // Low 64 bits: (w1*2^32 + w0) * 2^-32 = w1 - hi(m*q) with m = w0*q^-1.
-  const uint32_t m = acc.w0 * f.qinv;
+  const uint32_t m = w0 * f.qinv;
   const uint32_t u = __umulhi(m, f.q);
-  uint32_t lo_part = acc.w1 - u;           // in (-q, 2^32): fix the negative case
-  if (acc.w1 < u) lo_part += f.q;          // now any word in [0, 2^32)
-  lo_part = reduce_word(lo_part, f);       // canonical
+  uint32_t lo_part = w1 - u;     // in (-q, 2^32): fix the negative case
+  if (w1 < u) lo_part += f.q;    // now any word in [0, 2^32)
+  lo_part = reduce_word(lo_part, f);  // canonical
   // High word: w2 * 2^64 * 2^-32 = w2 * 2^32 = mont_mul(w2, 2^64 mod q).
   const uint32_t hi_part = mont_mul(acc.w2, f.r2, f.q, f.qinv);
   return add_mod(lo_part, hi_part, f.q);

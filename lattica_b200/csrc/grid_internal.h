@@ -79,12 +79,11 @@ int launch_ntt(const grid_gpu_plan* p, int mode, const uint32_t* a, const uint32
                uint32_t* out, size_t npolys, cudaStream_t s);
 int ntt_max_degree();
 
-// commit.cu
-int launch_matvec(const grid_gpu_plan* p, const uint32_t* a_evals, size_t rows, size_t cols,
-                  const uint32_t* s_evals, size_t batch, uint32_t* t_evals, int accumulate,
-                  cudaStream_t s);
-int launch_gram(const grid_gpu_plan* p, const uint32_t* s_evals, size_t r, size_t n,
-                uint32_t* g_evals, cudaStream_t s);
+// commit.cu: out_e[m][n] = sum_k X[m][k][e] * Y[n][k][e] for every evaluation point.
+enum EmmOut : int { EMM_DENSE = 0, EMM_UPPER = 1 };
+size_t emm_workspace_words(const grid_gpu_plan* p, int M, int N, int K, int mode);
+int launch_emm(const grid_gpu_plan* p, const uint32_t* X, const uint32_t* Y, int M, int N, int K,
+               int mode, uint32_t* out_evals, uint32_t* work, cudaStream_t s);
 int launch_pointwise(const grid_gpu_plan* p, uint32_t* dst, const uint32_t* rhs, size_t words,
                      cudaStream_t s);
 int launch_add(const grid_gpu_plan* p, uint32_t* dst, const uint32_t* rhs, size_t words,
@@ -93,8 +92,9 @@ int launch_add(const grid_gpu_plan* p, uint32_t* dst, const uint32_t* rhs, size_
 // decompose.cu
 int launch_decompose_balanced(const grid_gpu_plan* p, const uint32_t* polys, size_t npolys,
                               uint64_t base, size_t num_limbs, uint32_t* out, cudaStream_t s);
-int launch_gadget_decompose(const grid_gpu_plan* p, const uint32_t* x, size_t len,
-                            uint64_t base, size_t digits, uint32_t* out, cudaStream_t s);
+int launch_gadget_decompose(const grid_gpu_plan* p, const uint32_t* x, size_t len, uint64_t base,
+                            size_t digits, int digit_major, uint32_t* out, cudaStream_t s);
+size_t gadget_digit_count(uint64_t q, uint64_t base);
 
 // jl.cu
 int launch_jl_project(const FieldParams& f, const uint8_t seed[32], size_t rows,
@@ -102,6 +102,14 @@ int launch_jl_project(const FieldParams& f, const uint8_t seed[32], size_t rows,
                       uint32_t* p_out, int8_t* flat_out, void* scratch, size_t scratch_bytes,
                       int num_sms, int* d_err, cudaStream_t s);
 size_t jl_scratch_bytes(size_t rows, size_t num_parts, int num_sms);
+
+// plan.cu
+int host_pipeline(grid_gpu_plan* p, const uint32_t* const* ins, int nin, uint32_t* out,
+                  size_t nunits, size_t unit_words,
+                  int (*op)(grid_gpu_plan*, const uint32_t* const*, uint32_t*, size_t,
+                            cudaStream_t, void*),
+                  void* ctx);
+int finish_host_call(grid_gpu_plan* p, cudaStream_t s);
 
 // helpers
 int cuda_status(cudaError_t e);

@@ -1,0 +1,309 @@
+// Johnson-Lindenstrauss projection of the LaBRADOR prover on the GPU.
+//
+// Reference path replaced: JLMatrix::project_and_extract_jl_rows /
+// project_and_extract_seq (labrador/src/jl.rs:267-303, 388-508). Part i of the
+// witness uses the IETF ChaCha20 keystream (RFC 8439; the reference uses the
+// chacha20 0.10 crate) with key = seed, nonce = (u32 i, little endian) || 0^8,
+// block counter from 0. Column `col` consumes packed_len = ceil(rows/4) bytes
+// at keystream offset col*packed_len; row r reads bits 2*(r%4) of byte r/4:
+// 00 -> +1, 01 -> -1, 1x -> 0. p[row] = sum over parts and columns of
+// entry * coeff (mod q), accumulated on Montgomery words (the map to
+// Montgomery form is additive, so this is the reference's field sum).
+//
+// The keystream is regenerated on the fly (the reference materialises the
+// whole [rows][parts][d][n] i8 matrix, 2 GiB at the LaBRADOR round size);
+// the i8 extraction is a separate, optional kernel.
+//
+// Projection kernel: a warp takes 32 consecutive columns of one part; lane l
+// computes the keystream bytes of column c0 + l into shared memory, then owns
+// rows 8l .. 8l+7 and sweeps the 32 columns, adding the coefficient to a
+// 64-bit "plus" or "minus" accumulator per row (exact while one warp sees
+// fewer than 2^32 columns of 32-bit words). Per-lane totals are folded mod q and added to
+// 64-bit global row sums with atomics; a final kernel reduces them mod q.
+#include <cuda_runtime.h>
+
+#include "grid_field.cuh"
+#include "grid_internal.h"
+
+namespace grid {
+namespace {
+
+constexpr int kJlWarps = 8;
+constexpr int kJlThreads = kJlWarps * 32;
+
+struct ChachaKey {
+  uint32_t k[8];
+};
+
+__device__ __forceinline__ uint32_t rotl(uint32_t x, int r) { return __funnelshift_l(x, x, r); }
+
+#define GRID_QR(a, b, c, d)  \
+  a += b; d ^= a; d = rotl(d, 16); \
+  c += d; b ^= c; b = rotl(b, 12); \
+  a += b; d ^= a; d = rotl(d, 8);  \
+  c += d; b ^= c; b = rotl(b, 7);
+
+// RFC 8439 block function: out[16] = keystream words of block `counter`.
+__device__ __forceinline__ void chacha20_block(const ChachaKey& key, uint32_t counter,
+                                               uint32_t nonce0, uint32_t (&out)[16]) {
+  uint32_t x0 = 0x61707865u, x1 = 0x3320646eu, x2 = 0x79622d32u, x3 = 0x6b206574u;
+  uint32_t x4 = key.k[0], x5 = key.k[1], x6 = key.k[2], x7 = key.k[3];
+  uint32_t x8 = key.k[4], x9 = key.k[5], x10 = key.k[6], x11 = key.k[7];
+  uint32_t x12 = counter, x13 = nonce0, x14 = 0, x15 = 0;
+#pragma unroll
+  for (int i = 0; i < 10; ++i) {
+    GRID_QR(x0, x4, x8, x12);
+    GRID_QR(x1, x5, x9, x13);
+    GRID_QR(x2, x6, x10, x14);
+    GRID_QR(x3, x7, x11, x15);
+    GRID_QR(x0, x5, x10, x15);
+    GRID_QR(x1, x6, x11, x12);
+    GRID_QR(x2, x7, x8, x13);
+    GRID_QR(x3, x4, x9, x14);
+  }
+  out[0] = x0 + 0x61707865u; out[1] = x1 + 0x3320646eu;
+  out[2] = x2 + 0x79622d32u; out[3] = x3 + 0x6b206574u;
+  out[4] = x4 + key.k[0]; out[5] = x5 + key.k[1]; out[6] = x6 + key.k[2]; out[7] = x7 + key.k[3];
+  out[8] = x8 + key.k[4]; out[9] = x9 + key.k[5]; out[10] = x10 + key.k[6];
+  out[11] = x11 + key.k[7];
+  out[12] = x12 + counter; out[13] = x13 + nonce0; out[14] = x14; out[15] = x15;
+}
+
+// Keystream bytes [off, off + 64) of stream (key, nonce0) as 16 words
+// (unused tail bytes are whatever the next block holds; callers mask rows).
+__device__ __forceinline__ void keystream64(const ChachaKey& key, uint32_t nonce0, uint64_t off,
+                                            uint32_t (&w)[16]) {
+  const uint32_t blk = (uint32_t)(off >> 6);
+  const uint32_t sh = (uint32_t)(off & 63);
+  chacha20_block(key, blk, nonce0, w);
+  if (sh != 0) {
+    uint32_t nx[16];
+    chacha20_block(key, blk + 1, nonce0, nx);
+    // byte-shift the 128-byte window (w ++ nx) left by sh bytes
+    const uint32_t ws = sh >> 2, bs = (sh & 3) * 8;
+    uint32_t r[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      const uint32_t j = i + ws;
+      const uint32_t lo = j < 16 ? w[j] : nx[j - 16];
+      const uint32_t j2 = j + 1;
+      const uint32_t hi = j2 < 16 ? w[j2] : (j2 < 32 ? nx[j2 - 16] : 0u);
+      r[i] = bs ? __funnelshift_r(lo, hi, bs) : lo;
+    }
+#pragma unroll
+    for (int i = 0; i < 16; ++i) w[i] = r[i];
+  }
+}
+
+template <bool kWholeBlocks>
+__global__ void __launch_bounds__(kJlThreads) jl_project_kernel(
+    const uint32_t* __restrict__ parts, unsigned long long cols, int num_parts, int rows,
+    int packed_len, ChachaKey key, unsigned long long* __restrict__ gsum_pos,
+    unsigned long long* __restrict__ gsum_neg, uint32_t q) {
+  __shared__ uint32_t ks[kJlWarps][32][17];
+  __shared__ uint32_t xs[kJlWarps][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned long long chunks_per_part = (cols + 31) / 32;
+  const unsigned long long total = chunks_per_part * (unsigned long long)num_parts;
+  const unsigned long long stride = (unsigned long long)gridDim.x * kJlWarps;
+  unsigned long long pos[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  unsigned long long neg[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  const int word = lane >> 1, shift = (lane & 1) * 16;
+
+  for (unsigned long long ch = (unsigned long long)blockIdx.x * kJlWarps + warp; ch < total;
+       ch += stride) {
+    const uint32_t part = (uint32_t)(ch / chunks_per_part);
+    const unsigned long long c = (ch % chunks_per_part) * 32 + lane;
+    uint32_t w[16];
+    uint32_t x = 0;
+    if (c < cols) {
+      if constexpr (kWholeBlocks)
+        chacha20_block(key, (uint32_t)c, part, w);  // 256 rows: column c is block c
+      else
+        keystream64(key, part, c * (unsigned long long)packed_len, w);
+      x = parts[(unsigned long long)part * cols + c];
+    } else {
+#pragma unroll
+      for (int i = 0; i < 16; ++i) w[i] = 0xFFFFFFFFu;  // code 11 -> 0
+    }
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < 16; ++i) ks[warp][lane][i] = w[i];
+    xs[warp][lane] = x;
+    __syncwarp();
+#pragma unroll 4
+    for (int cc = 0; cc < 32; ++cc) {
+      const uint32_t h = ks[warp][cc][word] >> shift;
+      const uint32_t xc = xs[warp][cc];
+      const uint32_t lo = h & 0x5555u, hi = (h >> 1) & 0x5555u;
+      const uint32_t plus = ~(lo | hi) & 0x5555u;  // code 00
+      const uint32_t minus = lo & ~hi;             // code 01
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        pos[k] += (unsigned long long)(xc & (0u - ((plus >> (2 * k)) & 1u)));
+        neg[k] += (unsigned long long)(xc & (0u - ((minus >> (2 * k)) & 1u)));
+      }
+    }
+  }
+  // Fold to residues and publish. Rows beyond `rows` only saw code 11.
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    const int row = lane * 8 + k;
+    if (row < rows && (pos[k] | neg[k])) {
+      atomicAdd(&gsum_pos[row], pos[k] % q);
+      atomicAdd(&gsum_neg[row], neg[k] % q);
+    }
+  }
+}
+
+__global__ void jl_finish_kernel(const unsigned long long* __restrict__ gsum_pos,
+                                 const unsigned long long* __restrict__ gsum_neg, uint32_t* p_out,
+                                 int rows, uint32_t q) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r < rows) {
+    const uint32_t a = (uint32_t)(gsum_pos[r] % q), b = (uint32_t)(gsum_neg[r] % q);
+    p_out[r] = sub_mod(a, b, q);
+  }
+}
+
+// Entry -> int8 table for one keystream byte: 4 rows, 2 bits each.
+__device__ __forceinline__ uint32_t entries_of_byte(uint32_t byte) {
+  uint32_t out = 0;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const uint32_t c = (byte >> (2 * i)) & 3u;
+    const uint32_t v = c == 0 ? 0x01u : (c == 1 ? 0xFFu : 0x00u);
+    out |= v << (8 * i);
+  }
+  return out;
+}
+
+// flat[row][part][k][j] (int8) for col = j*d + k. A warp handles one (part, k)
+// and 128 consecutive j, 4 per lane, so each row store is a 4-byte word and
+// a warp writes 128 contiguous bytes per row.
+template <bool kWholeBlocks>
+__global__ void __launch_bounds__(kJlThreads) jl_flat_kernel(unsigned long long cols, int d,
+                                                             int num_parts, int rows,
+                                                             int packed_len, ChachaKey key,
+                                                             int8_t* __restrict__ flat) {
+  __shared__ uint32_t lut[256];
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) lut[i] = entries_of_byte(i);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned long long n = cols / d;
+  const unsigned long long jchunks = (n + 127) / 128;
+  const unsigned long long total = (unsigned long long)num_parts * d * jchunks;
+  const unsigned long long plane = (unsigned long long)num_parts * cols;  // bytes per row
+  const unsigned long long stride = (unsigned long long)gridDim.x * kJlWarps;
+  const bool vec_ok = (n % 4) == 0;
+  for (unsigned long long wk = (unsigned long long)blockIdx.x * kJlWarps + warp; wk < total;
+       wk += stride) {
+    const unsigned long long jc = wk % jchunks;
+    const unsigned long long pk = wk / jchunks;  // part * d + k
+    const uint32_t part = (uint32_t)(pk / d);
+    const uint32_t k = (uint32_t)(pk % d);
+    const unsigned long long j0 = jc * 128 + lane * 4;
+    uint32_t w[4][16];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const unsigned long long j = j0 + u;
+      if (j < n) {
+        if constexpr (kWholeBlocks)
+          chacha20_block(key, (uint32_t)(j * d + k), part, w[u]);
+        else
+          keystream64(key, part, (j * d + k) * (unsigned long long)packed_len, w[u]);
+      } else {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) w[u][i] = 0xFFFFFFFFu;
+      }
+    }
+    int8_t* base = flat + pk * n + j0;
+#pragma unroll
+    for (int b = 0; b < 64; ++b) {
+      if (b >= packed_len) break;
+      uint32_t e[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) e[u] = lut[(w[u][b >> 2] >> ((b & 3) * 8)) & 0xFFu];
+      // transpose 4 columns x 4 rows of bytes: out[r] = (e0.r, e1.r, e2.r, e3.r)
+      const uint32_t t01l = __byte_perm(e[0], e[1], 0x5140);
+      const uint32_t t23l = __byte_perm(e[2], e[3], 0x5140);
+      const uint32_t t01h = __byte_perm(e[0], e[1], 0x7362);
+      const uint32_t t23h = __byte_perm(e[2], e[3], 0x7362);
+      uint32_t o[4];
+      o[0] = __byte_perm(t01l, t23l, 0x5410);
+      o[1] = __byte_perm(t01l, t23l, 0x7632);
+      o[2] = __byte_perm(t01h, t23h, 0x5410);
+      o[3] = __byte_perm(t01h, t23h, 0x7632);
+#pragma unroll
+      for (int r4 = 0; r4 < 4; ++r4) {
+        const int row = b * 4 + r4;
+        if (row >= rows) break;
+        int8_t* dst = base + (unsigned long long)row * plane;
+        if (vec_ok && j0 + 3 < n) {
+          *reinterpret_cast<uint32_t*>(dst) = o[r4];
+        } else {
+          for (int u = 0; u < 4; ++u)
+            if (j0 + u < n) dst[u] = (int8_t)((o[r4] >> (8 * u)) & 0xFFu);
+        }
+      }
+    }
+  }
+}
+
+}  // namespace
+
+size_t jl_scratch_bytes(size_t rows, size_t, int) { return 2 * rows * sizeof(unsigned long long); }
+
+int launch_jl_project(const FieldParams& f, const uint8_t seed[32], size_t rows,
+                      const uint32_t* parts, size_t num_parts, size_t cols, size_t d,
+                      uint32_t* p_out, int8_t* flat_out, void* scratch, size_t scratch_bytes,
+                      int num_sms, int*, cudaStream_t s) {
+  if (rows == 0 || rows > 256 || d == 0 || cols % d != 0 || num_parts == 0 ||
+      num_parts > 0xFFFFFFFFull)
+    return GRID_ERR_INVALID_PARAMETERS;
+  if (scratch_bytes < jl_scratch_bytes(rows, num_parts, num_sms)) return GRID_ERR_INVALID_PARAMETERS;
+  ChachaKey key;
+  for (int i = 0; i < 8; ++i)
+    key.k[i] = (uint32_t)seed[4 * i] | ((uint32_t)seed[4 * i + 1] << 8) |
+               ((uint32_t)seed[4 * i + 2] << 16) | ((uint32_t)seed[4 * i + 3] << 24);
+  const int packed_len = (int)((rows + 3) / 4);
+  unsigned long long* gpos = static_cast<unsigned long long*>(scratch);
+  unsigned long long* gneg = gpos + rows;
+  cudaError_t e = cudaMemsetAsync(gpos, 0, 2 * rows * sizeof(unsigned long long), s);
+  if (e != cudaSuccess) return cuda_status(e);
+  if (cols > 0) {
+    const unsigned long long chunks = (cols + 31) / 32 * num_parts;
+    unsigned long long blocks = (chunks + kJlWarps - 1) / kJlWarps;
+    const unsigned long long cap = (unsigned long long)num_sms * 8;
+    if (blocks > cap) blocks = cap;
+    if (packed_len == 64)
+      jl_project_kernel<true><<<(unsigned)blocks, kJlThreads, 0, s>>>(
+          parts, cols, (int)num_parts, (int)rows, packed_len, key, gpos, gneg, f.q);
+    else
+      jl_project_kernel<false><<<(unsigned)blocks, kJlThreads, 0, s>>>(
+          parts, cols, (int)num_parts, (int)rows, packed_len, key, gpos, gneg, f.q);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_status(e);
+  }
+  jl_finish_kernel<<<(unsigned)((rows + 255) / 256), 256, 0, s>>>(gpos, gneg, p_out, (int)rows, f.q);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_status(e);
+  if (flat_out && cols > 0) {
+    const unsigned long long n = cols / d;
+    const unsigned long long work = (unsigned long long)num_parts * d * ((n + 127) / 128);
+    unsigned long long blocks = (work + kJlWarps - 1) / kJlWarps;
+    const unsigned long long cap = (unsigned long long)num_sms * 8;
+    if (blocks > cap) blocks = cap;
+    if (packed_len == 64)
+      jl_flat_kernel<true><<<(unsigned)blocks, kJlThreads, 0, s>>>(
+          cols, (int)d, (int)num_parts, (int)rows, packed_len, key, flat_out);
+    else
+      jl_flat_kernel<false><<<(unsigned)blocks, kJlThreads, 0, s>>>(
+          cols, (int)d, (int)num_parts, (int)rows, packed_len, key, flat_out);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_status(e);
+  }
+  return GRID_OK;
+}
+
+}  // namespace grid

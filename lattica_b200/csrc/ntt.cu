@@ -3,26 +3,31 @@
 // Reference path replaced: TwistedNttPlan::{forward,inverse}_in_place_trusted
 // (algebra/src/poly/ntt.rs:75-104) over the bit-reverse + DIT forward and
 // GS + n^-1 + bit-reverse inverse (algebra/src/arith/ntt.rs:620-681), and the
-// config-style "NTT -> Montgomery pointwise -> INTT" chain.
+// "NTT -> Montgomery pointwise -> INTT" chain of a negacyclic product.
 //
 // Design (sm_100a):
 //  * The twist by psi^i, the bit-reversal and the n^-1 scale are folded into
 //    a merged Cooley-Tukey / Gentleman-Sande pair with twiddles psi^brv(k).
-//    The forward transform leaves evaluation x(psi^(2*brv(j)+1)) in register
-//    j; the reference's natural-order slot k is register brv(k), so output
-//    ordering is pure register renaming at the store.
-//  * One warp streams tiles of 32 (d <= 64) or 32/T (d = 128, 256) polys.
-//    Tiles move HBM <-> shared memory with TMA bulk copies (one 256-byte piece
-//    per lane) into 16-byte-padded slots, so per-thread 128-bit shared loads
-//    are bank-conflict free; mbarriers track arrival, bulk-group waits track
-//    store completion, and the next tile's input is prefetched into the other
-//    buffer while the current tile computes.
-//  * d <= 64: one thread holds a whole polynomial in registers; every twiddle
-//    index is a compile-time constant, so twiddles come from the kernel
-//    parameter block (constant bank operands).
-//  * d = 128 / 256: T = 2 / 4 threads per polynomial, 64 coefficients each;
-//    log2(T) stages cross threads through warp shuffles; twiddles are staged
-//    once per block into shared memory.
+//    The forward transform leaves evaluation x(psi^(2*brv(j)+1)) at position
+//    j; the reference's natural-order slot k is position brv(k), so output
+//    ordering is register renaming at the store.
+//  * The forward transform runs on lazy words (any 32-bit representative,
+//    grid_field.cuh), saving the canonical reduction of every sum; the
+//    inverse runs on canonical words.
+//  * One persistent CTA of kWarps warps per SM. Warps stream tiles of 32
+//    (d <= 64) or 32/T (d = 128, 256) polys through shared memory with TMA
+//    bulk copies (one piece per lane) into 16-byte-padded slots, so per-thread
+//    128-bit shared loads are bank-conflict free; mbarriers track arrival and
+//    each lane's bulk group tracks its store. The next tile's input is
+//    prefetched into the other buffer while the current tile computes.
+//  * The transforms are fully unrolled (register-resident data), which makes
+//    the kernel body larger than the instruction cache, so the warps of a CTA
+//    run in lock step: a CTA barrier after every stage keeps all of them
+//    inside one stage's code.
+//  * d <= 64: one thread per polynomial, every twiddle index a compile-time
+//    constant taken from the kernel parameter block. d = 128 / 256: T = 2 / 4
+//    threads per polynomial, 64 coefficients each; log2(T) stages cross
+//    threads through warp shuffles; twiddles staged in shared memory.
 #include <cuda_runtime.h>
 
 #include "grid_async.cuh"
@@ -32,8 +37,8 @@
 namespace grid {
 namespace {
 
-constexpr int kWarpsPerBlock = 4;
-constexpr int kThreads = kWarpsPerBlock * 32;
+constexpr int kWarps = 12;  // warps per (persistent) CTA
+constexpr int kThreads = kWarps * 32;
 
 __host__ __device__ constexpr int ilog2(int x) { return x <= 1 ? 0 : 1 + ilog2(x >> 1); }
 
@@ -43,48 +48,57 @@ __host__ __device__ constexpr int brv(int x, int bits) {
   return r;
 }
 
-__device__ __forceinline__ void ct_bfly(uint32_t& u, uint32_t& v, uint32_t w, uint32_t wq,
-                                        uint32_t q) {
-  const uint32_t t = mont_mul_c(v, w, wq, q);
-  v = sub_mod(u, t, q);
-  u = add_mod(u, t, q);
+struct Consts {
+  uint32_t q, qinv, r1;
+};
+
+__device__ __forceinline__ Consts consts_of(const FieldParams& f) {
+  return Consts{f.q, f.qinv, f.r1};
 }
 
+// CT butterfly on lazy words: (u, v) -> (u + w v, u - w v).
+__device__ __forceinline__ void ct_bfly(uint32_t& u, uint32_t& v, uint32_t w, uint32_t wq,
+                                        const Consts& c) {
+  const uint32_t t = mont_c(v, w, wq, c.q);
+  v = sub_lazy(u, t, c.q);
+  u = add_lazy(u, t, c.r1);
+}
+
+// GS butterfly on canonical words: (u, v) -> (u + v, (u - v) w).
 __device__ __forceinline__ void gs_bfly(uint32_t& u, uint32_t& v, uint32_t w, uint32_t wq,
-                                        uint32_t q) {
-  const uint32_t s = add_mod(u, v, q);
-  const uint32_t d = sub_mod(u, v, q);
+                                        const Consts& c) {
+  const uint32_t s = add_canon(u, v, c.q);
+  const uint32_t d = sub_lazy(u, v, c.q);
   u = s;
-  v = mont_mul_c(d, w, wq, q);
+  v = mont_c(d, w, wq, c.q);
 }
 
 // ---------------------------------------------------------------------------
-// Thread-per-polynomial transforms (d <= 64). x holds positions 0..D-1.
+// Thread-per-polynomial transforms (d <= 64).
 // ---------------------------------------------------------------------------
 template <int D, int LEN>
-__device__ __forceinline__ void fwd1_stages(uint32_t (&x)[D], const Tw1<D>& tw) {
-  const uint32_t q = tw.f.q;
+__device__ __forceinline__ void fwd1_stages(uint32_t (&x)[D], const Tw1<D>& tw, const Consts& c) {
 #pragma unroll
   for (int g = 0; g < D / (2 * LEN); ++g) {
     const int k = D / (2 * LEN) + g;
 #pragma unroll
     for (int j = g * 2 * LEN; j < g * 2 * LEN + LEN; ++j)
-      ct_bfly(x[j], x[j + LEN], tw.fw[k][0], tw.fw[k][1], q);
+      ct_bfly(x[j], x[j + LEN], tw.fw[k][0], tw.fw[k][1], c);
   }
-  if constexpr (LEN > 1) fwd1_stages<D, LEN / 2>(x, tw);
+  __syncthreads();
+  if constexpr (LEN > 1) fwd1_stages<D, LEN / 2>(x, tw, c);
 }
 
 template <int D, int LEN>
-__device__ __forceinline__ void inv1_stages(uint32_t (&x)[D], const Tw1<D>& tw) {
-  const uint32_t q = tw.f.q;
+__device__ __forceinline__ void inv1_stages(uint32_t (&x)[D], const Tw1<D>& tw, const Consts& c) {
   if constexpr (LEN == D / 2) {
     // Last GS stage (single group, k = 1) with d^-1 folded in.
 #pragma unroll
     for (int j = 0; j < LEN; ++j) {
-      const uint32_t s = add_mod(x[j], x[j + LEN], q);
-      const uint32_t d = sub_mod(x[j], x[j + LEN], q);
-      x[j] = mont_mul_c(s, tw.ninv[0], tw.ninv[1], q);
-      x[j + LEN] = mont_mul_c(d, tw.iw1n[0], tw.iw1n[1], q);
+      const uint32_t s = add_canon(x[j], x[j + LEN], c.q);
+      const uint32_t d = sub_lazy(x[j], x[j + LEN], c.q);
+      x[j] = mont_c(s, tw.ninv[0], tw.ninv[1], c.q);
+      x[j + LEN] = mont_c(d, tw.iw1n[0], tw.iw1n[1], c.q);
     }
   } else {
 #pragma unroll
@@ -92,116 +106,147 @@ __device__ __forceinline__ void inv1_stages(uint32_t (&x)[D], const Tw1<D>& tw) 
       const int k = D / (2 * LEN) + g;
 #pragma unroll
       for (int j = g * 2 * LEN; j < g * 2 * LEN + LEN; ++j)
-        gs_bfly(x[j], x[j + LEN], tw.iw[k][0], tw.iw[k][1], q);
+        gs_bfly(x[j], x[j + LEN], tw.iw[k][0], tw.iw[k][1], c);
     }
-    inv1_stages<D, LEN * 2>(x, tw);
+    __syncthreads();
+    inv1_stages<D, LEN * 2>(x, tw, c);
   }
 }
 
+// Per-warp TMA pipeline state shared by both kernel families.
+struct WarpPipe {
+  uint64_t* bars;  // [buf * 2 + {0: a, 1: b}]
+  uint32_t parity = 0, pending = 0;
+
+  __device__ void init(uint64_t* b, int lane) {
+    bars = b;
+    if (lane == 0) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i) mbar_init(&bars[i], 1);
+      fence_mbar_init();
+    }
+    __syncwarp();
+  }
+  // Arm barrier `bar` for `bytes`; false (and nothing armed) if bytes == 0.
+  __device__ bool arm(int bar, uint32_t bytes, int lane) {
+    if (bytes == 0) return false;
+    if (lane == 0) mbar_arrive_expect_tx(&bars[bar], bytes);
+    __syncwarp();
+    pending |= 1u << bar;
+    return true;
+  }
+  __device__ bool wait(int bar, int* err) {
+    if (!(pending & (1u << bar))) return true;
+    const bool ok = mbar_wait(&bars[bar], (parity >> bar) & 1u, err);
+    parity ^= 1u << bar;
+    pending &= ~(1u << bar);
+    return ok;
+  }
+  __device__ void drain(int* err) {
+    for (int bar = 0; bar < 4; ++bar)
+      if (pending & (1u << bar)) mbar_wait(&bars[bar], (parity >> bar) & 1u, err);
+    pending = 0;
+  }
+};
+
+__device__ __forceinline__ uint32_t polys_left(unsigned long long p0, unsigned long long n,
+                                               uint32_t cap) {
+  if (p0 >= n) return 0;
+  const unsigned long long left = n - p0;
+  return left < cap ? (uint32_t)left : cap;
+}
+
 template <int D, int MODE>
-__global__ void __launch_bounds__(kThreads) ntt1_kernel(const uint32_t* __restrict__ a,
-                                                        const uint32_t* __restrict__ b,
-                                                        uint32_t* out, unsigned long long npolys,
-                                                        const __grid_constant__ Tw1<D> tw,
-                                                        int* __restrict__ err) {
+__global__ void __launch_bounds__(kThreads, 1) ntt1_kernel(const uint32_t* __restrict__ a,
+                                                           const uint32_t* __restrict__ b,
+                                                           uint32_t* out, unsigned long long npolys,
+                                                           const __grid_constant__ Tw1<D> tw,
+                                                           int* __restrict__ err) {
   constexpr int LOGD = ilog2(D);
-  constexpr int PS = D + 4;                 // padded slot stride (words)
-  constexpr uint32_t PIECE = D * 4;         // bytes each lane moves per tile
-  constexpr int BUF = 32 * PS;              // words per tile buffer
+  constexpr int PS = D + 4;          // padded slot stride (words)
+  constexpr uint32_t PIECE = D * 4;  // bytes each lane moves per tile
+  constexpr int BUF = 32 * PS;       // words per tile buffer
+  constexpr unsigned long long BT = 32ull * kWarps;  // polys per CTA tile
   extern __shared__ __align__(128) uint32_t smem[];
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   uint32_t* wbase = smem + warp * 2 * BUF;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kWarpsPerBlock * 2 * BUF) + warp * 4;
-  if (lane == 0) {
-#pragma unroll
-    for (int i = 0; i < 4; ++i) mbar_init(&bars[i], 1);
-    fence_mbar_init();
-  }
-  __syncwarp();
+  WarpPipe pipe;
+  pipe.init(reinterpret_cast<uint64_t*>(smem + kWarps * 2 * BUF) + warp * 4, lane);
+  const Consts c = consts_of(tw.f);
 
-  const unsigned long long ntiles = (npolys + 31) >> 5;
-  const unsigned long long stride = (unsigned long long)gridDim.x * kWarpsPerBlock;
-  unsigned long long tile = (unsigned long long)blockIdx.x * kWarpsPerBlock + warp;
-  uint32_t parity = 0, pending = 0;
-
-  auto issue = [&](uint32_t* buf, const uint32_t* src, unsigned long long t, int bar) {
-    const unsigned long long p0 = t << 5;
-    const unsigned long long left = npolys - p0;
-    const uint32_t np = left < 32 ? (uint32_t)left : 32u;
-    if (lane == 0) mbar_arrive_expect_tx(&bars[bar], np * PIECE);
-    __syncwarp();
-    if ((uint32_t)lane < np) bulk_load(buf + lane * PS, src + (p0 + lane) * D, PIECE, &bars[bar]);
-    pending |= 1u << bar;
-  };
-  auto wait = [&](int bar) -> bool {
-    const bool ok = mbar_wait(&bars[bar], (parity >> bar) & 1u, err);
-    parity ^= 1u << bar;
-    pending &= ~(1u << bar);
-    return __all_sync(0xffffffffu, ok);  // keep the warp's control flow uniform
+  const unsigned long long nbt = (npolys + BT - 1) / BT;
+  auto issue = [&](uint32_t* buf, const uint32_t* src, unsigned long long bt, int bar) {
+    const unsigned long long p0 = bt * BT + warp * 32ull;
+    const uint32_t np = polys_left(p0, npolys, 32);
+    if (pipe.arm(bar, np * PIECE, lane) && (uint32_t)lane < np)
+      bulk_load(buf + lane * PS, src + (p0 + lane) * D, PIECE, &pipe.bars[bar]);
   };
 
   bool ok = true;
   int buf = 0;
-  if (tile < ntiles) issue(wbase, a, tile, 0);
-  for (; tile < ntiles; tile += stride, buf ^= 1) {
-    uint32_t* s = wbase + buf * BUF;
-    uint32_t* slot = s + lane * PS;
-    const unsigned long long p0 = tile << 5;
-    const unsigned long long left = npolys - p0;
-    const uint32_t np = left < 32 ? (uint32_t)left : 32u;
+  unsigned long long bt = blockIdx.x;
+  if (bt < nbt) issue(wbase, a, bt, 0);
+  for (; bt < nbt; bt += gridDim.x, buf ^= 1) {  // trip count is uniform over the CTA
+    uint32_t* slot = wbase + buf * BUF + lane * PS;
+    const unsigned long long p0 = bt * BT + warp * 32ull;
+    const uint32_t np = polys_left(p0, npolys, 32);
 
-    if (!wait(buf * 2)) { ok = false; break; }
+    ok = __syncthreads_and(pipe.wait(buf * 2, err));
+    if (!ok) break;
     uint32_t x[D];
     const uint4* sv = reinterpret_cast<const uint4*>(slot);
 #pragma unroll
-    for (int c = 0; c < D / 4; ++c) {
-      const uint4 v = sv[c];
+    for (int cc = 0; cc < D / 4; ++cc) {
+      const uint4 v = sv[cc];
       if constexpr (MODE == MODE_INV) {
-        x[brv(4 * c + 0, LOGD)] = v.x;
-        x[brv(4 * c + 1, LOGD)] = v.y;
-        x[brv(4 * c + 2, LOGD)] = v.z;
-        x[brv(4 * c + 3, LOGD)] = v.w;
+        x[brv(4 * cc + 0, LOGD)] = v.x;
+        x[brv(4 * cc + 1, LOGD)] = v.y;
+        x[brv(4 * cc + 2, LOGD)] = v.z;
+        x[brv(4 * cc + 3, LOGD)] = v.w;
       } else {
-        x[4 * c + 0] = v.x;
-        x[4 * c + 1] = v.y;
-        x[4 * c + 2] = v.z;
-        x[4 * c + 3] = v.w;
+        x[4 * cc + 0] = v.x;
+        x[4 * cc + 1] = v.y;
+        x[4 * cc + 2] = v.z;
+        x[4 * cc + 3] = v.w;
       }
     }
     fence_proxy_async_smem();
     __syncwarp();
-    const unsigned long long next = tile + stride;
-    if (next < ntiles) {
-      bulk_wait_read_all();
+    if (bt + gridDim.x < nbt) {
+      bulk_wait_read_all();  // this lane's previous store out of the other buffer is done
       __syncwarp();
-      issue(wbase + (buf ^ 1) * BUF, a, next, (buf ^ 1) * 2);
+      issue(wbase + (buf ^ 1) * BUF, a, bt + gridDim.x, (buf ^ 1) * 2);
     }
-    if constexpr (MODE == MODE_MULINV) issue(s, b, tile, buf * 2 + 1);
+    if constexpr (MODE == MODE_MULINV) issue(wbase + buf * BUF, b, bt, buf * 2 + 1);
 
-    if constexpr (MODE != MODE_INV) fwd1_stages<D, D / 2>(x, tw);
+    if constexpr (MODE != MODE_INV) fwd1_stages<D, D / 2>(x, tw, c);
     if constexpr (MODE == MODE_MULINV) {
-      if (!wait(buf * 2 + 1)) { ok = false; break; }
-      const uint32_t q = tw.f.q, qinv = tw.f.qinv;
+      ok = __syncthreads_and(pipe.wait(buf * 2 + 1, err));
+      if (!ok) break;
 #pragma unroll
-      for (int c = 0; c < D / 4; ++c) {
-        const uint4 v = sv[c];
-        x[brv(4 * c + 0, LOGD)] = mont_mul(x[brv(4 * c + 0, LOGD)], v.x, q, qinv);
-        x[brv(4 * c + 1, LOGD)] = mont_mul(x[brv(4 * c + 1, LOGD)], v.y, q, qinv);
-        x[brv(4 * c + 2, LOGD)] = mont_mul(x[brv(4 * c + 2, LOGD)], v.z, q, qinv);
-        x[brv(4 * c + 3, LOGD)] = mont_mul(x[brv(4 * c + 3, LOGD)], v.w, q, qinv);
+      for (int cc = 0; cc < D / 4; ++cc) {
+        const uint4 v = sv[cc];
+        x[brv(4 * cc + 0, LOGD)] = mont_v(x[brv(4 * cc + 0, LOGD)], v.x, c.q, c.qinv);
+        x[brv(4 * cc + 1, LOGD)] = mont_v(x[brv(4 * cc + 1, LOGD)], v.y, c.q, c.qinv);
+        x[brv(4 * cc + 2, LOGD)] = mont_v(x[brv(4 * cc + 2, LOGD)], v.z, c.q, c.qinv);
+        x[brv(4 * cc + 3, LOGD)] = mont_v(x[brv(4 * cc + 3, LOGD)], v.w, c.q, c.qinv);
       }
+      __syncthreads();
     }
-    if constexpr (MODE != MODE_FWD) inv1_stages<D, 1>(x, tw);
+    if constexpr (MODE != MODE_FWD) inv1_stages<D, 1>(x, tw, c);
 
     uint4* so = reinterpret_cast<uint4*>(slot);
 #pragma unroll
-    for (int c = 0; c < D / 4; ++c) {
+    for (int cc = 0; cc < D / 4; ++cc) {
       if constexpr (MODE == MODE_FWD) {
-        so[c] = make_uint4(x[brv(4 * c + 0, LOGD)], x[brv(4 * c + 1, LOGD)],
-                           x[brv(4 * c + 2, LOGD)], x[brv(4 * c + 3, LOGD)]);
+        // lazy words -> canonical (x * 2^32 * 2^-32)
+        so[cc] = make_uint4(mont_v(x[brv(4 * cc + 0, LOGD)], c.r1, c.q, c.qinv),
+                            mont_v(x[brv(4 * cc + 1, LOGD)], c.r1, c.q, c.qinv),
+                            mont_v(x[brv(4 * cc + 2, LOGD)], c.r1, c.q, c.qinv),
+                            mont_v(x[brv(4 * cc + 3, LOGD)], c.r1, c.q, c.qinv));
       } else {
-        so[c] = make_uint4(x[4 * c + 0], x[4 * c + 1], x[4 * c + 2], x[4 * c + 3]);
+        so[cc] = make_uint4(x[4 * cc + 0], x[4 * cc + 1], x[4 * cc + 2], x[4 * cc + 3]);
       }
     }
     fence_proxy_async_smem();
@@ -210,22 +255,18 @@ __global__ void __launch_bounds__(kThreads) ntt1_kernel(const uint32_t* __restri
       bulk_commit();
     }
   }
-  if (!ok) {
-    // Let copies already in flight land before the block's shared memory goes away.
-    for (int bar = 0; bar < 4; ++bar)
-      if (pending & (1u << bar)) mbar_wait(&bars[bar], (parity >> bar) & 1u, err);
-  }
+  if (!ok) pipe.drain(err);  // let copies already in flight land
   bulk_wait_all();
 }
 
 // ---------------------------------------------------------------------------
 // T threads per polynomial (d = 128, 256). Thread t of a polynomial holds the
 // 4-word chunks c = T*m + t (m = 0 .. D/(4T)-1): local element e = 4m + s is
-// global position i = 4T*m + 4t + s.
+// position i = 4T*m + 4t + s.
 // ---------------------------------------------------------------------------
 template <int D, int T, int LEN>
 __device__ __forceinline__ void fwdT_stages(uint32_t (&x)[D / T], const uint2* __restrict__ tws,
-                                            int t, uint32_t q) {
+                                            int t, const Consts& c) {
   constexpr int E = D / T;
   constexpr int LOG2LEN = ilog2(2 * LEN);
   if constexpr (LEN >= 4 * T) {
@@ -235,7 +276,7 @@ __device__ __forceinline__ void fwdT_stages(uint32_t (&x)[D / T], const uint2* _
       if ((e & STEP) == 0) {
         const int k = D / (2 * LEN) + ((4 * T * (e >> 2)) >> LOG2LEN);
         const uint2 w = tws[k];
-        ct_bfly(x[e], x[e + STEP], w.x, w.y, q);
+        ct_bfly(x[e], x[e + STEP], w.x, w.y, c);
       }
     }
   } else if constexpr (LEN >= 4) {
@@ -245,10 +286,10 @@ __device__ __forceinline__ void fwdT_stages(uint32_t (&x)[D / T], const uint2* _
     for (int e = 0; e < E; ++e) {
       const int k = D / (2 * LEN) + ((4 * T * (e >> 2) + 4 * t) >> LOG2LEN);
       const uint2 w = tws[k];
-      const uint32_t prod = mont_mul_c(x[e], w.x, w.y, q);
+      const uint32_t prod = mont_c(x[e], w.x, w.y, c.q);
       const uint32_t mine = upper ? prod : x[e];
       const uint32_t other = __shfl_xor_sync(0xffffffffu, mine, M);
-      x[e] = upper ? sub_mod(other, mine, q) : add_mod(mine, other, q);
+      x[e] = upper ? sub_lazy(other, mine, c.q) : add_lazy(mine, other, c.r1);
     }
   } else {
 #pragma unroll
@@ -256,16 +297,17 @@ __device__ __forceinline__ void fwdT_stages(uint32_t (&x)[D / T], const uint2* _
       if ((e & LEN) == 0) {
         const int k = D / (2 * LEN) + ((4 * T * (e >> 2) + 4 * t + (e & 3)) >> LOG2LEN);
         const uint2 w = tws[k];
-        ct_bfly(x[e], x[e + LEN], w.x, w.y, q);
+        ct_bfly(x[e], x[e + LEN], w.x, w.y, c);
       }
     }
   }
-  if constexpr (LEN > 1) fwdT_stages<D, T, LEN / 2>(x, tws, t, q);
+  __syncthreads();
+  if constexpr (LEN > 1) fwdT_stages<D, T, LEN / 2>(x, tws, t, c);
 }
 
 template <int D, int T, int LEN>
 __device__ __forceinline__ void invT_stages(uint32_t (&x)[D / T], const uint2* __restrict__ tws,
-                                            int t, uint32_t q) {
+                                            int t, const Consts& c) {
   constexpr int E = D / T;
   constexpr int LOG2LEN = ilog2(2 * LEN);
   const uint2* iw = tws + D;
@@ -276,10 +318,10 @@ __device__ __forceinline__ void invT_stages(uint32_t (&x)[D / T], const uint2* _
 #pragma unroll
     for (int e = 0; e < E; ++e) {
       if ((e & STEP) == 0) {
-        const uint32_t s = add_mod(x[e], x[e + STEP], q);
-        const uint32_t d = sub_mod(x[e], x[e + STEP], q);
-        x[e] = mont_mul_c(s, n0.x, n0.y, q);
-        x[e + STEP] = mont_mul_c(d, n1.x, n1.y, q);
+        const uint32_t s = add_canon(x[e], x[e + STEP], c.q);
+        const uint32_t d = sub_lazy(x[e], x[e + STEP], c.q);
+        x[e] = mont_c(s, n0.x, n0.y, c.q);
+        x[e + STEP] = mont_c(d, n1.x, n1.y, c.q);
       }
     }
   } else {
@@ -290,7 +332,7 @@ __device__ __forceinline__ void invT_stages(uint32_t (&x)[D / T], const uint2* _
         if ((e & STEP) == 0) {
           const int k = D / (2 * LEN) + ((4 * T * (e >> 2)) >> LOG2LEN);
           const uint2 w = iw[k];
-          gs_bfly(x[e], x[e + STEP], w.x, w.y, q);
+          gs_bfly(x[e], x[e + STEP], w.x, w.y, c);
         }
       }
     } else if constexpr (LEN >= 4) {
@@ -302,8 +344,9 @@ __device__ __forceinline__ void invT_stages(uint32_t (&x)[D / T], const uint2* _
         const uint2 w = iw[k];
         const uint32_t other = __shfl_xor_sync(0xffffffffu, x[e], M);
         // lower keeps u + v; upper gets (u - v) * w with u = other, v = x[e]
-        const uint32_t s = upper ? sub_mod(other, x[e], q) : add_mod(x[e], other, q);
-        const uint32_t prod = mont_mul_c(s, w.x, w.y, q);
+        const uint32_t s =
+            upper ? sub_lazy(other, x[e], c.q) : add_canon(x[e], other, c.q);
+        const uint32_t prod = mont_c(s, w.x, w.y, c.q);
         x[e] = upper ? prod : s;
       }
     } else {
@@ -312,85 +355,69 @@ __device__ __forceinline__ void invT_stages(uint32_t (&x)[D / T], const uint2* _
         if ((e & LEN) == 0) {
           const int k = D / (2 * LEN) + ((4 * T * (e >> 2) + 4 * t + (e & 3)) >> LOG2LEN);
           const uint2 w = iw[k];
-          gs_bfly(x[e], x[e + LEN], w.x, w.y, q);
+          gs_bfly(x[e], x[e + LEN], w.x, w.y, c);
         }
       }
     }
-    invT_stages<D, T, LEN * 2>(x, tws, t, q);
+    __syncthreads();
+    invT_stages<D, T, LEN * 2>(x, tws, t, c);
   }
 }
 
 template <int D, int T, int MODE>
-__global__ void __launch_bounds__(kThreads) nttT_kernel(const uint32_t* __restrict__ a,
-                                                        const uint32_t* __restrict__ b,
-                                                        uint32_t* out, unsigned long long npolys,
-                                                        const uint2* __restrict__ gtw,
-                                                        FieldParams f, int* __restrict__ err) {
+__global__ void __launch_bounds__(kThreads, 1) nttT_kernel(const uint32_t* __restrict__ a,
+                                                           const uint32_t* __restrict__ b,
+                                                           uint32_t* out, unsigned long long npolys,
+                                                           const uint2* __restrict__ gtw,
+                                                           FieldParams f, int* __restrict__ err) {
   constexpr int LOGD = ilog2(D);
-  constexpr int E = D / T;                   // words per thread
-  constexpr int PW = 32 / T;                 // polys per warp tile
-  constexpr int PS = D + 4 * T;              // padded slot stride (words)
-  constexpr uint32_t PIECE = E * 4;          // bytes each lane moves
+  constexpr int E = D / T;            // words per thread
+  constexpr int PW = 32 / T;          // polys per warp tile
+  constexpr int PS = D + 4 * T;       // padded slot stride (words)
+  constexpr uint32_t PIECE = E * 4;   // bytes each lane moves
   constexpr int BUF = PW * PS;
-  constexpr int TWN = 2 * D + 2;             // uint2 twiddle entries
+  constexpr int TWN = 2 * D + 2;      // uint2 twiddle entries
+  constexpr unsigned long long BT = (unsigned long long)PW * kWarps;
   extern __shared__ __align__(128) uint32_t smem[];
   uint2* tws = reinterpret_cast<uint2*>(smem);
-  uint32_t* tiles = smem + 2 * TWN + 4;      // keep 16-byte alignment
+  uint32_t* tiles = smem + 2 * TWN + 4;  // keeps 16-byte alignment
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
-  const int pl = lane / T;                   // poly within tile
+  const int pl = lane / T;  // poly within the warp tile
   const int t = lane % T;
   for (int i = threadIdx.x; i < TWN; i += blockDim.x) tws[i] = gtw[i];
   uint32_t* wbase = tiles + warp * 2 * BUF;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(tiles + kWarpsPerBlock * 2 * BUF) + warp * 4;
-  if (lane == 0) {
-#pragma unroll
-    for (int i = 0; i < 4; ++i) mbar_init(&bars[i], 1);
-    fence_mbar_init();
-  }
+  WarpPipe pipe;
+  pipe.init(reinterpret_cast<uint64_t*>(tiles + kWarps * 2 * BUF) + warp * 4, lane);
   __syncthreads();
+  const Consts c = consts_of(f);
+  const int bt_t = brv(4 * t, LOGD);  // bit-reversed contribution of t
 
-  const unsigned long long ntiles = (npolys + PW - 1) / PW;
-  const unsigned long long stride = (unsigned long long)gridDim.x * kWarpsPerBlock;
-  unsigned long long tile = (unsigned long long)blockIdx.x * kWarpsPerBlock + warp;
-  uint32_t parity = 0, pending = 0;
-  const uint32_t q = f.q, qinv = f.qinv;
-  const int bt = brv(4 * t, LOGD);           // bit-reversed contribution of t
-
-  auto issue = [&](uint32_t* buf, const uint32_t* src, unsigned long long tl, int bar) {
-    const unsigned long long p0 = tl * PW;
-    const unsigned long long left = npolys - p0;
-    const uint32_t np = left < (unsigned long long)PW ? (uint32_t)left : (uint32_t)PW;
-    if (lane == 0) mbar_arrive_expect_tx(&bars[bar], np * D * 4);
-    __syncwarp();
-    if ((uint32_t)pl < np)
-      bulk_load(buf + pl * PS + t * E, src + (p0 + pl) * D + t * E, PIECE, &bars[bar]);
-    pending |= 1u << bar;
-  };
-  auto wait = [&](int bar) -> bool {
-    const bool ok = mbar_wait(&bars[bar], (parity >> bar) & 1u, err);
-    parity ^= 1u << bar;
-    pending &= ~(1u << bar);
-    return __all_sync(0xffffffffu, ok);  // keep the warp's control flow uniform
+  const unsigned long long nbt = (npolys + BT - 1) / BT;
+  auto issue = [&](uint32_t* buf, const uint32_t* src, unsigned long long bt, int bar) {
+    const unsigned long long p0 = bt * BT + (unsigned long long)warp * PW;
+    const uint32_t np = polys_left(p0, npolys, PW);
+    if (pipe.arm(bar, np * D * 4, lane) && (uint32_t)pl < np)
+      bulk_load(buf + pl * PS + t * E, src + (p0 + pl) * D + t * E, PIECE, &pipe.bars[bar]);
   };
 
   bool ok = true;
   int buf = 0;
-  if (tile < ntiles) issue(wbase, a, tile, 0);
-  for (; tile < ntiles; tile += stride, buf ^= 1) {
-    uint32_t* s = wbase + buf * BUF;
-    uint32_t* slot = s + pl * PS;
-    const unsigned long long p0 = tile * PW;
-    const unsigned long long left = npolys - p0;
-    const uint32_t np = left < (unsigned long long)PW ? (uint32_t)left : (uint32_t)PW;
+  unsigned long long bt = blockIdx.x;
+  if (bt < nbt) issue(wbase, a, bt, 0);
+  for (; bt < nbt; bt += gridDim.x, buf ^= 1) {
+    uint32_t* slot = wbase + buf * BUF + pl * PS;
+    const unsigned long long p0 = bt * BT + (unsigned long long)warp * PW;
+    const uint32_t np = polys_left(p0, npolys, PW);
 
-    if (!wait(buf * 2)) { ok = false; break; }
+    ok = __syncthreads_and(pipe.wait(buf * 2, err));
+    if (!ok) break;
     uint32_t x[E];
     if constexpr (MODE == MODE_INV) {
 #pragma unroll
       for (int e = 0; e < E; ++e) {
         const int i = 4 * T * (e >> 2) + (e & 3);
-        x[e] = slot[brv(i, LOGD) | bt];
+        x[e] = slot[brv(i, LOGD) | bt_t];
       }
     } else {
 #pragma unroll
@@ -404,31 +431,32 @@ __global__ void __launch_bounds__(kThreads) nttT_kernel(const uint32_t* __restri
     }
     fence_proxy_async_smem();
     __syncwarp();
-    const unsigned long long next = tile + stride;
-    if (next < ntiles) {
+    if (bt + gridDim.x < nbt) {
       bulk_wait_read_all();
       __syncwarp();
-      issue(wbase + (buf ^ 1) * BUF, a, next, (buf ^ 1) * 2);
+      issue(wbase + (buf ^ 1) * BUF, a, bt + gridDim.x, (buf ^ 1) * 2);
     }
-    if constexpr (MODE == MODE_MULINV) issue(s, b, tile, buf * 2 + 1);
+    if constexpr (MODE == MODE_MULINV) issue(wbase + buf * BUF, b, bt, buf * 2 + 1);
 
-    if constexpr (MODE != MODE_INV) fwdT_stages<D, T, D / 2>(x, tws, t, q);
+    if constexpr (MODE != MODE_INV) fwdT_stages<D, T, D / 2>(x, tws, t, c);
     if constexpr (MODE == MODE_MULINV) {
-      if (!wait(buf * 2 + 1)) { ok = false; break; }
+      ok = __syncthreads_and(pipe.wait(buf * 2 + 1, err));
+      if (!ok) break;
 #pragma unroll
       for (int e = 0; e < E; ++e) {
         const int i = 4 * T * (e >> 2) + (e & 3);
-        x[e] = mont_mul(x[e], slot[brv(i, LOGD) | bt], q, qinv);
+        x[e] = mont_v(x[e], slot[brv(i, LOGD) | bt_t], c.q, c.qinv);
       }
+      __syncthreads();
     }
-    if constexpr (MODE != MODE_FWD) invT_stages<D, T, 1>(x, tws, t, q);
+    if constexpr (MODE != MODE_FWD) invT_stages<D, T, 1>(x, tws, t, c);
 
-    __syncwarp();  // every lane done reading the slot before it is overwritten
+    __syncwarp();  // every lane of the warp done reading its slots
     if constexpr (MODE == MODE_FWD) {
 #pragma unroll
       for (int e = 0; e < E; ++e) {
         const int i = 4 * T * (e >> 2) + (e & 3);
-        slot[brv(i, LOGD) | bt] = x[e];
+        slot[brv(i, LOGD) | bt_t] = mont_v(x[e], c.r1, c.q, c.qinv);
       }
     } else {
 #pragma unroll
@@ -443,10 +471,7 @@ __global__ void __launch_bounds__(kThreads) nttT_kernel(const uint32_t* __restri
       bulk_commit();
     }
   }
-  if (!ok) {
-    for (int bar = 0; bar < 4; ++bar)
-      if (pending & (1u << bar)) mbar_wait(&bars[bar], (parity >> bar) & 1u, err);
-  }
+  if (!ok) pipe.drain(err);
   bulk_wait_all();
 }
 
@@ -470,10 +495,9 @@ Tw1<D> make_tw1(const grid_gpu_plan* p) {
   return tw;
 }
 
-int grid_size(const grid_gpu_plan* p, unsigned long long tiles, int blocks_per_sm) {
-  const unsigned long long want = (tiles + kWarpsPerBlock - 1) / kWarpsPerBlock;
+int grid_size(const grid_gpu_plan* p, unsigned long long block_tiles, int blocks_per_sm) {
   const unsigned long long cap = (unsigned long long)p->num_sms * blocks_per_sm;
-  unsigned long long g = want < cap ? want : cap;
+  const unsigned long long g = block_tiles < cap ? block_tiles : cap;
   return g < 1 ? 1 : (int)g;
 }
 
@@ -481,12 +505,12 @@ template <int D, int MODE>
 int run1(const grid_gpu_plan* p, const uint32_t* a, const uint32_t* b, uint32_t* out,
          size_t npolys, cudaStream_t s) {
   constexpr int PS = D + 4;
-  constexpr size_t smem = (size_t)kWarpsPerBlock * 2 * 32 * PS * 4 + kWarpsPerBlock * 4 * 8;
+  constexpr size_t smem = (size_t)kWarps * 2 * 32 * PS * 4 + kWarps * 4 * 8;
   static int bps_cache[kMaxDevices] = {};
   int bps = 0;
   const int st = prepare_kernel(ntt1_kernel<D, MODE>, smem, kThreads, p->device, bps_cache, &bps);
   if (st) return st;
-  const unsigned long long tiles = (npolys + 31) / 32;
+  const unsigned long long tiles = (npolys + 32ull * kWarps - 1) / (32ull * kWarps);
   const Tw1<D> tw = make_tw1<D>(p);
   ntt1_kernel<D, MODE><<<grid_size(p, tiles, bps), kThreads, smem, s>>>(
       a, b, out, (unsigned long long)npolys, tw, p->d_err);
@@ -498,14 +522,15 @@ int runT(const grid_gpu_plan* p, const uint32_t* a, const uint32_t* b, uint32_t*
          size_t npolys, cudaStream_t s) {
   constexpr int PW = 32 / T;
   constexpr int PS = D + 4 * T;
-  constexpr size_t smem =
-      (size_t)(2 * (2 * D + 2) + 4) * 4 + (size_t)kWarpsPerBlock * 2 * PW * PS * 4 +
-      kWarpsPerBlock * 4 * 8;
+  constexpr size_t smem = (size_t)(2 * (2 * D + 2) + 4) * 4 +
+                          (size_t)kWarps * 2 * PW * PS * 4 + kWarps * 4 * 8;
   static int bps_cache[kMaxDevices] = {};
   int bps = 0;
-  const int st = prepare_kernel(nttT_kernel<D, T, MODE>, smem, kThreads, p->device, bps_cache, &bps);
+  const int st =
+      prepare_kernel(nttT_kernel<D, T, MODE>, smem, kThreads, p->device, bps_cache, &bps);
   if (st) return st;
-  const unsigned long long tiles = (npolys + PW - 1) / PW;
+  const unsigned long long tiles =
+      (npolys + (unsigned long long)PW * kWarps - 1) / ((unsigned long long)PW * kWarps);
   nttT_kernel<D, T, MODE><<<grid_size(p, tiles, bps), kThreads, smem, s>>>(
       a, b, out, (unsigned long long)npolys, p->d_tw, p->f, p->d_err);
   return cuda_status(cudaGetLastError());

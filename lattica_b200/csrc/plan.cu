@@ -228,13 +228,19 @@ int host_pipeline(grid_gpu_plan* p, const uint32_t* const* ins, int nin, uint32_
                                     cudaMemcpyDeviceToHost, s);
     if (e != cudaSuccess) { status = cuda_status(e); break; }
   }
-  cudaError_t e0 = cudaStreamSynchronize(p->stream);
   cudaError_t e1 = cudaStreamSynchronize(p->stream2);
+  const int fin = finish_host_call(p, p->stream);
   if (status) return status;
-  if (e0 != cudaSuccess) return cuda_status(e0);
   if (e1 != cudaSuccess) return cuda_status(e1);
+  return fin;
+}
+
+// Synchronise `s`, then read and clear the plan's device error word.
+int finish_host_call(grid_gpu_plan* p, cudaStream_t s) {
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_status(e);
   int derr = 0;
-  cudaError_t e = cudaMemcpy(&derr, p->d_err, sizeof(int), cudaMemcpyDeviceToHost);
+  e = cudaMemcpy(&derr, p->d_err, sizeof(int), cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return cuda_status(e);
   if (derr) {
     cudaMemset(p->d_err, 0, sizeof(int));

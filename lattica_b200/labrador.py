@@ -1,0 +1,206 @@
+"""LaBRADOR prover hot calls on the GPU, mirroring the reference surface:
+`CommitKey::inner_commit_slice / inner_commit_decomposed` (labrador/src/crs.rs),
+`compute_garbage_g` (labrador/src/main_protocol/garbage.rs), `JLMatrix`
+(labrador/src/jl.rs) and `decompose_polys` (labrador/src/main_protocol/mod.rs).
+
+Witness layout: r parts x n polys x d Montgomery words (LabradorWitness parts,
+each a slice of CyclotomicPolyRing<R, d>).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from .commit import PreparedMatrix
+from .ntt import TwistedNttPlan, _is_torch, _stream_ptr, raise_status
+
+JL_MAX_RETRY = 100  # labrador/src/jl.rs:27
+
+
+def garbage_index(r: int, i: int, j: int) -> int:
+    """Upper-triangular index (main_protocol/mod.rs:664-670)."""
+    return i * r - (i * (i - 1)) // 2 + (j - i)
+
+
+def garbage_count(r: int) -> int:
+    return r * (r + 1) // 2
+
+
+@dataclass
+class DecomposedPolys:
+    """DecomposedPolys (main_protocol/mod.rs:361-375): flat[poly][limb] polys."""
+
+    flat: np.ndarray
+    num_polys: int
+    num_limbs: int
+    base: int
+
+
+def decompose_polys(plan: TwistedNttPlan, polys, base: int, num_limbs: int) -> DecomposedPolys:
+    """Balanced base-`base` decomposition (decompose_polys, main_protocol/mod.rs:731-747)."""
+    p = np.ascontiguousarray(polys, dtype=np.uint32).reshape(-1, plan.d)
+    out = np.empty((p.shape[0], num_limbs, plan.d), dtype=np.uint32)
+    st = _lib.load().grid_gpu_decompose_balanced(plan.handle, p.ctypes.data, p.shape[0], base,
+                                                 num_limbs, out.ctypes.data)
+    raise_status(st, "grid_gpu_decompose_balanced")
+    return DecomposedPolys(out.reshape(-1, plan.d), p.shape[0], num_limbs, base)
+
+
+def compute_garbage_g(plan: TwistedNttPlan, witness):
+    """g_ij = <s_i, s_j> for i <= j in garbage_index order (garbage.rs:76-93).
+    witness: (r, n, d) numpy uint32 or a CUDA tensor."""
+    r, n, d = (int(x) for x in witness.shape)
+    if d != plan.d:
+        raise ValueError("witness ring degree does not match the plan")
+    lib = _lib.load()
+    if _is_torch(witness):
+        import torch
+        g = torch.empty((garbage_count(r), d), dtype=witness.dtype, device=witness.device)
+        nb = C.c_size_t()
+        raise_status(lib.grid_gpu_gram_workspace(plan.handle, r, n, C.byref(nb)), "gram_ws")
+        ws = torch.empty(max(16, nb.value), dtype=torch.uint8, device=witness.device)
+        st = lib.grid_gpu_gram_dev(plan.handle, witness.data_ptr(), r, n, g.data_ptr(),
+                                   ws.data_ptr(), ws.numel(), _stream_ptr(witness))
+    else:
+        w = np.ascontiguousarray(witness, dtype=np.uint32)
+        g = np.empty((garbage_count(r), d), dtype=np.uint32)
+        st = lib.grid_gpu_gram(plan.handle, w.ctypes.data, r, n, g.ctypes.data)
+    raise_status(st, "grid_gpu_gram")
+    return g
+
+
+class CommitKey:
+    """The inner-commitment matrix A (kappa x n) of a LaBRADOR CommitKey
+    (labrador/src/crs.rs:111-216), kept resident on the device."""
+
+    def __init__(self, plan: TwistedNttPlan, a, kappa: int, n: int, is_evals: bool = False):
+        self.plan, self.kappa, self.n = plan, kappa, n
+        self.a = PreparedMatrix(plan, a, kappa, n, is_evals)
+
+    def inner_commit_slice(self, s_i):
+        """t_i = A * s_i (crs.rs:211-216); s_i (n, d) or a batch (r, n, d)."""
+        return self.a.mul_vec(s_i)
+
+    def inner_commit_decomposed(self, witness, b1: int, t1: int) -> DecomposedPolys:
+        """t_i = A s_i for every part, balanced limbs (crs.rs:225-256)."""
+        t = self.inner_commit_slice(witness)
+        return decompose_polys(self.plan, np.asarray(t).reshape(-1, self.plan.d), b1, t1)
+
+
+class JLMatrix:
+    """Seeded JL projection (labrador/src/jl.rs:34-509): ChaCha20 keystream,
+    key = seed, nonce = part index."""
+
+    def __init__(self, seed: bytes, rows: int, cols: int):
+        if cols <= 0:
+            raise ValueError("JL projection columns must be > 0 (n * d)")
+        if len(seed) != 32:
+            raise ValueError("JL seed must be 32 bytes")
+        self.seed, self.rows, self._cols = bytes(seed), rows, cols
+
+    @classmethod
+    def from_seed(cls, rows: int, cols: int, seed: bytes) -> "JLMatrix":
+        return cls(seed, rows, cols)
+
+    def cols(self) -> int:
+        return self._cols
+
+    def project_and_extract_jl_rows(self, plan: TwistedNttPlan, parts, num_parts: int, d: int,
+                                    extract: bool = True):
+        """(p, jl_rows_flat) like project_and_extract_jl_rows (jl.rs:267-303).
+        parts: (num_parts, cols) words; flat: rows*num_parts*cols int8."""
+        if d <= 0 or self._cols % d:
+            raise ValueError(f"cols ({self._cols}) must be divisible by ring degree d ({d})")
+        parts = np.ascontiguousarray(parts, dtype=np.uint32).reshape(-1)
+        if parts.size != num_parts * self._cols:
+            raise ValueError("parts count / length mismatch")
+        p = np.empty(self.rows, dtype=np.uint32)
+        flat = np.empty(self.rows * num_parts * self._cols, dtype=np.int8) if extract else None
+        seed = (C.c_uint8 * 32).from_buffer_copy(self.seed)
+        st = _lib.load().grid_gpu_jl_project(plan.handle, seed, self.rows, parts.ctypes.data,
+                                             num_parts, self._cols, d, p.ctypes.data,
+                                             flat.ctypes.data if extract else None)
+        raise_status(st, "grid_gpu_jl_project")
+        return p, flat
+
+    def project_multi(self, plan: TwistedNttPlan, parts, num_parts: int, d: int):
+        return self.project_and_extract_jl_rows(plan, parts, num_parts, d, extract=False)[0]
+
+
+@dataclass
+class RoundOutputs:
+    t_limbs: object   # (r*kappa*t1, d)
+    g: object         # (r(r+1)/2, d)
+    g_limbs: object   # (r(r+1)/2*t2, d) or None
+    p: object         # (jl_rows,) or None
+    jl_flat: object   # int8 or None
+
+
+def prover_round_dev(key: CommitKey, witness, b1: int, t1: int, b2: int, t2: int,
+                     jl_seed: bytes | None, jl_rows: int = 256, extract: bool = False,
+                     workspace=None) -> RoundOutputs:
+    """The GPU hot calls of one prove_step (step_prover.rs:118-170) on a CUDA
+    witness tensor (r, n, d): inner commitments + limbs, Gram + limbs, JL."""
+    import torch
+    r, n, d = (int(x) for x in witness.shape)
+    plan = key.plan
+    lib = _lib.load()
+    dev = witness.device
+    kappa = key.kappa
+    t_limbs = torch.empty((r * kappa * t1, d), dtype=torch.int32, device=dev)
+    g = torch.empty((garbage_count(r), d), dtype=torch.int32, device=dev)
+    g_limbs = torch.empty((garbage_count(r) * t2, d), dtype=torch.int32, device=dev) if t2 else None
+    p = torch.empty(jl_rows, dtype=torch.int32, device=dev) if jl_seed else None
+    flat = (torch.empty(jl_rows * r * n * d, dtype=torch.int8, device=dev)
+            if (jl_seed and extract) else None)
+    if workspace is None:
+        nb = C.c_size_t()
+        raise_status(lib.grid_gpu_prover_round_workspace(key.a.handle, r, jl_rows, C.byref(nb)),
+                     "prover_round_workspace")
+        workspace = torch.empty(max(16, nb.value), dtype=torch.uint8, device=dev)
+    seed = (C.c_uint8 * 32).from_buffer_copy(jl_seed) if jl_seed else None
+    st = lib.grid_gpu_prover_round_dev(
+        key.a.handle, witness.data_ptr(), r, b1, t1, b2, t2, seed, jl_rows, t_limbs.data_ptr(),
+        g.data_ptr(), g_limbs.data_ptr() if g_limbs is not None else None,
+        p.data_ptr() if p is not None else None, flat.data_ptr() if flat is not None else None,
+        workspace.data_ptr(), workspace.numel(), _stream_ptr(witness))
+    raise_status(st, "grid_gpu_prover_round_dev")
+    return RoundOutputs(t_limbs, g, g_limbs, p, flat)
+
+
+def _canonical(words, q: int):
+    """Montgomery words -> canonical integers (value = word * 2^-32 mod q)."""
+    rinv = pow(1 << 32, -1, q)
+    w = np.asarray(words, dtype=np.uint64).ravel()
+    return [(int(x) * rinv) % q for x in w]
+
+
+def squared_l2_norm_u128(words, q: int) -> int:
+    """Centered squared L2 norm, exact (main_protocol/mod.rs:225-247)."""
+    half = q // 2
+    total = 0
+    for v in _canonical(words, q):
+        a = q - v if v > half else v
+        total += a * a
+    if total >= 1 << 128:
+        raise OverflowError("norm overflow: sum exceeds u128")
+    return total
+
+
+def verify_norm(p_words, q: int, beta: float, rows: int = 256,
+                verify_factor: float = 128.0 ** 0.5) -> bool:
+    """||p||^2 <= (verify_factor * beta)^2 (jl.rs:533-547, JLProfile::paper_default)."""
+    import math
+    if not math.isfinite(beta) or beta <= 0.0:
+        return False
+    if len(np.asarray(p_words).ravel()) != rows:
+        return False
+    try:
+        norm_sq = float(squared_l2_norm_u128(p_words, q))
+    except OverflowError:
+        return False
+    threshold = (verify_factor * beta) * (verify_factor * beta)
+    return norm_sq <= threshold
