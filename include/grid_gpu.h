@@ -56,7 +56,8 @@ typedef enum grid_status {
   GRID_ERR_TIMEOUT = 11,           /* a bounded device-side wait gave up */
   GRID_ERR_UNSUPPORTED_DEGREE = 12, /* valid plan, but no kernel compiled for this d */
   GRID_ERR_MISALIGNED = 13,
-  GRID_ERR_NO_DEVICE = 14
+  GRID_ERR_NO_DEVICE = 14,
+  GRID_ERR_SCRATCH_LIMIT = 15      /* needs more than the no-alloc entry point's fixed buffer */
 } grid_status;
 
 typedef struct grid_gpu_plan grid_gpu_plan;
@@ -200,6 +201,20 @@ int grid_gpu_gadget_decompose_dev(const grid_gpu_plan* plan, const uint32_t* x, 
                                   uint64_t base, int digit_major, uint32_t* out, void* stream);
 int grid_gpu_gadget_decompose(grid_gpu_plan* plan, const uint32_t* x, size_t len, uint64_t base,
                               int digit_major, uint32_t* out);
+
+/* ---- Gram matrix without allocation (no counterpart in the reference) ----
+ * Same result as grid_gpu_gram_dev, for callers that cannot allocate device
+ * memory (a latency-bound prover loop, where cudaMalloc would synchronise the
+ * device, or a plugin whose host owns the memory pool): the scratch comes from
+ * a buffer compiled into the library, grid_gpu_noalloc_scratch_bytes() bytes
+ * (48 MiB) on every GPU that loads it, held until exit. Problems needing more
+ * (grid_gpu_gram_workspace) return GRID_ERR_SCRATCH_LIMIT. The first call on a
+ * device looks up the buffer's device address (cudaGetSymbolAddress); make that
+ * first call before any stream capture. All calls share the buffer: calls
+ * that overlap on the GPU race, so order them (for example on one stream). */
+size_t grid_gpu_noalloc_scratch_bytes(void);
+int grid_gpu_gram_noalloc_dev(const grid_gpu_plan* plan, const uint32_t* S, size_t r, size_t n,
+                              uint32_t* G, void* stream);
 
 /* ---- fused LaBRADOR prover round: the hot calls of prove_step
  *      (labrador/src/main_protocol/step_prover.rs:118-170) on one witness ----

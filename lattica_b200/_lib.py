@@ -17,7 +17,7 @@ STATUS_NAMES = {
     0: "OK", 1: "LengthMismatch", 2: "LengthNotPowerOfTwo", 3: "UnsupportedSize",
     4: "UnsupportedTwist", 5: "InvalidParameters", 6: "DimensionMismatch",
     7: "InvalidModulus", 8: "NullPointer", 9: "OutOfMemory", 10: "Cuda", 11: "Timeout",
-    12: "UnsupportedDegree", 13: "Misaligned", 14: "NoDevice",
+    12: "UnsupportedDegree", 13: "Misaligned", 14: "NoDevice", 15: "ScratchLimit",
 }
 
 _u32p = C.POINTER(C.c_uint32)
@@ -80,6 +80,8 @@ SIGNATURES = {
     "grid_gpu_prover_round_dev": (C.c_int, [_vp, _vp, C.c_size_t, C.c_uint64, C.c_size_t,
                                             C.c_uint64, C.c_size_t, _vp, C.c_size_t, _vp, _vp,
                                             _vp, _vp, _vp, _vp, C.c_size_t, _vp]),
+    "grid_gpu_noalloc_scratch_bytes": (C.c_size_t, []),
+    "grid_gpu_gram_noalloc_dev": (C.c_int, [_vp, _vp, C.c_size_t, C.c_size_t, _vp, _vp]),
     "grid_gpu_host_register": (C.c_int, [_vp, C.c_size_t]),
     "grid_gpu_host_unregister": (C.c_int, [_vp]),
 }

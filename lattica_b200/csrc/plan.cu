@@ -298,6 +298,7 @@ const char* grid_gpu_status_string(int status) {
     case GRID_ERR_UNSUPPORTED_DEGREE: return "no kernel compiled for this ring degree";
     case GRID_ERR_MISALIGNED: return "device buffer not 16-byte aligned";
     case GRID_ERR_NO_DEVICE: return "no CUDA device";
+    case GRID_ERR_SCRATCH_LIMIT: return "problem exceeds the no-alloc entry point's fixed scratch buffer";
     default: return "unknown status";
   }
 }

@@ -34,7 +34,7 @@ def test_library_exports_every_declared_symbol():
     assert declared <= set(_lib.SIGNATURES), sorted(declared - set(_lib.SIGNATURES))
     assert lib.grid_gpu_abi_version() >> 16 == 1
     assert lib.grid_gpu_max_degree() == 256
-    for code in range(15):
+    for code in range(16):
         assert lib.grid_gpu_status_string(code) not in (None, b"unknown status")
 
 
