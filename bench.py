@@ -173,6 +173,179 @@ def cpu_baseline(q, d, n_full):
             "sample": f"{reps} x {sample} polys of the {n_full}-poly workload, 1 thread"}
 
 
+def _mont_words(q, values):
+    """Signed integers -> PrimeField<q, u32> Montgomery words (host numpy)."""
+    v = np.asarray(values, dtype=np.int64) % q
+    return ((v.astype(object) << 32) % q).astype(np.uint64).astype(np.uint32)
+
+
+def _events_ms(fn, n, stream):
+    import torch
+    times = []
+    for _ in range(n):
+        s0 = torch.cuda.Event(enable_timing=True)
+        s1 = torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        fn()
+        s1.record(stream)
+        s1.synchronize()
+        times.append(s0.elapsed_time(s1))
+    return times
+
+
+def _pct(xs, p):
+    xs = sorted(xs)
+    return xs[min(len(xs) - 1, int(round(p / 100.0 * (len(xs) - 1))))]
+
+
+def measure_commit_plain(dev, reps=50):
+    """Plain Ajtai commit: A = 8 x 64 ring matrix (d = 64, q = 4294966657),
+    64 witnesses of 64 ternary polys; t = A s per witness."""
+    import ctypes as C
+    import torch
+    from lattica_b200 import TwistedNttPlan, _lib
+    from lattica_b200.commit import PreparedMatrix
+    q, d, rows, cols, batch = Q64, 64, 8, 64, 64
+    lib = _lib.load()
+    plan = TwistedNttPlan(q, d)
+    rng = np.random.default_rng(11)
+    A = rng.integers(0, q, (rows, cols, d), dtype=np.uint64).astype(np.uint32)
+    s_host = _mont_words(q, rng.integers(-1, 2, (batch, cols, d))).reshape(batch, cols, d)
+    M = PreparedMatrix(plan, A, rows, cols)
+    s = torch.from_numpy(s_host.view(np.int32)).to(dev)
+    t = torch.empty((batch, rows, d), dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    ws_b = M.workspace_bytes(batch)
+    ws = torch.empty(max(16, ws_b), dtype=torch.uint8, device=dev)
+    ws1 = torch.empty(max(16, M.workspace_bytes(1)), dtype=torch.uint8, device=dev)
+
+    def batched():
+        st = lib.grid_gpu_commit_dev(M.handle, s.data_ptr(), batch, t.data_ptr(), ws.data_ptr(),
+                                     ws.numel(), stream.cuda_stream)
+        assert st == 0
+
+    def per_call():  # one C-ABI call per commitment
+        for i in range(batch):
+            st = lib.grid_gpu_commit_dev(M.handle, s[i].data_ptr(), 1, t[i].data_ptr(),
+                                         ws1.data_ptr(), ws1.numel(), stream.cuda_stream)
+            assert st == 0
+
+    for _ in range(5):
+        batched()
+        per_call()
+    tb = _events_ms(batched, reps, stream)
+    tp = _events_ms(per_call, max(5, reps // 5), stream)
+    hs = torch.from_numpy(s_host.view(np.int32).copy()).pin_memory()
+    ht = torch.empty((batch, rows, d), dtype=torch.int32).pin_memory()
+    e2e = []
+    for i in range(reps + 3):
+        t0 = time.perf_counter()
+        st = lib.grid_gpu_commit(M.handle, hs.data_ptr(), batch, ht.data_ptr())
+        assert st == 0
+        if i >= 3:
+            e2e.append((time.perf_counter() - t0) * 1e3)
+    med_b, med_p, med_e = statistics.median(tb), statistics.median(tp), statistics.median(e2e)
+    return {"workload": "plain Ajtai commit: A 8x64, d=64, 64 ternary witnesses per batch",
+            "commits_per_s": batch / (med_b / 1e3), "batch_ms_p50": med_b,
+            "per_call_commits_per_s": batch / (med_p / 1e3),
+            "e2e_commits_per_s": batch / (med_e / 1e3), "e2e_batch_ms_p50": med_e,
+            "e2e_h2d_bytes": s_host.nbytes, "e2e_d2h_bytes": batch * rows * d * 4}
+
+
+def measure_round(dev, reps=50):
+    """LaBRADOR prover round on one instance: r = 64 witness vectors of
+    n = 2048 polys (d = 64, coefficients in [-2^11, 2^11]); inner commitments by
+    a 16 x 2048 matrix + base-2^8 balanced limbs (4), the r x r Gram (upper
+    triangle) + limbs, the 256-row JL projection."""
+    import torch
+    from lattica_b200 import TwistedNttPlan
+    from lattica_b200.labrador import CommitKey, prover_round_dev
+    q, d, r, n, kappa = Q64, 64, 64, 2048, 16
+    plan = TwistedNttPlan(q, d)
+    g = torch.Generator(device=dev).manual_seed(5)
+    A = torch.randint(0, q, (kappa, n, d), dtype=torch.int64, device=dev, generator=g).to(torch.int32)
+    key = CommitKey(plan, A, kappa, n)
+    coeffs = torch.randint(-2048, 2049, (r, n, d), dtype=torch.int64, device=dev, generator=g) % q
+    wit = ((coeffs * ((1 << 32) % q)) % q).to(torch.int32)  # Montgomery words x * 2^32 mod q
+    del coeffs
+    seed = bytes(range(32))
+    stream = torch.cuda.current_stream(dev)
+    ws = None
+    for _ in range(3):
+        out = prover_round_dev(key, wit, 256, 4, 256, 4, seed, 256)
+    torch.cuda.synchronize()
+    times = _events_ms(lambda: prover_round_dev(key, wit, 256, 4, 256, 4, seed, 256), reps, stream)
+    times_x = _events_ms(lambda: prover_round_dev(key, wit, 256, 4, 256, 4, seed, 256, extract=True),
+                         max(5, reps // 5), stream)
+    # end to end: witness from pinned host memory, outputs back to the host
+    hw = wit.cpu().pin_memory()
+    outs_host = None
+    e2e = []
+    for i in range(reps + 2):
+        t0 = time.perf_counter()
+        dw = hw.to(dev, non_blocking=True)
+        o = prover_round_dev(key, dw, 256, 4, 256, 4, seed, 256)
+        outs_host = [x.to("cpu", non_blocking=True) for x in (o.t_limbs, o.g, o.g_limbs, o.p)]
+        torch.cuda.synchronize()
+        if i >= 2:
+            e2e.append((time.perf_counter() - t0) * 1e3)
+    d2h = sum(x.numel() * x.element_size() for x in outs_host)
+    return {"workload": "LaBRADOR round: r=64, n=2048, d=64, kappa=16, JL 256 rows, base 2^8 x4 limbs",
+            "round_ms_p50": _pct(times, 50), "round_ms_p99": _pct(times, 99),
+            "round_with_jl_extraction_ms_p50": _pct(times_x, 50),
+            "e2e_round_ms_p50": _pct(e2e, 50), "e2e_round_ms_p99": _pct(e2e, 99),
+            "e2e_h2d_bytes": hw.numel() * 4, "e2e_d2h_bytes": d2h, "rounds": reps}
+
+
+def measure_batch(dev, reps=10):
+    """Uneven batched commits: 4096 instances, n log-uniform in [64, 8192],
+    rank m uniform in {8, 16, 32}, d = 64, ternary witnesses; one m x 8192
+    matrix per rank shared by its instances (instance uses the first n
+    columns). Batched (one CUDA-graph replay) vs one commit call per instance."""
+    import torch
+    from lattica_b200 import TwistedNttPlan
+    from lattica_b200.batch import UnevenCommitBatch, per_call_commit, sample_uneven_instances
+    from lattica_b200.commit import PreparedMatrix
+    q, d, ranks = Q64, 64, (8, 16, 32)
+    plan = TwistedNttPlan(q, d)
+    g = torch.Generator(device=dev).manual_seed(3)
+    mats = []
+    for m in ranks:
+        A = torch.randint(0, q, (m, 8192, d), dtype=torch.int64, device=dev, generator=g).to(torch.int32)
+        mats.append(PreparedMatrix(plan, A, m, 8192))
+        del A
+    items, s_polys, t_polys = sample_uneven_instances(4096, 7)
+    r1 = (1 << 32) % q
+    tern = torch.randint(-1, 2, (s_polys, d), dtype=torch.int64, device=dev, generator=g) % q
+    s = ((tern * r1) % q).to(torch.int32)
+    del tern
+    t = torch.zeros((t_polys, d), dtype=torch.int32, device=dev)
+    batch = UnevenCommitBatch(plan, mats, items)
+    tune = batch.autotune(s, t)
+    side = torch.cuda.Stream(dev)
+    with torch.cuda.stream(side):
+        batch.commit_dev(s, t, graph=True, stream=side)
+        side.synchronize()
+        tb = _events_ms(lambda: batch.commit_dev(s, t, graph=True, stream=side), reps, side)
+    t2 = torch.zeros_like(t)
+    per_call_commit(plan, mats, items, s, t2)
+    stream = torch.cuda.current_stream(dev)
+    tp = _events_ms(lambda: per_call_commit(plan, mats, items, s, t2), 3, stream)
+    same = bool(torch.equal(t, t2))
+    n = len(items)
+    macs = sum(ranks[m] * nn for _, _, nn, m in items) * d
+    return {"workload": "uneven batched commits: 4096 instances, n log-uniform [64, 8192], "
+                        "m in {8,16,32}, d=64",
+            "batched_commits_per_s": n / (statistics.median(tb) / 1e3),
+            "batched_ms_p50": statistics.median(tb),
+            "per_call_commits_per_s": n / (statistics.median(tp) / 1e3),
+            "per_call_ms_p50": statistics.median(tp),
+            "speedup_vs_per_call": statistics.median(tp) / statistics.median(tb),
+            "outputs_identical": same, "mod_macs": macs,
+            "autotune": {k: v for k, v in tune.items() if k in ("k_split", "cached", "ms")},
+            "schedule": batch.config()}
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -286,6 +459,9 @@ def run_ours(args, rank, world, local_rank):
         "gpu_launches": args.steps,
         "clocks": sampler.summary(),
     }
+    if args.secondary:
+        line["secondary"] = {"commit": measure_commit_plain(dev), "round": measure_round(dev),
+                             "batch": measure_batch(dev)}
     if world == 1:
         line["cpu_baseline"] = cpu_baseline(q, d, WORKLOADS[args.workload][2])
     print(json.dumps(line), flush=True)
@@ -298,6 +474,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="ntt64")
+    ap.add_argument("--no-secondary", dest="secondary", action="store_false",
+                    help="skip the plain-commit and prover-round measurements")
     ap.add_argument("--polys", type=int, default=0,
                     help="override the polynomial count (smaller cases for profiling)")
     args = ap.parse_args()

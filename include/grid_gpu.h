@@ -143,6 +143,9 @@ int grid_gpu_matrix_create(grid_gpu_plan* plan, const uint32_t* A, size_t rows, 
 int grid_gpu_matrix_create_dev(grid_gpu_plan* plan, const uint32_t* A, size_t rows, size_t cols,
                                int a_is_evals, grid_gpu_matrix** out, void* stream);
 int grid_gpu_matrix_destroy(grid_gpu_matrix* m);
+/* A view of the first `cols` columns of a prepared matrix (shares its device
+ * evaluations; destroy the view before the parent). */
+int grid_gpu_matrix_view(const grid_gpu_matrix* parent, size_t cols, grid_gpu_matrix** out);
 int grid_gpu_matrix_shape(const grid_gpu_matrix* m, size_t* rows, size_t* cols);
 int grid_gpu_matrix_device_evals(const grid_gpu_matrix* m, const uint32_t** evals);
 
@@ -201,6 +204,39 @@ int grid_gpu_gadget_decompose_dev(const grid_gpu_plan* plan, const uint32_t* x, 
                                   uint64_t base, int digit_major, uint32_t* out, void* stream);
 int grid_gpu_gadget_decompose(grid_gpu_plan* plan, const uint32_t* x, size_t len, uint64_t base,
                               int digit_major, uint32_t* out);
+
+/* ---- uneven batched commitments: many AjtaiCommitmentScheme::commit calls
+ *      (commit/src/ajtai/mod.rs:429-441) of different lengths in one launch
+ *      sequence (NTT of all witnesses, one persistent grouped matmul, INTT) --
+ * Instance i commits s_i (n polys starting at poly s_offset of the packed
+ * witness buffer) with the first n columns of matrix `matrix` (rows <= 32)
+ * and writes rows polys starting at poly t_offset of the packed output. */
+typedef struct grid_gpu_batch grid_gpu_batch;
+typedef struct grid_gpu_batch_item {
+  uint64_t s_offset;
+  uint64_t t_offset;
+  uint32_t n;
+  uint32_t matrix;
+} grid_gpu_batch_item;
+typedef struct grid_gpu_batch_config {
+  uint32_t k_split;     /* K range of one work item (multiple of 16); set by the autotuner */
+  uint32_t work_items;  /* output of get_config */
+  uint32_t tiles;       /* output of get_config */
+} grid_gpu_batch_config;
+int grid_gpu_batch_create(grid_gpu_plan* plan, grid_gpu_matrix* const* mats, size_t nmats,
+                          const grid_gpu_batch_item* items, size_t nitems, grid_gpu_batch** out);
+int grid_gpu_batch_destroy(grid_gpu_batch* batch);
+int grid_gpu_batch_set_config(grid_gpu_batch* batch, const grid_gpu_batch_config* cfg);
+int grid_gpu_batch_get_config(const grid_gpu_batch* batch, grid_gpu_batch_config* cfg);
+/* Polys the packed witness / output buffers must hold. */
+int grid_gpu_batch_shape(const grid_gpu_batch* batch, uint64_t* s_polys, uint64_t* t_polys);
+int grid_gpu_batch_workspace(const grid_gpu_batch* batch, size_t* bytes);
+int grid_gpu_batch_commit_dev(grid_gpu_batch* batch, const uint32_t* s, uint32_t* t,
+                              void* workspace, size_t workspace_bytes, void* stream);
+/* Same work, captured once per (s, t, workspace, stream) into a CUDA graph and
+ * replayed; `stream` must be a non-default stream. */
+int grid_gpu_batch_commit_graph(grid_gpu_batch* batch, const uint32_t* s, uint32_t* t,
+                                void* workspace, size_t workspace_bytes, void* stream);
 
 /* ---- Gram matrix without allocation (no counterpart in the reference) ----
  * Same result as grid_gpu_gram_dev, for callers that cannot allocate device

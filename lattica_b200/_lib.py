@@ -24,6 +24,15 @@ _u32p = C.POINTER(C.c_uint32)
 _vp = C.c_void_p
 
 
+class BatchItem(C.Structure):
+    _fields_ = [("s_offset", C.c_uint64), ("t_offset", C.c_uint64), ("n", C.c_uint32),
+                ("matrix", C.c_uint32)]
+
+
+class BatchConfig(C.Structure):
+    _fields_ = [("k_split", C.c_uint32), ("work_items", C.c_uint32), ("tiles", C.c_uint32)]
+
+
 class PlanInfo(C.Structure):
     _fields_ = [("q", C.c_uint32), ("d", C.c_uint32), ("generator", C.c_uint32),
                 ("psi", C.c_uint32), ("omega", C.c_uint32), ("n_inv", C.c_uint32),
@@ -54,6 +63,7 @@ SIGNATURES = {
     "grid_gpu_matrix_create_dev": (C.c_int, [_vp, _vp, C.c_size_t, C.c_size_t, C.c_int,
                                              C.POINTER(_vp), _vp]),
     "grid_gpu_matrix_destroy": (C.c_int, [_vp]),
+    "grid_gpu_matrix_view": (C.c_int, [_vp, C.c_size_t, C.POINTER(_vp)]),
     "grid_gpu_matrix_shape": (C.c_int, [_vp, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
     "grid_gpu_matrix_device_evals": (C.c_int, [_vp, C.POINTER(_vp)]),
     "grid_gpu_commit_workspace": (C.c_int, [_vp, C.c_size_t, C.POINTER(C.c_size_t)]),
@@ -80,6 +90,14 @@ SIGNATURES = {
     "grid_gpu_prover_round_dev": (C.c_int, [_vp, _vp, C.c_size_t, C.c_uint64, C.c_size_t,
                                             C.c_uint64, C.c_size_t, _vp, C.c_size_t, _vp, _vp,
                                             _vp, _vp, _vp, _vp, C.c_size_t, _vp]),
+    "grid_gpu_batch_create": (C.c_int, [_vp, _vp, C.c_size_t, _vp, C.c_size_t, C.POINTER(_vp)]),
+    "grid_gpu_batch_destroy": (C.c_int, [_vp]),
+    "grid_gpu_batch_set_config": (C.c_int, [_vp, _vp]),
+    "grid_gpu_batch_get_config": (C.c_int, [_vp, _vp]),
+    "grid_gpu_batch_shape": (C.c_int, [_vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    "grid_gpu_batch_workspace": (C.c_int, [_vp, C.POINTER(C.c_size_t)]),
+    "grid_gpu_batch_commit_dev": (C.c_int, [_vp, _vp, _vp, _vp, C.c_size_t, _vp]),
+    "grid_gpu_batch_commit_graph": (C.c_int, [_vp, _vp, _vp, _vp, C.c_size_t, _vp]),
     "grid_gpu_noalloc_scratch_bytes": (C.c_size_t, []),
     "grid_gpu_gram_noalloc_dev": (C.c_int, [_vp, _vp, C.c_size_t, C.c_size_t, _vp, _vp]),
     "grid_gpu_host_register": (C.c_int, [_vp, C.c_size_t]),

@@ -1,0 +1,387 @@
+// Uneven batched commitments in one persistent, graph-capturable launch.
+//
+// Many Ajtai commitments t_i = A_{m_i}[:, :n_i] * s_i with different witness
+// lengths n_i and different public matrices (each instance uses the first n_i
+// columns of its matrix, e.g. one matrix per rank m) run as one sequence:
+//   1. one NTT of every witness polynomial (packed s buffer -> s_hat),
+//   2. a persistent grouped evaluation-domain matmul: instances are grouped by
+//      matrix and sorted by length into tiles of 32; a work item is (tile,
+//      8 evaluation points, K range); CTAs pull work items from an atomic
+//      counter and add canonical partial sums into 64-bit accumulators,
+//   3. a fold of the accumulators mod q and one INTT of every output.
+// The reference runs each commitment separately (AjtaiCommitmentScheme::commit,
+// commit/src/ajtai/mod.rs:429-441, through PreparedLinearOps,
+// commit/src/linear.rs:717-770); the results are the same words.
+//
+// The K range per work item (k_split) is the tunable schedule parameter; the
+// host autotuner (lattica_b200/batch.py) times candidates and stores the best.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <new>
+#include <tuple>
+#include <vector>
+
+#include "grid_field.cuh"
+#include "grid_internal.h"
+
+namespace grid {
+namespace {
+
+constexpr int TM = 32, TN = 32, EG = 8, KC = 16, PAD = 4;
+constexpr int ROW = TM + PAD;
+constexpr int kThreads = 256;
+
+struct MatDev {
+  const uint32_t* evals;
+  uint32_t rows, ld;  // ld: row stride in polys
+};
+struct ItemDev {
+  unsigned long long s_off, t_off;
+  uint32_t n, pad;
+};
+struct TileDev {
+  uint32_t first, count, matrix, kmax;
+};
+struct WorkDev {
+  uint32_t tile, k0, k1, eg;
+};
+
+__global__ void __launch_bounds__(kThreads) batch_emm_kernel(
+    const WorkDev* __restrict__ work, unsigned nwork, const TileDev* __restrict__ tiles,
+    const ItemDev* __restrict__ items, const MatDev* __restrict__ mats,
+    const uint32_t* __restrict__ s_hat, unsigned long long* __restrict__ acc,
+    unsigned* __restrict__ counter, int d, FieldParams f) {
+  __shared__ __align__(16) uint32_t Xs[KC * EG * ROW];
+  __shared__ __align__(16) uint32_t Ys[KC * EG * ROW];
+  __shared__ ItemDev sitems[TM];
+  __shared__ unsigned widx;
+  const int t = threadIdx.x;
+  const int eg = t & 7, tn = (t >> 3) & 3, tm = t >> 5;
+
+  for (;;) {
+    if (t == 0) widx = atomicAdd(counter, 1u);
+    __syncthreads();
+    const unsigned w = widx;
+    if (w >= nwork) break;
+    const WorkDev wk = work[w];
+    const TileDev tile = tiles[wk.tile];
+    const MatDev mat = mats[tile.matrix];
+    if (t < TM) {
+      ItemDev it = {0, 0, 0, 0};
+      if ((uint32_t)t < tile.count) it = items[tile.first + t];
+      sitems[t] = it;
+    }
+    __syncthreads();
+    const int e0 = wk.eg * EG;
+
+    Acc96 a[4][8];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) acc96_zero(a[i][j]);
+
+    for (uint32_t k0 = wk.k0; k0 < wk.k1; k0 += KC) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int u = t + kThreads * i;  // (mm, kk, half)
+        const int half = u & 1;
+        const int kk = (u >> 1) & (KC - 1);
+        const int mm = u >> 5;
+        const uint32_t k = k0 + kk;
+        uint4 vx = make_uint4(0, 0, 0, 0), vy = make_uint4(0, 0, 0, 0);
+        if (k < wk.k1) {
+          const ItemDev& it = sitems[mm];
+          if (k < it.n)
+            vx = *reinterpret_cast<const uint4*>(s_hat + (it.s_off + k) * d + e0 + half * 4);
+          if ((uint32_t)mm < mat.rows)
+            vy = *reinterpret_cast<const uint4*>(mat.evals + ((size_t)mm * mat.ld + k) * d + e0 +
+                                                 half * 4);
+        }
+        uint32_t* xs = Xs + (kk * EG + half * 4) * ROW + mm;
+        uint32_t* ys = Ys + (kk * EG + half * 4) * ROW + mm;
+        xs[0] = vx.x; xs[ROW] = vx.y; xs[2 * ROW] = vx.z; xs[3 * ROW] = vx.w;
+        ys[0] = vy.x; ys[ROW] = vy.y; ys[2 * ROW] = vy.z; ys[3 * ROW] = vy.w;
+      }
+      __syncthreads();
+#pragma unroll 4
+      for (int kk = 0; kk < KC; ++kk) {
+        const uint4 xv = *reinterpret_cast<const uint4*>(Xs + (kk * EG + eg) * ROW + tm * 4);
+        const uint4 y0 = *reinterpret_cast<const uint4*>(Ys + (kk * EG + eg) * ROW + tn * 8);
+        const uint4 y1 = *reinterpret_cast<const uint4*>(Ys + (kk * EG + eg) * ROW + tn * 8 + 4);
+        const uint32_t xr[4] = {xv.x, xv.y, xv.z, xv.w};
+        const uint32_t yr[8] = {y0.x, y0.y, y0.z, y0.w, y1.x, y1.y, y1.z, y1.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 8; ++j) acc96_mad(a[i][j], xr[i], yr[j]);
+      }
+      __syncthreads();
+    }
+    const int e = e0 + eg;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int m = tm * 4 + i;
+      if ((uint32_t)m >= tile.count) continue;
+      const unsigned long long t_off = sitems[m].t_off;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int row = tn * 8 + j;
+        if ((uint32_t)row >= mat.rows) continue;
+        atomicAdd(&acc[(t_off + row) * d + e], (unsigned long long)acc96_reduce(a[i][j], f));
+      }
+    }
+    __syncthreads();  // sitems / widx are rewritten by the next work item
+  }
+}
+
+__global__ void fold_kernel(const unsigned long long* __restrict__ acc, uint32_t* __restrict__ out,
+                            size_t n, uint32_t q) {
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+    out[i] = (uint32_t)(acc[i] % q);
+}
+
+size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+}  // namespace
+}  // namespace grid
+
+using namespace grid;
+
+struct grid_gpu_batch {
+  grid_gpu_plan* plan = nullptr;
+  std::vector<MatDev> mats;
+  std::vector<ItemDev> sorted;    // items grouped by matrix, longest first
+  std::vector<TileDev> tiles;
+  uint64_t s_polys = 0, t_polys = 0;
+  uint32_t k_split = 1024;
+  // device tables
+  MatDev* d_mats = nullptr;
+  ItemDev* d_items = nullptr;
+  TileDev* d_tiles = nullptr;
+  WorkDev* d_work = nullptr;
+  unsigned nwork = 0;
+  // captured graphs, keyed by (s, t, workspace, stream)
+  std::mutex mu;
+  std::map<std::tuple<const void*, void*, void*, void*>, cudaGraphExec_t> graphs;
+  int num_sms = 0;
+};
+
+namespace {
+
+int rebuild_work(grid_gpu_batch* b) {
+  std::vector<WorkDev> work;
+  const uint32_t groups = b->plan->d / EG;
+  for (uint32_t ti = 0; ti < b->tiles.size(); ++ti) {
+    const TileDev& tl = b->tiles[ti];
+    for (uint32_t k0 = 0; k0 < tl.kmax; k0 += b->k_split) {
+      const uint32_t k1 = std::min(tl.kmax, k0 + b->k_split);
+      for (uint32_t g = 0; g < groups; ++g) work.push_back(WorkDev{ti, k0, k1, g});
+    }
+  }
+  // Longest K ranges first (all tiles carry 32 rows of work per K step).
+  std::stable_sort(work.begin(), work.end(), [](const WorkDev& x, const WorkDev& y) {
+    return (x.k1 - x.k0) > (y.k1 - y.k0);
+  });
+  if (b->d_work) cudaFree(b->d_work);
+  b->d_work = nullptr;
+  b->nwork = (unsigned)work.size();
+  if (work.empty()) return GRID_OK;
+  cudaError_t e = cudaMalloc(&b->d_work, work.size() * sizeof(WorkDev));
+  if (e == cudaSuccess)
+    e = cudaMemcpy(b->d_work, work.data(), work.size() * sizeof(WorkDev), cudaMemcpyHostToDevice);
+  for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
+  b->graphs.clear();
+  return cuda_status(e);
+}
+
+size_t ws_bytes(const grid_gpu_batch* b) {
+  const size_t d = b->plan->d;
+  return round_up(b->s_polys * d * 4, 256) + round_up(b->t_polys * d * 8, 256) + 256;
+}
+
+int run_sequence(grid_gpu_batch* b, const uint32_t* s, uint32_t* t, void* ws, cudaStream_t st) {
+  const grid_gpu_plan* p = b->plan;
+  const size_t d = p->d;
+  char* base = static_cast<char*>(ws);
+  uint32_t* s_hat = reinterpret_cast<uint32_t*>(base);
+  unsigned long long* acc =
+      reinterpret_cast<unsigned long long*>(base + round_up(b->s_polys * d * 4, 256));
+  unsigned* counter = reinterpret_cast<unsigned*>(base + round_up(b->s_polys * d * 4, 256) +
+                                                  round_up(b->t_polys * d * 8, 256));
+  int rc = launch_ntt(p, MODE_FWD, s, nullptr, s_hat, b->s_polys, st);
+  if (rc) return rc;
+  cudaError_t e = cudaMemsetAsync(acc, 0, b->t_polys * d * 8, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(counter, 0, sizeof(unsigned), st);
+  if (e != cudaSuccess) return cuda_status(e);
+  if (b->nwork) {
+    int bps = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, batch_emm_kernel, kThreads, 0);
+    if (bps < 1) bps = 1;
+    const unsigned grid = std::min<unsigned>(b->nwork, (unsigned)(p->num_sms * bps));
+    batch_emm_kernel<<<grid, kThreads, 0, st>>>(b->d_work, b->nwork, b->d_tiles, b->d_items,
+                                                 b->d_mats, s_hat, acc, counter, (int)d, p->f);
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(e);
+  }
+  const size_t words = b->t_polys * d;
+  unsigned blocks = (unsigned)std::min<size_t>((words + 255) / 256, (size_t)p->num_sms * 8);
+  fold_kernel<<<blocks ? blocks : 1, 256, 0, st>>>(acc, t, words, p->f.q);
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(e);
+  return launch_ntt(p, MODE_INV, t, nullptr, t, b->t_polys, st);
+}
+
+}  // namespace
+
+extern "C" {
+
+int grid_gpu_batch_create(grid_gpu_plan* plan, grid_gpu_matrix* const* mats, size_t nmats,
+                          const grid_gpu_batch_item* items, size_t nitems, grid_gpu_batch** out) {
+  if (!plan || !out || (!mats && nmats) || (!items && nitems)) return GRID_ERR_NULL_POINTER;
+  *out = nullptr;
+  if (nmats == 0 || nitems == 0 || nitems > (1u << 30)) return GRID_ERR_INVALID_PARAMETERS;
+  for (size_t i = 0; i < nmats; ++i) {
+    if (!mats[i]) return GRID_ERR_NULL_POINTER;
+    if (mats[i]->plan != plan) return GRID_ERR_INVALID_PARAMETERS;
+    if (mats[i]->rows > (size_t)TN) return GRID_ERR_INVALID_PARAMETERS;  // ranks up to 32
+  }
+  grid_gpu_batch* b = new (std::nothrow) grid_gpu_batch();
+  if (!b) return GRID_ERR_OUT_OF_MEMORY;
+  b->plan = plan;
+  b->num_sms = plan->num_sms;
+  for (size_t i = 0; i < nmats; ++i)
+    b->mats.push_back(MatDev{mats[i]->d_evals, (uint32_t)mats[i]->rows, (uint32_t)mats[i]->ld});
+  std::vector<std::pair<uint32_t, uint32_t>> order;  // (matrix, index)
+  for (size_t i = 0; i < nitems; ++i) {
+    const grid_gpu_batch_item& it = items[i];
+    if (it.matrix >= nmats || it.n == 0 || it.n > mats[it.matrix]->cols) {
+      delete b;
+      return GRID_ERR_DIMENSION_MISMATCH;
+    }
+    b->s_polys = std::max<uint64_t>(b->s_polys, it.s_offset + it.n);
+    b->t_polys = std::max<uint64_t>(b->t_polys, it.t_offset + mats[it.matrix]->rows);
+    order.emplace_back(it.matrix, (uint32_t)i);
+  }
+  std::stable_sort(order.begin(), order.end(), [&](const auto& x, const auto& y) {
+    if (x.first != y.first) return x.first < y.first;
+    return items[x.second].n > items[y.second].n;
+  });
+  for (size_t i = 0; i < order.size();) {
+    const uint32_t m = order[i].first;
+    size_t j = i;
+    TileDev tl{(uint32_t)b->sorted.size(), 0, m, 0};
+    while (j < order.size() && order[j].first == m && j - i < (size_t)TM) {
+      const grid_gpu_batch_item& it = items[order[j].second];
+      b->sorted.push_back(ItemDev{it.s_offset, it.t_offset, it.n, 0});
+      tl.kmax = std::max(tl.kmax, it.n);
+      ++j;
+    }
+    tl.count = (uint32_t)(j - i);
+    b->tiles.push_back(tl);
+    i = j;
+  }
+  cudaError_t e = cudaMalloc(&b->d_mats, b->mats.size() * sizeof(MatDev));
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_items, b->sorted.size() * sizeof(ItemDev));
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_tiles, b->tiles.size() * sizeof(TileDev));
+  if (e == cudaSuccess)
+    e = cudaMemcpy(b->d_mats, b->mats.data(), b->mats.size() * sizeof(MatDev),
+                   cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(b->d_items, b->sorted.data(), b->sorted.size() * sizeof(ItemDev),
+                   cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(b->d_tiles, b->tiles.data(), b->tiles.size() * sizeof(TileDev),
+                   cudaMemcpyHostToDevice);
+  int rc = cuda_status(e);
+  if (!rc) rc = rebuild_work(b);
+  if (rc) {
+    grid_gpu_batch_destroy(b);
+    return rc;
+  }
+  *out = b;
+  return GRID_OK;
+}
+
+int grid_gpu_batch_destroy(grid_gpu_batch* b) {
+  if (!b) return GRID_ERR_NULL_POINTER;
+  for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
+  if (b->d_mats) cudaFree(b->d_mats);
+  if (b->d_items) cudaFree(b->d_items);
+  if (b->d_tiles) cudaFree(b->d_tiles);
+  if (b->d_work) cudaFree(b->d_work);
+  delete b;
+  return GRID_OK;
+}
+
+int grid_gpu_batch_set_config(grid_gpu_batch* b, const grid_gpu_batch_config* cfg) {
+  if (!b || !cfg) return GRID_ERR_NULL_POINTER;
+  if (cfg->k_split < KC || cfg->k_split % KC) return GRID_ERR_INVALID_PARAMETERS;
+  std::lock_guard<std::mutex> lk(b->mu);
+  b->k_split = cfg->k_split;
+  return rebuild_work(b);
+}
+
+int grid_gpu_batch_get_config(const grid_gpu_batch* b, grid_gpu_batch_config* cfg) {
+  if (!b || !cfg) return GRID_ERR_NULL_POINTER;
+  cfg->k_split = b->k_split;
+  cfg->work_items = b->nwork;
+  cfg->tiles = (uint32_t)b->tiles.size();
+  return GRID_OK;
+}
+
+int grid_gpu_batch_shape(const grid_gpu_batch* b, uint64_t* s_polys, uint64_t* t_polys) {
+  if (!b || !s_polys || !t_polys) return GRID_ERR_NULL_POINTER;
+  *s_polys = b->s_polys;
+  *t_polys = b->t_polys;
+  return GRID_OK;
+}
+
+int grid_gpu_batch_workspace(const grid_gpu_batch* b, size_t* bytes) {
+  if (!b || !bytes) return GRID_ERR_NULL_POINTER;
+  *bytes = ws_bytes(b);
+  return GRID_OK;
+}
+
+int grid_gpu_batch_commit_dev(grid_gpu_batch* b, const uint32_t* s, uint32_t* t, void* workspace,
+                              size_t workspace_bytes, void* stream) {
+  if (!b || !s || !t || !workspace) return GRID_ERR_NULL_POINTER;
+  if (workspace_bytes < ws_bytes(b)) return GRID_ERR_INVALID_PARAMETERS;
+  if (((uintptr_t)s | (uintptr_t)t | (uintptr_t)workspace) & 15u) return GRID_ERR_MISALIGNED;
+  std::lock_guard<std::mutex> lk(b->mu);
+  return run_sequence(b, s, t, workspace, (cudaStream_t)stream);
+}
+
+int grid_gpu_batch_commit_graph(grid_gpu_batch* b, const uint32_t* s, uint32_t* t,
+                                void* workspace, size_t workspace_bytes, void* stream) {
+  if (!b || !s || !t || !workspace) return GRID_ERR_NULL_POINTER;
+  if (workspace_bytes < ws_bytes(b)) return GRID_ERR_INVALID_PARAMETERS;
+  if (((uintptr_t)s | (uintptr_t)t | (uintptr_t)workspace) & 15u) return GRID_ERR_MISALIGNED;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (!st) return GRID_ERR_INVALID_PARAMETERS;  // capture needs a non-default stream
+  std::lock_guard<std::mutex> lk(b->mu);
+  const auto key = std::make_tuple((const void*)s, (void*)t, workspace, (void*)st);
+  auto it = b->graphs.find(key);
+  if (it == b->graphs.end()) {
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return cuda_status(e);
+    const int rc = run_sequence(b, s, t, workspace, st);
+    e = cudaStreamEndCapture(st, &g);
+    if (rc) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (e != cudaSuccess) return cuda_status(e);
+    cudaGraphExec_t exec = nullptr;
+    e = cudaGraphInstantiate(&exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_status(e);
+    it = b->graphs.emplace(key, exec).first;
+  }
+  return cuda_status(cudaGraphLaunch(it->second, st));
+}
+
+}  // extern "C"

@@ -62,8 +62,8 @@ int commit_core(const grid_gpu_matrix* A, const uint32_t* s, size_t batch, uint3
   if (!cv.ok) return GRID_ERR_INVALID_PARAMETERS;
   int rc = launch_ntt(p, MODE_FWD, s, nullptr, s_hat, batch * A->cols, st);
   if (rc) return rc;
-  rc = launch_emm(p, s_hat, A->d_evals, (int)batch, (int)A->rows, (int)A->cols, EMM_DENSE, t,
-                  work, st);
+  rc = launch_emm(p, s_hat, A->d_evals, (int)batch, (int)A->rows, (int)A->cols, (int)A->ld,
+                  EMM_DENSE, t, work, st);
   if (rc) return rc;
   return launch_ntt(p, MODE_INV, t, nullptr, t, batch * A->rows, st);
 }
@@ -85,6 +85,7 @@ int grid_gpu_matrix_create_dev(grid_gpu_plan* p, const uint32_t* A, size_t rows,
   m->plan = p;
   m->rows = rows;
   m->cols = cols;
+  m->ld = cols;
   cudaStream_t st = (cudaStream_t)stream;
   cudaError_t e = cudaMalloc(&m->d_evals, rows * cols * p->d * 4);
   if (e != cudaSuccess) {
@@ -131,8 +132,24 @@ int grid_gpu_matrix_create(grid_gpu_plan* p, const uint32_t* A, size_t rows, siz
 
 int grid_gpu_matrix_destroy(grid_gpu_matrix* m) {
   if (!m) return GRID_ERR_NULL_POINTER;
-  if (m->d_evals) cudaFree(m->d_evals);
+  if (m->owned && m->d_evals) cudaFree(m->d_evals);
   delete m;
+  return GRID_OK;
+}
+
+int grid_gpu_matrix_view(const grid_gpu_matrix* parent, size_t cols, grid_gpu_matrix** out) {
+  if (!parent || !out) return GRID_ERR_NULL_POINTER;
+  *out = nullptr;
+  if (cols == 0 || cols > parent->cols) return GRID_ERR_DIMENSION_MISMATCH;
+  grid_gpu_matrix* m = new (std::nothrow) grid_gpu_matrix();
+  if (!m) return GRID_ERR_OUT_OF_MEMORY;
+  m->plan = parent->plan;
+  m->rows = parent->rows;
+  m->cols = cols;
+  m->ld = parent->ld;
+  m->d_evals = parent->d_evals;
+  m->owned = false;
+  *out = m;
   return GRID_OK;
 }
 
@@ -250,7 +267,7 @@ int grid_gpu_gram_dev(const grid_gpu_plan* p, const uint32_t* S, size_t r, size_
   if (!cv.ok) return GRID_ERR_INVALID_PARAMETERS;
   int rc = launch_ntt(p, MODE_FWD, S, nullptr, s_hat, r * n, st);
   if (rc) return rc;
-  rc = launch_emm(p, s_hat, s_hat, (int)r, (int)r, (int)n, EMM_UPPER, G, work, st);
+  rc = launch_emm(p, s_hat, s_hat, (int)r, (int)r, (int)n, (int)n, EMM_UPPER, G, work, st);
   if (rc) return rc;
   return launch_ntt(p, MODE_INV, G, nullptr, G, r * (r + 1) / 2, st);
 }
@@ -429,11 +446,13 @@ int grid_gpu_prover_round_dev(const grid_gpu_matrix* A, const uint32_t* S, size_
   // Witness to the evaluation domain once; shared by the commitment and the Gram.
   int rc = launch_ntt(p, MODE_FWD, S, nullptr, s_hat, r * n, st);
   // 1. inner commitments t_i = A s_i, then balanced limbs (inner_commit_decomposed)
-  if (!rc) rc = launch_emm(p, s_hat, A->d_evals, (int)r, (int)kappa, (int)n, EMM_DENSE, t, work, st);
+  if (!rc)
+    rc = launch_emm(p, s_hat, A->d_evals, (int)r, (int)kappa, (int)n, (int)A->ld, EMM_DENSE, t,
+                    work, st);
   if (!rc) rc = launch_ntt(p, MODE_INV, t, nullptr, t, r * kappa, st);
   if (!rc) rc = launch_decompose_balanced(p, t, r * kappa, b1, t1, t_limbs, st);
   // 2. garbage g_ij = <s_i, s_j>, i <= j, then balanced limbs
-  if (!rc) rc = launch_emm(p, s_hat, s_hat, (int)r, (int)r, (int)n, EMM_UPPER, g, work, st);
+  if (!rc) rc = launch_emm(p, s_hat, s_hat, (int)r, (int)r, (int)n, (int)n, EMM_UPPER, g, work, st);
   if (!rc) rc = launch_ntt(p, MODE_INV, g, nullptr, g, r * (r + 1) / 2, st);
   if (!rc && g_limbs) rc = launch_decompose_balanced(p, g, r * (r + 1) / 2, b2, t2, g_limbs, st);
   // 3. JL projection of the coefficient vectors (one part per witness vector)

@@ -17,8 +17,8 @@
 // Kernel "emm": a CTA owns 8 consecutive evaluation points (one 32-byte
 // sector per (row, k)), a 32 x 32 output tile and a K range; operands are
 // staged through shared memory in 16-deep K chunks; each thread keeps a 4 x 8
-// register tile of exact 96-bit accumulators (mad.lo.cc / madc.hi.cc / addc:
-// three integer instructions per modular MAC) and reduces once at the end.
+// register tile of exact 96-bit accumulators (64-bit product added to a 64-bit
+// sum, carries counted in a third word) and reduces once at the end.
 // Partial sums of a K split are canonical residues, so splits add exactly.
 #include <cuda_runtime.h>
 
@@ -35,12 +35,14 @@ constexpr int kEmmThreads = 256;
 
 enum OutMode : int { OUT_DENSE = 0, OUT_UPPER = 1 };
 
-// X: [M][K][d], Y: [N][K][d]. Dense output: [M][N][d]; upper output (X == Y,
-// M == N): packed upper triangle i <= j in row-major order (garbage_index).
+// X: [M][K][d], Y: [N][ldy][d] (first K of ldy columns used). Dense output:
+// [M][N][d]; upper output (X == Y, M == N): packed upper triangle i <= j in
+// row-major order (garbage_index).
 // With splits > 1 the CTA of split s writes to out + s * split_stride.
 __global__ void __launch_bounds__(kEmmThreads) emm_kernel(
     const uint32_t* __restrict__ X, const uint32_t* __restrict__ Y, uint32_t* __restrict__ out,
-    int M, int N, int K, int d, int mode, int k_per_split, size_t split_stride, FieldParams f) {
+    int M, int N, int K, int ldy, int d, int mode, int k_per_split, size_t split_stride,
+    FieldParams f) {
   __shared__ __align__(16) uint32_t Xs[KC * EG * ROWX];
   __shared__ __align__(16) uint32_t Ys[KC * EG * ROWY];
 
@@ -80,7 +82,7 @@ __global__ void __launch_bounds__(kEmmThreads) emm_kernel(
         if (m < M)
           vx = *reinterpret_cast<const uint4*>(X + ((size_t)m * K + k) * d + e0 + half * 4);
         if (n < N)
-          vy = *reinterpret_cast<const uint4*>(Y + ((size_t)n * K + k) * d + e0 + half * 4);
+          vy = *reinterpret_cast<const uint4*>(Y + ((size_t)n * ldy + k) * d + e0 + half * 4);
       }
       uint32_t* xs = Xs + (kk * EG + half * 4) * ROWX + mm;
       uint32_t* ys = Ys + (kk * EG + half * 4) * ROWY + mm;
@@ -154,7 +156,7 @@ size_t emm_workspace_words(const grid_gpu_plan* p, int M, int N, int K, int mode
 
 // out_evals: dense [M][N][d] or packed-upper [M(M+1)/2][d]. work: >= emm_workspace_words.
 int launch_emm(const grid_gpu_plan* p, const uint32_t* X, const uint32_t* Y, int M, int N, int K,
-               int mode, uint32_t* out_evals, uint32_t* work, cudaStream_t s) {
+               int ldy, int mode, uint32_t* out_evals, uint32_t* work, cudaStream_t s) {
   if (M <= 0 || N <= 0 || K <= 0) return GRID_OK;
   if (p->d % EG) return GRID_ERR_UNSUPPORTED_DEGREE;
   const int tiles_m = (M + BM - 1) / BM, tiles_n = (N + BN - 1) / BN;
@@ -167,7 +169,8 @@ int launch_emm(const grid_gpu_plan* p, const uint32_t* X, const uint32_t* Y, int
   dim3 grid(p->d / EG, tiles_m * tiles_n, splits);
   uint32_t* dst = splits > 1 ? work : out_evals;
   if (splits > 1 && !work) return GRID_ERR_NULL_POINTER;
-  emm_kernel<<<grid, kEmmThreads, 0, s>>>(X, Y, dst, M, N, K, (int)p->d, mode, kps, stride, p->f);
+  emm_kernel<<<grid, kEmmThreads, 0, s>>>(X, Y, dst, M, N, K, ldy, (int)p->d, mode, kps, stride,
+                                          p->f);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_status(e);
   if (splits > 1) {

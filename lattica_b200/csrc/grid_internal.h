@@ -69,7 +69,9 @@ struct grid_gpu_plan {
 struct grid_gpu_matrix {
   grid_gpu_plan* plan = nullptr;
   size_t rows = 0, cols = 0;
-  uint32_t* d_evals = nullptr;  // rows x cols polys in the twisted evaluation domain
+  size_t ld = 0;                // row stride in polys (cols of the owning matrix)
+  uint32_t* d_evals = nullptr;  // rows x ld polys in the twisted evaluation domain
+  bool owned = true;            // false for views sharing another matrix's evaluations
 };
 
 namespace grid {
@@ -83,7 +85,7 @@ int ntt_max_degree();
 enum EmmOut : int { EMM_DENSE = 0, EMM_UPPER = 1 };
 size_t emm_workspace_words(const grid_gpu_plan* p, int M, int N, int K, int mode);
 int launch_emm(const grid_gpu_plan* p, const uint32_t* X, const uint32_t* Y, int M, int N, int K,
-               int mode, uint32_t* out_evals, uint32_t* work, cudaStream_t s);
+               int ldy, int mode, uint32_t* out_evals, uint32_t* work, cudaStream_t s);
 int launch_pointwise(const grid_gpu_plan* p, uint32_t* dst, const uint32_t* rhs, size_t words,
                      cudaStream_t s);
 int launch_add(const grid_gpu_plan* p, uint32_t* dst, const uint32_t* rhs, size_t words,

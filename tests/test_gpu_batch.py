@@ -1,0 +1,91 @@
+"""Uneven batched commitments: the one-sequence batched path (plain and CUDA
+graph), the per-call path and the oracle agree word for word; the autotuner
+persists its choice."""
+import json
+
+import numpy as np
+import pytest
+
+Q = 4294966657
+
+pytestmark = pytest.mark.gpu
+
+
+def _setup(cuda, oracle, ranks, n_hi, num, seed):
+    import torch
+    from lattica_b200 import TwistedNttPlan
+    from lattica_b200.batch import sample_uneven_instances
+    from lattica_b200.commit import PreparedMatrix
+    d = 64
+    plan = TwistedNttPlan(Q, d)
+    rng = np.random.default_rng(seed)
+    mats_host = [rng.integers(0, Q, (m, n_hi, d), dtype=np.uint64).astype(np.uint32) for m in ranks]
+    mats = [PreparedMatrix(plan, A, A.shape[0], n_hi) for A in mats_host]
+    items, s_polys, t_polys = sample_uneven_instances(num, seed, n_lo=1, n_hi=n_hi, ranks=ranks)
+    s_host = rng.integers(0, Q, (s_polys, d), dtype=np.uint64).astype(np.uint32)
+    s = torch.from_numpy(s_host.view(np.int32)).to(cuda)
+    return plan, mats, mats_host, items, s_host, s, t_polys
+
+
+def _oracle_expect(oracle, mats_host, items, s_host, t_polys):
+    P = oracle.Plan(Q, 64)
+    want = np.zeros((t_polys, 64), np.uint32)
+    for so, to, n, m in items:
+        A = np.ascontiguousarray(mats_host[m][:, :n, :])
+        rows = A.shape[0]
+        t = P.matvec(A, rows, n, s_host[so:so + n], 1).reshape(rows, 64)
+        want[to:to + rows] = t
+    return want
+
+
+def test_batched_uneven_commits_match_oracle_and_per_call(cuda, oracle, tmp_path):
+    import torch
+    from lattica_b200.batch import UnevenCommitBatch, per_call_commit
+    ranks = (3, 8, 32)
+    plan, mats, mats_host, items, s_host, s, t_polys = _setup(cuda, oracle, ranks, 300, 70, 4)
+    want = _oracle_expect(oracle, mats_host, items, s_host, t_polys)
+    batch = UnevenCommitBatch(plan, mats, items)
+    assert batch.s_polys == s_host.shape[0] and batch.t_polys == t_polys
+    t = torch.zeros((t_polys, 64), dtype=torch.int32, device=cuda)
+    for k_split in (16, 64, 256, 4096):
+        batch.set_k_split(k_split)
+        t.zero_()
+        batch.commit_dev(s, t)
+        torch.cuda.synchronize()
+        assert np.array_equal(t.cpu().numpy().view(np.uint32), want), k_split
+    # graph capture on a side stream, replayed twice
+    side = torch.cuda.Stream(cuda)
+    with torch.cuda.stream(side):
+        for _ in range(2):
+            t.zero_()
+            batch.commit_dev(s, t, graph=True, stream=side)
+    side.synchronize()
+    assert np.array_equal(t.cpu().numpy().view(np.uint32), want)
+    # per-call path
+    t2 = torch.zeros_like(t)
+    per_call_commit(plan, mats, items, s, t2)
+    assert torch.equal(t, t2)
+    # autotuner: picks a candidate, persists it, reuses it
+    cache = tmp_path / "autotune.json"
+    res = batch.autotune(s, t, candidates=(64, 256), reps=2, cache_path=str(cache))
+    assert res["k_split"] in (64, 256) and not res["cached"]
+    assert json.loads(cache.read_text())[batch.signature()]["k_split"] == res["k_split"]
+    res2 = batch.autotune(s, t, candidates=(64, 256), cache_path=str(cache))
+    assert res2["cached"] and res2["k_split"] == res["k_split"]
+    batch.commit_dev(s, t)
+    torch.cuda.synchronize()
+    assert np.array_equal(t.cpu().numpy().view(np.uint32), want)
+    plan.check_device()
+
+
+def test_batch_rejects_bad_items(cuda):
+    import ctypes as C
+    from lattica_b200 import CommitmentError, TwistedNttPlan
+    from lattica_b200.batch import UnevenCommitBatch
+    from lattica_b200.commit import PreparedMatrix
+    plan = TwistedNttPlan(Q, 64)
+    M = PreparedMatrix(plan, np.zeros((4, 10, 64), np.uint32), 4, 10)
+    with pytest.raises(CommitmentError):
+        UnevenCommitBatch(plan, [M], [(0, 0, 11, 0)])   # n beyond the matrix
+    with pytest.raises(CommitmentError):
+        UnevenCommitBatch(plan, [M], [(0, 0, 5, 1)])    # no such matrix
