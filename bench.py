@@ -346,6 +346,58 @@ def measure_batch(dev, reps=10):
             "schedule": batch.config()}
 
 
+def measure_serve(dev, rates=(1000, 2000, 5000, 10000, 20000, 50000), seconds=0.4):
+    """Served mixed stream, open-loop Poisson arrivals: 70% commits (n
+    log-uniform [64, 4096], m in {8, 16, 32}), 25% Gram + JL steps (r in
+    {8, 16, 32, 64}, n = 1024), 5% LaBRADOR rounds (r = 64, n = 2048,
+    kappa = 16); d = 64. Continuous batching over 4 streams vs the plain
+    per-call path (one request at a time), at each offered rate; latency from
+    scheduled arrival to the result on the host."""
+    import torch
+    from lattica_b200 import TwistedNttPlan
+    from lattica_b200.commit import PreparedMatrix
+    from lattica_b200.labrador import CommitKey
+    from lattica_b200.serve import RingServer, sample_requests, run_load
+    q, d = Q64, 64
+    plan = TwistedNttPlan(q, d)
+    g = torch.Generator(device=dev).manual_seed(9)
+    mats = {}
+    for m in (8, 16, 32):
+        A = torch.randint(0, q, (m, 4096, d), dtype=torch.int64, device=dev, generator=g)
+        mats[m] = PreparedMatrix(plan, A.to(torch.int32), m, 4096)
+        del A
+    A = torch.randint(0, q, (16, 2048, d), dtype=torch.int64, device=dev, generator=g)
+    key = CommitKey(plan, A.to(torch.int32), 16, 2048)
+    del A
+    arena, pool_polys = 1 << 18, 1 << 19
+    coeffs = torch.randint(-2048, 2049, (pool_polys, d), dtype=torch.int64, device=dev, generator=g)
+    pool = (((coeffs % q) * ((1 << 32) % q)) % q).to(torch.int32)
+    del coeffs
+    torch.cuda.synchronize()
+
+    def schedule(seed, count, rate):
+        out = sample_requests(seed, count, rate, commit_arena=arena, pool_polys=pool_polys)
+        for _, r in out:
+            r.keep = False
+        return out
+
+    out = {"workload": "served stream: 70% commits n~logU[64,4096] m in {8,16,32}; 25% Gram+JL "
+                       "r in {8,16,32,64} n=1024; 5% LaBRADOR rounds r=64 n=2048; d=64; "
+                       f"Poisson arrivals, {seconds} s of arrivals per rate",
+           "rates": {}}
+    for mode in ("continuous", "plain"):
+        with RingServer(plan, mats, key, pool, mode=mode) as srv:
+            run_load(srv, schedule(1, 300, 3000.0))           # warm-up
+            for lam in rates:
+                res = run_load(srv, schedule(100 + lam, max(200, int(lam * seconds)), float(lam)))
+                out["rates"].setdefault(str(lam), {})[mode] = res
+    best = {m: max(v[m]["commits_per_s"] for v in out["rates"].values())
+            for m in ("continuous", "plain")}
+    out["max_commits_per_s"] = best
+    out["commits_per_s_ratio"] = best["continuous"] / best["plain"]
+    return out
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -462,6 +514,8 @@ def run_ours(args, rank, world, local_rank):
     if args.secondary:
         line["secondary"] = {"commit": measure_commit_plain(dev), "round": measure_round(dev),
                              "batch": measure_batch(dev)}
+        if args.serve:
+            line["secondary"]["serve"] = measure_serve(dev)
     if world == 1:
         line["cpu_baseline"] = cpu_baseline(q, d, WORKLOADS[args.workload][2])
     print(json.dumps(line), flush=True)
@@ -476,6 +530,8 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="ntt64")
     ap.add_argument("--no-secondary", dest="secondary", action="store_false",
                     help="skip the plain-commit and prover-round measurements")
+    ap.add_argument("--no-serve", dest="serve", action="store_false",
+                    help="skip the served-stream measurement")
     ap.add_argument("--polys", type=int, default=0,
                     help="override the polynomial count (smaller cases for profiling)")
     args = ap.parse_args()

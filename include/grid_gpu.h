@@ -237,6 +237,18 @@ int grid_gpu_batch_commit_dev(grid_gpu_batch* batch, const uint32_t* s, uint32_t
  * replayed; `stream` must be a non-default stream. */
 int grid_gpu_batch_commit_graph(grid_gpu_batch* batch, const uint32_t* s, uint32_t* t,
                                 void* workspace, size_t workspace_bytes, void* stream);
+/* One-shot form for request loops: no handle and no device allocation; the
+ * work tables are built on the host and copied into the caller's workspace.
+ * k_split 0 lets the library pick the K range from the batch's size (about
+ * four work items per SM, at most 8192); both calls must get the same value. */
+int grid_gpu_batch_oneshot_workspace(grid_gpu_plan* plan, grid_gpu_matrix* const* mats,
+                                     size_t nmats, const grid_gpu_batch_item* items,
+                                     size_t nitems, uint32_t k_split, size_t* bytes);
+int grid_gpu_batch_commit_oneshot_dev(grid_gpu_plan* plan, grid_gpu_matrix* const* mats,
+                                      size_t nmats, const grid_gpu_batch_item* items,
+                                      size_t nitems, uint32_t k_split, const uint32_t* s,
+                                      uint32_t* t, void* workspace, size_t workspace_bytes,
+                                      void* stream);
 
 /* ---- Gram matrix without allocation (no counterpart in the reference) ----
  * Same result as grid_gpu_gram_dev, for callers that cannot allocate device

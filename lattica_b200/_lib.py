@@ -98,6 +98,10 @@ SIGNATURES = {
     "grid_gpu_batch_workspace": (C.c_int, [_vp, C.POINTER(C.c_size_t)]),
     "grid_gpu_batch_commit_dev": (C.c_int, [_vp, _vp, _vp, _vp, C.c_size_t, _vp]),
     "grid_gpu_batch_commit_graph": (C.c_int, [_vp, _vp, _vp, _vp, C.c_size_t, _vp]),
+    "grid_gpu_batch_oneshot_workspace": (C.c_int, [_vp, _vp, C.c_size_t, _vp, C.c_size_t,
+                                                   C.c_uint32, C.POINTER(C.c_size_t)]),
+    "grid_gpu_batch_commit_oneshot_dev": (C.c_int, [_vp, _vp, C.c_size_t, _vp, C.c_size_t,
+                                                    C.c_uint32, _vp, _vp, _vp, C.c_size_t, _vp]),
     "grid_gpu_noalloc_scratch_bytes": (C.c_size_t, []),
     "grid_gpu_gram_noalloc_dev": (C.c_int, [_vp, _vp, C.c_size_t, C.c_size_t, _vp, _vp]),
     "grid_gpu_host_register": (C.c_int, [_vp, C.c_size_t]),

@@ -173,29 +173,34 @@ struct grid_gpu_batch {
 
 namespace {
 
-int rebuild_work(grid_gpu_batch* b) {
+std::vector<WorkDev> make_work(const std::vector<TileDev>& tiles, uint32_t groups,
+                               uint32_t k_split) {
   std::vector<WorkDev> work;
-  const uint32_t groups = b->plan->d / EG;
-  for (uint32_t ti = 0; ti < b->tiles.size(); ++ti) {
-    const TileDev& tl = b->tiles[ti];
-    for (uint32_t k0 = 0; k0 < tl.kmax; k0 += b->k_split) {
-      const uint32_t k1 = std::min(tl.kmax, k0 + b->k_split);
+  for (uint32_t ti = 0; ti < tiles.size(); ++ti) {
+    const TileDev& tl = tiles[ti];
+    for (uint32_t k0 = 0; k0 < tl.kmax; k0 += k_split) {
+      const uint32_t k1 = std::min(tl.kmax, k0 + k_split);
       for (uint32_t g = 0; g < groups; ++g) work.push_back(WorkDev{ti, k0, k1, g});
     }
   }
-  // Longest K ranges first (all tiles carry 32 rows of work per K step).
+  // Longest K ranges first (every tile carries up to 32 x 32 outputs per K step).
   std::stable_sort(work.begin(), work.end(), [](const WorkDev& x, const WorkDev& y) {
     return (x.k1 - x.k0) > (y.k1 - y.k0);
   });
+  return work;
+}
+
+int rebuild_work(grid_gpu_batch* b) {
+  const std::vector<WorkDev> work = make_work(b->tiles, b->plan->d / EG, b->k_split);
   if (b->d_work) cudaFree(b->d_work);
   b->d_work = nullptr;
   b->nwork = (unsigned)work.size();
+  for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
+  b->graphs.clear();
   if (work.empty()) return GRID_OK;
   cudaError_t e = cudaMalloc(&b->d_work, work.size() * sizeof(WorkDev));
   if (e == cudaSuccess)
     e = cudaMemcpy(b->d_work, work.data(), work.size() * sizeof(WorkDev), cudaMemcpyHostToDevice);
-  for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
-  b->graphs.clear();
   return cuda_status(e);
 }
 
@@ -204,65 +209,93 @@ size_t ws_bytes(const grid_gpu_batch* b) {
   return round_up(b->s_polys * d * 4, 256) + round_up(b->t_polys * d * 8, 256) + 256;
 }
 
-int run_sequence(grid_gpu_batch* b, const uint32_t* s, uint32_t* t, void* ws, cudaStream_t st) {
-  const grid_gpu_plan* p = b->plan;
+// NTT(s) -> grouped matmul -> fold -> INTT(t), with device tables given.
+int run_core(const grid_gpu_plan* p, const MatDev* d_mats, const ItemDev* d_items,
+             const TileDev* d_tiles, const WorkDev* d_work, unsigned nwork, uint64_t s_polys,
+             uint64_t t_polys, const uint32_t* s, uint32_t* t, void* ws, cudaStream_t st) {
   const size_t d = p->d;
   char* base = static_cast<char*>(ws);
   uint32_t* s_hat = reinterpret_cast<uint32_t*>(base);
   unsigned long long* acc =
-      reinterpret_cast<unsigned long long*>(base + round_up(b->s_polys * d * 4, 256));
-  unsigned* counter = reinterpret_cast<unsigned*>(base + round_up(b->s_polys * d * 4, 256) +
-                                                  round_up(b->t_polys * d * 8, 256));
-  int rc = launch_ntt(p, MODE_FWD, s, nullptr, s_hat, b->s_polys, st);
+      reinterpret_cast<unsigned long long*>(base + round_up(s_polys * d * 4, 256));
+  unsigned* counter = reinterpret_cast<unsigned*>(base + round_up(s_polys * d * 4, 256) +
+                                                  round_up(t_polys * d * 8, 256));
+  int rc = launch_ntt(p, MODE_FWD, s, nullptr, s_hat, s_polys, st);
   if (rc) return rc;
-  cudaError_t e = cudaMemsetAsync(acc, 0, b->t_polys * d * 8, st);
+  cudaError_t e = cudaMemsetAsync(acc, 0, t_polys * d * 8, st);
   if (e == cudaSuccess) e = cudaMemsetAsync(counter, 0, sizeof(unsigned), st);
   if (e != cudaSuccess) return cuda_status(e);
-  if (b->nwork) {
+  if (nwork) {
+    static int bps_cache[kMaxDevices] = {};
     int bps = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, batch_emm_kernel, kThreads, 0);
-    if (bps < 1) bps = 1;
-    const unsigned grid = std::min<unsigned>(b->nwork, (unsigned)(p->num_sms * bps));
-    batch_emm_kernel<<<grid, kThreads, 0, st>>>(b->d_work, b->nwork, b->d_tiles, b->d_items,
-                                                 b->d_mats, s_hat, acc, counter, (int)d, p->f);
+    rc = prepare_kernel(batch_emm_kernel, 0, kThreads, p->device, bps_cache, &bps);
+    if (rc) return rc;
+    const unsigned grid = std::min<unsigned>(nwork, (unsigned)(p->num_sms * bps));
+    batch_emm_kernel<<<grid, kThreads, 0, st>>>(d_work, nwork, d_tiles, d_items, d_mats, s_hat,
+                                                 acc, counter, (int)d, p->f);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(e);
   }
-  const size_t words = b->t_polys * d;
+  const size_t words = t_polys * d;
   unsigned blocks = (unsigned)std::min<size_t>((words + 255) / 256, (size_t)p->num_sms * 8);
   fold_kernel<<<blocks ? blocks : 1, 256, 0, st>>>(acc, t, words, p->f.q);
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(e);
-  return launch_ntt(p, MODE_INV, t, nullptr, t, b->t_polys, st);
+  return launch_ntt(p, MODE_INV, t, nullptr, t, t_polys, st);
+}
+
+int run_sequence(grid_gpu_batch* b, const uint32_t* s, uint32_t* t, void* ws, cudaStream_t st) {
+  return run_core(b->plan, b->d_mats, b->d_items, b->d_tiles, b->d_work, b->nwork, b->s_polys,
+                  b->t_polys, s, t, ws, st);
 }
 
 }  // namespace
 
-extern "C" {
+namespace {
 
-int grid_gpu_batch_create(grid_gpu_plan* plan, grid_gpu_matrix* const* mats, size_t nmats,
-                          const grid_gpu_batch_item* items, size_t nitems, grid_gpu_batch** out) {
-  if (!plan || !out || (!mats && nmats) || (!items && nitems)) return GRID_ERR_NULL_POINTER;
-  *out = nullptr;
+struct Tables {
+  std::vector<MatDev> mats;
+  std::vector<ItemDev> sorted;
+  std::vector<TileDev> tiles;
+  std::vector<WorkDev> work;
+  uint64_t s_polys = 0, t_polys = 0;
+  uint32_t k_split = 0;
+};
+
+// K range per work item when the caller leaves it to the library: about four
+// work items per SM, so a small batch (a few instances, one tile) still
+// spreads over the whole GPU instead of running its K loop on a few CTAs;
+// large batches reach the 8192 cap, where fewer accumulator atomics win.
+uint32_t auto_k_split(const std::vector<TileDev>& tiles, uint32_t groups, int num_sms) {
+  uint64_t steps = 0;  // KC-wide K steps over every tile and evaluation group
+  for (const TileDev& tl : tiles) steps += (tl.kmax + KC - 1) / KC;
+  steps *= groups;
+  const uint64_t target = 4ull * (uint64_t)(num_sms > 0 ? num_sms : 148);
+  uint64_t per = (steps + target - 1) / target;
+  per = std::max<uint64_t>(1, std::min<uint64_t>(per, 8192 / KC));
+  return (uint32_t)(per * KC);
+}
+
+// Group items by matrix, longest first, into tiles of TM; then cut every tile
+// into (K range, evaluation group) work items, longest K ranges first.
+int build_tables(const grid_gpu_plan* plan, grid_gpu_matrix* const* mats, size_t nmats,
+                 const grid_gpu_batch_item* items, size_t nitems, uint32_t k_split,
+                 Tables& tb) {
+  if (!plan || (!mats && nmats) || (!items && nitems)) return GRID_ERR_NULL_POINTER;
   if (nmats == 0 || nitems == 0 || nitems > (1u << 30)) return GRID_ERR_INVALID_PARAMETERS;
+  if (k_split != 0 && (k_split < (uint32_t)KC || k_split % KC)) return GRID_ERR_INVALID_PARAMETERS;
   for (size_t i = 0; i < nmats; ++i) {
     if (!mats[i]) return GRID_ERR_NULL_POINTER;
     if (mats[i]->plan != plan) return GRID_ERR_INVALID_PARAMETERS;
     if (mats[i]->rows > (size_t)TN) return GRID_ERR_INVALID_PARAMETERS;  // ranks up to 32
+    tb.mats.push_back(MatDev{mats[i]->d_evals, (uint32_t)mats[i]->rows, (uint32_t)mats[i]->ld});
   }
-  grid_gpu_batch* b = new (std::nothrow) grid_gpu_batch();
-  if (!b) return GRID_ERR_OUT_OF_MEMORY;
-  b->plan = plan;
-  b->num_sms = plan->num_sms;
-  for (size_t i = 0; i < nmats; ++i)
-    b->mats.push_back(MatDev{mats[i]->d_evals, (uint32_t)mats[i]->rows, (uint32_t)mats[i]->ld});
   std::vector<std::pair<uint32_t, uint32_t>> order;  // (matrix, index)
+  order.reserve(nitems);
   for (size_t i = 0; i < nitems; ++i) {
     const grid_gpu_batch_item& it = items[i];
-    if (it.matrix >= nmats || it.n == 0 || it.n > mats[it.matrix]->cols) {
-      delete b;
+    if (it.matrix >= nmats || it.n == 0 || it.n > mats[it.matrix]->cols)
       return GRID_ERR_DIMENSION_MISMATCH;
-    }
-    b->s_polys = std::max<uint64_t>(b->s_polys, it.s_offset + it.n);
-    b->t_polys = std::max<uint64_t>(b->t_polys, it.t_offset + mats[it.matrix]->rows);
+    tb.s_polys = std::max<uint64_t>(tb.s_polys, it.s_offset + it.n);
+    tb.t_polys = std::max<uint64_t>(tb.t_polys, it.t_offset + mats[it.matrix]->rows);
     order.emplace_back(it.matrix, (uint32_t)i);
   }
   std::stable_sort(order.begin(), order.end(), [&](const auto& x, const auto& y) {
@@ -272,17 +305,55 @@ int grid_gpu_batch_create(grid_gpu_plan* plan, grid_gpu_matrix* const* mats, siz
   for (size_t i = 0; i < order.size();) {
     const uint32_t m = order[i].first;
     size_t j = i;
-    TileDev tl{(uint32_t)b->sorted.size(), 0, m, 0};
+    TileDev tl{(uint32_t)tb.sorted.size(), 0, m, 0};
     while (j < order.size() && order[j].first == m && j - i < (size_t)TM) {
       const grid_gpu_batch_item& it = items[order[j].second];
-      b->sorted.push_back(ItemDev{it.s_offset, it.t_offset, it.n, 0});
+      tb.sorted.push_back(ItemDev{it.s_offset, it.t_offset, it.n, 0});
       tl.kmax = std::max(tl.kmax, it.n);
       ++j;
     }
     tl.count = (uint32_t)(j - i);
-    b->tiles.push_back(tl);
+    tb.tiles.push_back(tl);
     i = j;
   }
+  if (k_split == 0) k_split = auto_k_split(tb.tiles, plan->d / EG, plan->num_sms);
+  tb.k_split = k_split;
+  tb.work = make_work(tb.tiles, plan->d / EG, k_split);
+  return GRID_OK;
+}
+
+size_t tables_bytes(const Tables& tb) {
+  return round_up(tb.mats.size() * sizeof(MatDev), 256) +
+         round_up(tb.sorted.size() * sizeof(ItemDev), 256) +
+         round_up(tb.tiles.size() * sizeof(TileDev), 256) +
+         round_up(tb.work.size() * sizeof(WorkDev), 256);
+}
+
+size_t core_bytes(uint64_t s_polys, uint64_t t_polys, size_t d) {
+  return round_up(s_polys * d * 4, 256) + round_up(t_polys * d * 8, 256) + 256;
+}
+
+}  // namespace
+
+extern "C" {
+
+int grid_gpu_batch_create(grid_gpu_plan* plan, grid_gpu_matrix* const* mats, size_t nmats,
+                          const grid_gpu_batch_item* items, size_t nitems, grid_gpu_batch** out) {
+  if (!out) return GRID_ERR_NULL_POINTER;
+  *out = nullptr;
+  Tables tb;
+  int rc = build_tables(plan, mats, nmats, items, nitems, 1024, tb);
+  if (rc) return rc;
+  grid_gpu_batch* b = new (std::nothrow) grid_gpu_batch();
+  if (!b) return GRID_ERR_OUT_OF_MEMORY;
+  b->plan = plan;
+  b->num_sms = plan->num_sms;
+  b->k_split = 1024;
+  b->mats = std::move(tb.mats);
+  b->sorted = std::move(tb.sorted);
+  b->tiles = std::move(tb.tiles);
+  b->s_polys = tb.s_polys;
+  b->t_polys = tb.t_polys;
   cudaError_t e = cudaMalloc(&b->d_mats, b->mats.size() * sizeof(MatDev));
   if (e == cudaSuccess) e = cudaMalloc(&b->d_items, b->sorted.size() * sizeof(ItemDev));
   if (e == cudaSuccess) e = cudaMalloc(&b->d_tiles, b->tiles.size() * sizeof(TileDev));
@@ -295,7 +366,7 @@ int grid_gpu_batch_create(grid_gpu_plan* plan, grid_gpu_matrix* const* mats, siz
   if (e == cudaSuccess)
     e = cudaMemcpy(b->d_tiles, b->tiles.data(), b->tiles.size() * sizeof(TileDev),
                    cudaMemcpyHostToDevice);
-  int rc = cuda_status(e);
+  rc = cuda_status(e);
   if (!rc) rc = rebuild_work(b);
   if (rc) {
     grid_gpu_batch_destroy(b);
@@ -382,6 +453,52 @@ int grid_gpu_batch_commit_graph(grid_gpu_batch* b, const uint32_t* s, uint32_t* 
     it = b->graphs.emplace(key, exec).first;
   }
   return cuda_status(cudaGraphLaunch(it->second, st));
+}
+
+int grid_gpu_batch_oneshot_workspace(grid_gpu_plan* plan, grid_gpu_matrix* const* mats,
+                                     size_t nmats, const grid_gpu_batch_item* items,
+                                     size_t nitems, uint32_t k_split, size_t* bytes) {
+  if (!bytes) return GRID_ERR_NULL_POINTER;
+  Tables tb;
+  const int rc = build_tables(plan, mats, nmats, items, nitems, k_split, tb);
+  if (rc) return rc;
+  *bytes = core_bytes(tb.s_polys, tb.t_polys, plan->d) + tables_bytes(tb);
+  return GRID_OK;
+}
+
+int grid_gpu_batch_commit_oneshot_dev(grid_gpu_plan* plan, grid_gpu_matrix* const* mats,
+                                      size_t nmats, const grid_gpu_batch_item* items,
+                                      size_t nitems, uint32_t k_split, const uint32_t* s,
+                                      uint32_t* t, void* workspace, size_t workspace_bytes,
+                                      void* stream) {
+  if (!s || !t || !workspace) return GRID_ERR_NULL_POINTER;
+  if (((uintptr_t)s | (uintptr_t)t | (uintptr_t)workspace) & 15u) return GRID_ERR_MISALIGNED;
+  Tables tb;
+  int rc = build_tables(plan, mats, nmats, items, nitems, k_split, tb);
+  if (rc) return rc;
+  const size_t core = core_bytes(tb.s_polys, tb.t_polys, plan->d);
+  if (workspace_bytes < core + tables_bytes(tb)) return GRID_ERR_INVALID_PARAMETERS;
+  cudaStream_t st = (cudaStream_t)stream;
+  // Pack the four tables into one host image of the device layout and send
+  // it with a single copy. The source is pageable: the copy returns once its
+  // bytes are staged, so the image may go away when this call returns.
+  std::vector<char> image(tables_bytes(tb));
+  size_t off = 0;
+  char* const dev = static_cast<char*>(workspace) + core;
+  auto put = [&](const void* src, size_t n) -> void* {
+    if (n) std::memcpy(image.data() + off, src, n);
+    void* dst = dev + off;
+    off += round_up(n, 256);
+    return dst;
+  };
+  auto* dm = static_cast<const MatDev*>(put(tb.mats.data(), tb.mats.size() * sizeof(MatDev)));
+  auto* di = static_cast<const ItemDev*>(put(tb.sorted.data(), tb.sorted.size() * sizeof(ItemDev)));
+  auto* dt = static_cast<const TileDev*>(put(tb.tiles.data(), tb.tiles.size() * sizeof(TileDev)));
+  auto* dw = static_cast<const WorkDev*>(put(tb.work.data(), tb.work.size() * sizeof(WorkDev)));
+  rc = cuda_status(cudaMemcpyAsync(dev, image.data(), image.size(), cudaMemcpyHostToDevice, st));
+  if (rc) return rc;
+  return run_core(plan, dm, di, dt, dw, (unsigned)tb.work.size(), tb.s_polys, tb.t_polys, s, t,
+                  workspace, st);
 }
 
 }  // extern "C"

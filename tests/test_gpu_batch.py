@@ -65,6 +65,27 @@ def test_batched_uneven_commits_match_oracle_and_per_call(cuda, oracle, tmp_path
     t2 = torch.zeros_like(t)
     per_call_commit(plan, mats, items, s, t2)
     assert torch.equal(t, t2)
+    # one-shot path: tables built into the caller's workspace, no handle
+    import ctypes as C
+    from lattica_b200 import _lib
+    lib = _lib.load()
+    arr = (_lib.BatchItem * len(items))(*[_lib.BatchItem(*it) for it in items])
+    hs = (C.c_void_p * len(mats))(*[m.handle.value for m in mats])
+    for k_split in (0, 32, 1024):      # 0: the library picks the K range
+        nb = C.c_size_t()
+        assert lib.grid_gpu_batch_oneshot_workspace(plan.handle, hs, len(mats), arr, len(items),
+                                                    k_split, C.byref(nb)) == 0
+        ws = torch.empty(nb.value, dtype=torch.uint8, device=cuda)
+        t3 = torch.zeros_like(t)
+        st = lib.grid_gpu_batch_commit_oneshot_dev(
+            plan.handle, hs, len(mats), arr, len(items), k_split, s.data_ptr(), t3.data_ptr(),
+            ws.data_ptr(), ws.numel(), torch.cuda.current_stream(cuda).cuda_stream)
+        assert st == 0
+        torch.cuda.synchronize()
+        assert torch.equal(t3, t), k_split
+        assert lib.grid_gpu_batch_commit_oneshot_dev(
+            plan.handle, hs, len(mats), arr, len(items), k_split, s.data_ptr(), t3.data_ptr(),
+            ws.data_ptr(), ws.numel() - 256, 0) != 0     # workspace too small
     # autotuner: picks a candidate, persists it, reuses it
     cache = tmp_path / "autotune.json"
     res = batch.autotune(s, t, candidates=(64, 256), reps=2, cache_path=str(cache))
