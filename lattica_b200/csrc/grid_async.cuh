@@ -37,6 +37,11 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t by
                : "memory");
 }
 
+// Plain arrive (release semantics, shared::cta).
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(
@@ -54,6 +59,28 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
   for (uint32_t i = 0; i < kMaxSpins; ++i) {
     if (mbar_try_wait(bar, parity)) return true;
+  }
+  atomicExch(err, GRID_DEV_TIMEOUT);
+  return false;
+}
+
+// Bounded wait that lets the thread sleep in the barrier between polls
+// (suspend-time hint of 20 us; the thread resumes as soon as the phase
+// completes), so waiting warps take no issue slots from working ones. Gives
+// up after kMaxSleeps polls (about 1.3 s at most).
+constexpr uint32_t kMaxSleeps = 1u << 16;
+
+__device__ __forceinline__ bool mbar_wait_sleep(uint64_t* bar, uint32_t parity, int* err) {
+  for (uint32_t i = 0; i < kMaxSleeps; ++i) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity), "r"(20000u)
+        : "memory");
+    if (ok) return true;
   }
   atomicExch(err, GRID_DEV_TIMEOUT);
   return false;

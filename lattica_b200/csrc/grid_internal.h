@@ -55,9 +55,13 @@ struct grid_gpu_plan {
   int device = 0;
   grid::FieldParams f{};
   uint32_t generator = 0, psi = 0, omega = 0, n_inv = 0;  // Montgomery words
+  uint64_t psi_value = 0, n_inv_value = 0;                 // the same, canonical integers
   grid::TwiddleTable tw;
   // Device copy of the twiddle table as uint2 {w, wq}: fw[d], iw[d], {ninv}, {izeta1*ninv}.
   uint2* d_tw = nullptr;
+  // d = 64: byte planes of the Montgomery-form forward / inverse matrices for
+  // the tensor-core transform (2 x 16 KB); null selects the CUDA-core kernels.
+  void* d_tcw = nullptr;
   int* d_err = nullptr;
   cudaStream_t stream = nullptr;   // host-buffer entry points: first pipeline stream
   cudaStream_t stream2 = nullptr;  // second pipeline stream
@@ -80,6 +84,12 @@ namespace grid {
 int launch_ntt(const grid_gpu_plan* p, int mode, const uint32_t* a, const uint32_t* b,
                uint32_t* out, size_t npolys, cudaStream_t s);
 int ntt_max_degree();
+// ntt_tc.cu (d = 64, tcgen05)
+bool ntt_tc_available(const grid_gpu_plan* p);
+int launch_ntt_tc(const grid_gpu_plan* p, int mode, const uint32_t* a, const uint32_t* b,
+                  uint32_t* out, size_t npolys, cudaStream_t s);
+void build_tc_tables(uint32_t q, uint32_t d, uint64_t psi, uint64_t ninv,
+                     std::vector<unsigned char>& out);
 
 // commit.cu: out_e[m][n] = sum_k X[m][k][e] * Y[n][k][e] for every evaluation point.
 enum EmmOut : int { EMM_DENSE = 0, EMM_UPPER = 1 };

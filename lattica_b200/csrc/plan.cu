@@ -10,6 +10,7 @@
 //   TwistedNttPlan::build (psi)    algebra/src/poly/ntt.rs:139-154
 #include <cuda_runtime.h>
 
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -311,6 +312,14 @@ uint32_t grid_gpu_max_degree(void) { return kMaxDegree; }
 
 namespace {
 
+// d = 64 transforms run on the tensor cores unless the environment variable
+// GRID_GPU_NTT_ENGINE is "cuda_core" when the plan is created (the CUDA-core
+// kernels serve every degree; both give identical words).
+bool use_tensor_cores() {
+  const char* v = std::getenv("GRID_GPU_NTT_ENGINE");
+  return !(v && std::strcmp(v, "cuda_core") == 0);
+}
+
 // Validation and every host-side table of a plan (no device work).
 int fill_plan_host(uint64_t q, uint64_t d, grid_gpu_plan* p) {
   if (q < 3 || (q & 1) == 0 || q >= (1ull << 32) || !is_prime(q)) return GRID_ERR_INVALID_MODULUS;
@@ -335,9 +344,11 @@ int fill_plan_host(uint64_t q, uint64_t d, grid_gpu_plan* p) {
   p->f.r2 = (uint32_t)(((unsigned __int128)1 << 64) % q);
   p->generator = hf.to_mont(g);
   p->psi = hf.to_mont(psi);
+  p->psi_value = psi;
   p->omega = hf.to_mont(omega);
   const uint64_t ninv = hf.inv(d % q);
   p->n_inv = hf.to_mont(ninv);
+  p->n_inv_value = ninv;
 
   // Merged twiddles psi^brv(k), k in [1, d).
   TwiddleTable& tw = p->tw;
@@ -408,6 +419,14 @@ int grid_gpu_plan_create(uint64_t q, uint64_t d, grid_gpu_plan** out) {
     if ((e = cudaMalloc(&p->d_tw, dev_tw.size() * sizeof(uint2))) != cudaSuccess) break;
     if ((e = cudaMemcpy(p->d_tw, dev_tw.data(), dev_tw.size() * sizeof(uint2),
                         cudaMemcpyHostToDevice)) != cudaSuccess) break;
+    if (d == 64 && use_tensor_cores()) {
+      std::vector<unsigned char> tcw;
+      build_tc_tables(p->q, p->d, p->psi_value, p->n_inv_value, tcw);
+      if ((e = cudaMalloc(&p->d_tcw, tcw.size())) != cudaSuccess) break;
+      if ((e = cudaMemcpy(p->d_tcw, tcw.data(), tcw.size(), cudaMemcpyHostToDevice)) !=
+          cudaSuccess)
+        break;
+    }
     if ((e = cudaMalloc(&p->d_err, sizeof(int))) != cudaSuccess) break;
     if ((e = cudaMemset(p->d_err, 0, sizeof(int))) != cudaSuccess) break;
     if ((e = cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking)) != cudaSuccess) break;
@@ -432,6 +451,7 @@ int grid_gpu_plan_destroy(grid_gpu_plan* p) {
   for (auto& s : p->scratch)
     if (s.ptr) cudaFree(s.ptr);
   if (p->d_tw) cudaFree(p->d_tw);
+  if (p->d_tcw) cudaFree(p->d_tcw);
   if (p->d_err) cudaFree(p->d_err);
   if (p->stream) cudaStreamDestroy(p->stream);
   if (p->stream2) cudaStreamDestroy(p->stream2);
