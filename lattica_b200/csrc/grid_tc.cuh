@@ -115,5 +115,17 @@ __device__ __forceinline__ void tmem_ld_wait() {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// Wait for this thread's tensor-memory loads, naming the 16 registers they
+// fill so that no use of them can be scheduled above the wait.
+__device__ __forceinline__ void tmem_ld_wait(uint32_t (&r)[4][4]) {
+  asm volatile("tcgen05.wait::ld.sync.aligned;"
+               : "+r"(r[0][0]), "+r"(r[0][1]), "+r"(r[0][2]), "+r"(r[0][3]), "+r"(r[1][0]),
+                 "+r"(r[1][1]), "+r"(r[1][2]), "+r"(r[1][3]), "+r"(r[2][0]), "+r"(r[2][1]),
+                 "+r"(r[2][2]), "+r"(r[2][3]), "+r"(r[3][0]), "+r"(r[3][1]), "+r"(r[3][2]),
+                 "+r"(r[3][3])
+               :
+               : "memory");
+}
+
 }  // namespace tc
 }  // namespace grid
