@@ -64,7 +64,7 @@ static_assert(SMEM_BYTES <= 232448, "shared memory budget");
 enum Bar : int {
   AFULL0 = 0, AFULL1,  // input tile landed in buffer 0 / 1
   STAGED0, STAGED1,    // result tile written into buffer 0 / 1
-  FDONE, PREADY, IDONE, EREAD, NBARS
+  FDONE, FREAD, PREADY, IDONE, EREAD, NBARS
 };
 
 struct TcConsts {
@@ -98,21 +98,21 @@ __device__ __forceinline__ uint32_t redc64(uint64_t v, uint32_t q, uint32_t qinv
 }
 
 // 16 reduced results of this thread's row: columns col0 .. col0 + 15 of the
-// four E_l blocks (64 columns apart) starting at taddr; four tensor-memory
-// round trips of 4 columns x 4 blocks.
+// four E_l blocks (64 columns apart) starting at taddr; two tensor-memory
+// round trips of 8 columns x 4 blocks.
 __device__ __forceinline__ void reduce16(uint32_t taddr, const TcConsts& k, uint32_t* out) {
 #pragma unroll
-  for (int c = 0; c < 4; ++c) {
-    uint32_t e[4][4];
+  for (int c = 0; c < 2; ++c) {
+    uint32_t e[4][8];
 #pragma unroll
-    for (int l = 0; l < 4; ++l) tc::tmem_ld4(taddr + 64 * l + 4 * c, e[l]);
-    tc::tmem_ld_wait(e);
+    for (int l = 0; l < 4; ++l) tc::tmem_ld8(taddr + 64 * l + 8 * c, e[l]);
+    tc::tmem_ld_wait32(e);
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
+    for (int j = 0; j < 8; ++j) {
       uint64_t v = mad_wide(e[1][j], 256u, (uint64_t)e[0][j]);
       v = mad_wide(e[2][j], 65536u, v);
       v = mad_wide(e[3][j], 16777216u, v);
-      out[4 * c + j] = redc64(v, k.q, k.qinv);
+      out[8 * c + j] = redc64(v, k.q, k.qinv);
     }
   }
 }
@@ -153,11 +153,19 @@ __device__ __forceinline__ bool warp_wait(uint64_t* bar, uint32_t parity, int* e
   return __all_sync(0xffffffffu, ok);
 }
 
+// The epilogue's waits on MMA results are on the critical path: poll
+// without a suspend hint.
+__device__ __forceinline__ bool warp_wait_fast(uint64_t* bar, uint32_t parity, int* err) {
+  const bool ok = mbar_wait(bar, parity, err);
+  return __all_sync(0xffffffffu, ok);
+}
+
 // MODE_FWD / MODE_INV: one transform per tile, results written by phase F.
 // MODE_MULINV: F = forward + Montgomery product with b -> product tile;
 // E = inverse -> results. Per tile j of this CTA:
 //   MMA warp: fwd(j) once tile j is loaded and F(j-1) has read columns
-//             0-255; then inv(j-1) once E(j-2) has read columns 256-511
+//             0-255 (FREAD); then inv(j-1) once F(j-1) has written the
+//             product tile (PREADY) and E(j-2) has read columns 256-511
 //   epilogue: F(j), then E(j-1)
 //   loader:   buffer t & 1 holds input tile t until fwd(t) is done, then a
 //             result tile (single transform: tile t; two: tile t-1), which it
@@ -193,6 +201,7 @@ __global__ void __launch_bounds__(THREADS, 1)
       mbar_init(&bars[STAGED0], EPI_WARPS);
       mbar_init(&bars[STAGED1], EPI_WARPS);
       mbar_init(&bars[FDONE], 1);
+      mbar_init(&bars[FREAD], EPI_WARPS);
       mbar_init(&bars[PREADY], EPI_WARPS);
       mbar_init(&bars[IDONE], 1);
       mbar_init(&bars[EREAD], EPI_WARPS);
@@ -282,7 +291,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     bool ok = true;
     for (uint32_t j = 0; ok && j < n; ++j) {
       ok = warp_wait(&bars[AFULL0 + (j & 1)], (j >> 1) & 1, err);
-      if (ok && j >= 1) ok = warp_wait(&bars[PREADY], (j - 1) & 1, err);  // F(j-1) read R0
+      if (ok && j >= 1) ok = warp_wait(&bars[FREAD], (j - 1) & 1, err);  // F(j-1) read R0
       if (!ok) break;
       issue(R0, s0 + OFF_XA + (j & 1) * TILE, s0 + OFF_W, FDONE);
       if (kTwo && j >= 1) ok = inverse(j - 1);
@@ -290,7 +299,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     if (ok && n > 0) {
       if (kTwo) ok = inverse(n - 1);
       // the last results must be read before the columns are freed
-      if (ok) warp_wait(&bars[kTwo ? EREAD : PREADY], (n - 1) & 1, err);
+      if (ok) warp_wait(&bars[kTwo ? EREAD : FREAD], (n - 1) & 1, err);
     }
     if (!ok) {
       const int started[2] = {FDONE, IDONE};
@@ -331,7 +340,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     };
     // E(j): inverse results of tile j
     auto inverse_out = [&](uint32_t j) {
-      ok = ok && warp_wait(&bars[IDONE], j & 1, err);
+      ok = ok && warp_wait_fast(&bars[IDONE], j & 1, err);
       if (!ok) return;
       tc::fence_after_sync();
       uint32_t res[16];
@@ -346,12 +355,14 @@ __global__ void __launch_bounds__(THREADS, 1)
     if (kTwo && n > 0) load_b(0, bv);
     for (uint32_t j = 0; ok && j < n; ++j) {
       // F(j)
-      ok = warp_wait(&bars[FDONE], j & 1, err);
+      ok = warp_wait_fast(&bars[FDONE], j & 1, err);
       if (!ok) break;
       tc::fence_after_sync();
       uint32_t res[16];
       reduce16(R0 + lane_off, k, res);
       tc::fence_before_sync();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&bars[FREAD]);  // columns 0-255 free for fwd(j+1)
       if (kTwo) {
 #pragma unroll
         for (int c = 0; c < 4; ++c) {  // Montgomery product with b: t * b < q * 2^32
@@ -361,7 +372,7 @@ __global__ void __launch_bounds__(THREADS, 1)
           res[4 * c + 3] = redc64(mad_wide(res[4 * c + 3], bv[c].w, 0ull), k.q, k.qinv);
         }
         // inv(j-1) must be done reading the product tile
-        if (j >= 1) ok = warp_wait(&bars[IDONE], (j - 1) & 1, err);
+        if (j >= 1) ok = warp_wait_fast(&bars[IDONE], (j - 1) & 1, err);
         if (!ok) break;
         put_row(sm + OFF_PP, res);
         tc::fence_async_smem();
@@ -370,8 +381,6 @@ __global__ void __launch_bounds__(THREADS, 1)
         if (j + 1 < n) load_b(j + 1, bv);
         if (j >= 1) inverse_out(j - 1);
       } else {
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&bars[PREADY]);
         stage(j, res);
       }
     }
