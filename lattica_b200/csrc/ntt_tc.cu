@@ -239,14 +239,14 @@ __global__ void __launch_bounds__(THREADS, 1)
     };
     prefetch(0);
     prefetch(1);
+    prefetch(2);
     for (uint32_t t = 0; ok && t < n + lag; ++t) {
       const uint32_t buf = t & 1;
       const uint32_t dst = s0 + OFF_XA + buf * TILE;
-      prefetch(t + 2);
-      if (t >= 2 && t - 2 < n) ok = warp_wait(&bars[FDONE], t & 1, err);  // fwd(t - 2) done
+      if (t >= 2 && t - 2 < n) ok = warp_wait_fast(&bars[FDONE], t & 1, err);  // fwd(t - 2) done
       if (ok && t >= lag) {
         const uint32_t js = t - lag;
-        ok = warp_wait(&bars[STAGED0 + buf], staged_seen[buf]++ & 1, err);
+        ok = warp_wait_fast(&bars[STAGED0 + buf], staged_seen[buf]++ & 1, err);
         if (ok && lane == 0) {
           tma_store_2d(&tmap_out, 0, (int)tile_row0(js), dst);
           tma_store_2d(&tmap_out, 32, (int)tile_row0(js), dst + BOX);
@@ -265,6 +265,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         }
         __syncwarp();
       }
+      prefetch(t + 2);
     }
     if (lane == 0) bulk_wait_all();
     if (!ok)
@@ -283,15 +284,15 @@ __global__ void __launch_bounds__(THREADS, 1)
       __syncwarp();
     };
     auto inverse = [&](uint32_t j) -> bool {  // inv(j): after F(j) and E(j-1)
-      if (!warp_wait(&bars[PREADY], j & 1, err)) return false;
-      if (j >= 1 && !warp_wait(&bars[EREAD], (j - 1) & 1, err)) return false;
+      if (!warp_wait_fast(&bars[PREADY], j & 1, err)) return false;
+      if (j >= 1 && !warp_wait_fast(&bars[EREAD], (j - 1) & 1, err)) return false;
       issue(R1, s0 + OFF_PP, s0 + OFF_W + WMAT, IDONE);
       return true;
     };
     bool ok = true;
     for (uint32_t j = 0; ok && j < n; ++j) {
-      ok = warp_wait(&bars[AFULL0 + (j & 1)], (j >> 1) & 1, err);
-      if (ok && j >= 1) ok = warp_wait(&bars[FREAD], (j - 1) & 1, err);  // F(j-1) read R0
+      ok = warp_wait_fast(&bars[AFULL0 + (j & 1)], (j >> 1) & 1, err);
+      if (ok && j >= 1) ok = warp_wait_fast(&bars[FREAD], (j - 1) & 1, err);  // F(j-1) read R0
       if (!ok) break;
       issue(R0, s0 + OFF_XA + (j & 1) * TILE, s0 + OFF_W, FDONE);
       if (kTwo && j >= 1) ok = inverse(j - 1);
