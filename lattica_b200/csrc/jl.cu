@@ -22,8 +22,10 @@
 // 64-bit global row sums with atomics; a final kernel reduces them mod q.
 #include <cuda_runtime.h>
 
+#include "grid_async.cuh"
 #include "grid_field.cuh"
 #include "grid_internal.h"
+#include "grid_tc.cuh"
 
 namespace grid {
 namespace {
@@ -166,6 +168,153 @@ __global__ void jl_finish_kernel(const unsigned long long* __restrict__ gsum_pos
   }
 }
 
+// ---------------------------------------------------------------------------
+// Tensor-core projection. A CTA takes chunks of 256 columns of one part:
+// thread t computes the keystream of column c0 + t and writes its 256
+// entries shifted by one, M' = M + 1 in {0, 1, 2}, as column t of an
+// MN-major u8 A tile (rows contiguous), and the column's word as a
+// zero-padded 16-byte column of an MN-major u8 B tile (bytes = N). One u8
+// MMA per (128-row half, 32-column step) accumulates
+// D'[r][i] = sum_c M'[r][c] * byte_i(x_c) in tensor memory across all of the
+// CTA's chunks; then p_r = sum_i 2^(8i) (D'[r][i] - sum_c byte_i(x_c)) mod q.
+// D' < 2 * 255 * (columns per CTA) stays below 2^31 (the host bounds the
+// columns per CTA).
+// ---------------------------------------------------------------------------
+constexpr int kTcThreads = 256;
+constexpr int kTcCols = 256;                      // columns (K) per chunk
+constexpr uint32_t kTcA = 256u * kTcCols;         // A tile: 256 rows x 256 columns
+constexpr uint32_t kTcB = 16u * kTcCols;          // B tile: 16 bytes x 256 columns
+constexpr uint32_t kTcSmem = kTcA + kTcB + 1024 + 64 + 1024;  // + LUT, barrier, slack
+constexpr unsigned long long kTcMaxColsPerCta = 1ull << 22;    // 2 * 255 * 2^22 < 2^31
+
+// row m, column k of the A tile: 16-row x 8-column core matrices
+__device__ __forceinline__ uint32_t jl_a_off(uint32_t m, uint32_t k) {
+  return (k >> 3) * 2048u + (m >> 4) * 128u + (k & 7u) * 16u + (m & 15u);
+}
+
+// M' = M + 1 for the 4 codes of one keystream byte: 00 -> 2, 01 -> 0, 1x -> 1.
+__device__ __forceinline__ uint32_t shifted_entries_of_byte(uint32_t byte) {
+  uint32_t out = 0;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const uint32_t c = (byte >> (2 * i)) & 3u;
+    const uint32_t v = c == 0 ? 2u : (c == 1 ? 0u : 1u);
+    out |= v << (8 * i);
+  }
+  return out;
+}
+
+template <bool kWholeBlocks>
+__global__ void __launch_bounds__(kTcThreads) jl_tc_kernel(
+    const uint32_t* __restrict__ parts, unsigned long long cols, int rows, int packed_len,
+    ChachaKey key, unsigned long long nchunks, unsigned long long* __restrict__ gsum_pos,
+    uint32_t q, int* __restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char sm_raw[];
+  const uint32_t raw = smem_addr(sm_raw);
+  unsigned char* sm = sm_raw + (((raw + 1023u) & ~1023u) - raw);
+  const uint32_t s0 = smem_addr(sm);
+  uint32_t* lut = reinterpret_cast<uint32_t*>(sm + kTcA + kTcB);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kTcA + kTcB + 1024);
+  uint32_t* taddr_slot = reinterpret_cast<uint32_t*>(bar + 1);
+  uint32_t* colsum = taddr_slot + 2;  // [4]
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  for (int i = tid; i < 256; i += kTcThreads) lut[i] = shifted_entries_of_byte(i);
+  if (tid < 4) colsum[tid] = 0;
+  if (warp == 0) {
+    tc::tmem_alloc(taddr_slot, 32);
+    tc::tmem_relinquish();
+  }
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    fence_mbar_init();
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tbase = *taddr_slot;
+  // kind::i8, u8 x u8 -> s32, A and B MN-major, M = 128, N = 16
+  const uint32_t idesc = tc::idesc_u8(128, 16) | (1u << 15) | (1u << 16);
+
+  const unsigned long long per_part = (cols + kTcCols - 1) / kTcCols;
+  uint32_t bsum[4] = {0, 0, 0, 0};
+  bool ok = true;
+  uint32_t it = 0;
+  for (unsigned long long ch = blockIdx.x; ch < nchunks; ch += gridDim.x, ++it) {
+    const uint32_t part = (uint32_t)(ch / per_part);
+    const unsigned long long c = (ch % per_part) * kTcCols + tid;
+    uint32_t w[16];
+    uint32_t x = 0;
+    if (c < cols) {
+      if constexpr (kWholeBlocks)
+        chacha20_block(key, (uint32_t)c, part, w);
+      else
+        keystream64(key, part, c * (unsigned long long)packed_len, w);
+      x = parts[(unsigned long long)part * cols + c];
+    } else {
+#pragma unroll
+      for (int i = 0; i < 16; ++i) w[i] = 0xFFFFFFFFu;  // padding column: x = 0
+    }
+    // the previous chunk's MMAs must be done reading the tiles
+    if (it > 0) ok = __syncthreads_and(mbar_wait(bar, (it - 1) & 1, err));
+    if (!ok) break;
+#pragma unroll
+    for (int g = 0; g < 16; ++g)
+      *reinterpret_cast<uint4*>(sm + jl_a_off(16 * g, tid)) =
+          make_uint4(lut[w[g] & 0xFFu], lut[(w[g] >> 8) & 0xFFu], lut[(w[g] >> 16) & 0xFFu],
+                     lut[w[g] >> 24]);
+    *reinterpret_cast<uint4*>(sm + kTcA + (tid >> 3) * 128 + (tid & 7) * 16) =
+        make_uint4(x, 0, 0, 0);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) bsum[i] += (x >> (8 * i)) & 0xFFu;
+    tc::fence_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    if (tid == 0) {
+      tc::fence_after_sync();
+#pragma unroll
+      for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int ks = 0; ks < kTcCols / 32; ++ks)
+          tc::mma_u8(tbase + 16 * h, tc::smem_desc(s0 + h * 1024 + ks * 8192, 2048, 128),
+                     tc::smem_desc(s0 + kTcA + ks * 512, 128, 256), idesc,
+                     (it | (uint32_t)ks) != 0);
+      tc::mma_commit(bar);
+    }
+  }
+  if (ok && it > 0) ok = mbar_wait(bar, (it - 1) & 1, err);
+  ok = __syncthreads_and(ok);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    uint32_t v = bsum[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) atomicAdd(&colsum[i], v);
+  }
+  __syncthreads();
+  tc::fence_after_sync();
+  if (ok && it > 0 && warp < 4) {
+    uint32_t d0[4], d1[4];
+    tc::tmem_ld4(tc::tmem_addr(tbase, 32 * warp, 0), d0);
+    tc::tmem_ld4(tc::tmem_addr(tbase, 32 * warp, 16), d1);
+    tc::tmem_ld_wait();
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int row = 128 * h + 32 * warp + lane;
+      const uint32_t* dv = h ? d1 : d0;
+      long long v = 0;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) v += ((long long)dv[i] - (long long)colsum[i]) << (8 * i);
+      long long r = v % (long long)q;
+      if (r < 0) r += q;
+      if (row < rows) atomicAdd(&gsum_pos[row], (unsigned long long)r);
+    }
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tbase, 32);
+}
+
 // Entry -> int8 table for one keystream byte: 4 rows, 2 bits each.
 __device__ __forceinline__ uint32_t entries_of_byte(uint32_t byte) {
   uint32_t out = 0;
@@ -257,7 +406,7 @@ size_t jl_scratch_bytes(size_t rows, size_t, int) { return 2 * rows * sizeof(uns
 int launch_jl_project(const FieldParams& f, const uint8_t seed[32], size_t rows,
                       const uint32_t* parts, size_t num_parts, size_t cols, size_t d,
                       uint32_t* p_out, int8_t* flat_out, void* scratch, size_t scratch_bytes,
-                      int num_sms, int*, cudaStream_t s) {
+                      int num_sms, int* err, cudaStream_t s) {
   if (rows == 0 || rows > 256 || d == 0 || cols % d != 0 || num_parts == 0 ||
       num_parts > 0xFFFFFFFFull)
     return GRID_ERR_INVALID_PARAMETERS;
@@ -271,7 +420,31 @@ int launch_jl_project(const FieldParams& f, const uint8_t seed[32], size_t rows,
   unsigned long long* gneg = gpos + rows;
   cudaError_t e = cudaMemsetAsync(gpos, 0, 2 * rows * sizeof(unsigned long long), s);
   if (e != cudaSuccess) return cuda_status(e);
-  if (cols > 0) {
+  static int tc_bps_whole[kMaxDevices] = {}, tc_bps_part[kMaxDevices] = {};
+  int dev = 0, bps = 0;
+  const unsigned long long tc_chunks = (cols + kTcCols - 1) / kTcCols * num_parts;
+  bool use_tc = cols > 0 && cudaGetDevice(&dev) == cudaSuccess &&
+                (packed_len == 64
+                     ? prepare_kernel(jl_tc_kernel<true>, kTcSmem, kTcThreads, dev, tc_bps_whole,
+                                      &bps)
+                     : prepare_kernel(jl_tc_kernel<false>, kTcSmem, kTcThreads, dev, tc_bps_part,
+                                      &bps)) == GRID_OK;
+  unsigned long long tc_grid = (unsigned long long)num_sms * (unsigned long long)(bps > 0 ? bps : 1);
+  if (tc_grid > tc_chunks) tc_grid = tc_chunks;
+  // exactness bound of the int32 accumulators: columns per CTA
+  if (use_tc && tc_grid > 0 &&
+      (tc_chunks + tc_grid - 1) / tc_grid * (unsigned long long)kTcCols > kTcMaxColsPerCta)
+    use_tc = false;
+  if (use_tc) {
+    if (packed_len == 64)
+      jl_tc_kernel<true><<<(unsigned)tc_grid, kTcThreads, kTcSmem, s>>>(
+          parts, cols, (int)rows, packed_len, key, tc_chunks, gpos, f.q, err);
+    else
+      jl_tc_kernel<false><<<(unsigned)tc_grid, kTcThreads, kTcSmem, s>>>(
+          parts, cols, (int)rows, packed_len, key, tc_chunks, gpos, f.q, err);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_status(e);
+  } else if (cols > 0) {
     const unsigned long long chunks = (cols + 31) / 32 * num_parts;
     unsigned long long blocks = (chunks + kJlWarps - 1) / kJlWarps;
     const unsigned long long cap = (unsigned long long)num_sms * 8;
