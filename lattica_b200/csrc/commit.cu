@@ -22,44 +22,102 @@
 // Partial sums of a K split are canonical residues, so splits add exactly.
 #include <cuda_runtime.h>
 
+#include "grid_async.cuh"
 #include "grid_field.cuh"
 #include "grid_internal.h"
 
 namespace grid {
 namespace {
 
-constexpr int BM = 32, BN = 32, EG = 8, KC = 16, PAD = 4;
-constexpr int ROWX = BM + PAD;  // words per (k, e) row of the X tile
-constexpr int ROWY = BN + PAD;
+constexpr int EG = 8, KC = 16;
+// Words per staged row: 16 K steps x 8 evaluation points, padded by 2 so that
+// rows 4 apart start 8 banks apart.
+constexpr int RS = KC * EG + 2;
 constexpr int kEmmThreads = 256;
 
 enum OutMode : int { OUT_DENSE = 0, OUT_UPPER = 1 };
+
+// Output tile of a CTA: TMG groups of 4 rows of X by (32 / TMG) groups of 8
+// rows of Y, for 8 evaluation points; each of the 256 threads keeps one
+// evaluation point of a 4 x 8 sub-tile. TMG = 8 is the square 32 x 32 tile;
+// TMG = 16 (64 x 16) fits the short Y of a commitment (kappa = 16 rows of A).
+template <int TMG>
+struct EmmTile {
+  static constexpr int TNG = 32 / TMG;
+  static constexpr int BM = 4 * TMG, BN = 8 * TNG;
+  static constexpr int STAGE_WORDS = (BM + BN) * RS;
+  // Three stages where two CTAs per SM still fit in shared memory, else two.
+  static constexpr int STAGES = 3 * STAGE_WORDS * 4 <= 100 * 1024 ? 3 : 2;
+  static constexpr size_t SMEM = (size_t)STAGES * STAGE_WORDS * 4;
+};
 
 // X: [M][K][d], Y: [N][ldy][d] (first K of ldy columns used). Dense output:
 // [M][N][d]; upper output (X == Y, M == N): packed upper triangle i <= j in
 // row-major order (garbage_index).
 // With splits > 1 the CTA of split s writes to out + s * split_stride.
-__global__ void __launch_bounds__(kEmmThreads) emm_kernel(
+// Operands stream through a cp.async ring of STAGES chunks (X rows, then Y
+// rows, each in global order: [k][e]); two CTAs per SM. A warp covers 8
+// evaluation points x 4 consecutive row groups of X, so its X reads hit 32
+// distinct banks and its Y reads are broadcasts.
+template <int TMG>
+__global__ void __launch_bounds__(kEmmThreads, 2) emm_kernel(
     const uint32_t* __restrict__ X, const uint32_t* __restrict__ Y, uint32_t* __restrict__ out,
     int M, int N, int K, int ldy, int d, int mode, int k_per_split, size_t split_stride,
     FieldParams f) {
-  __shared__ __align__(16) uint32_t Xs[KC * EG * ROWX];
-  __shared__ __align__(16) uint32_t Ys[KC * EG * ROWY];
+  using Tl = EmmTile<TMG>;
+  constexpr int BM = Tl::BM, BN = Tl::BN, STAGES = Tl::STAGES;
+  constexpr int SW = Tl::STAGE_WORDS;
+  extern __shared__ __align__(16) uint32_t emm_smem[];
 
   const int tiles_n = (N + BN - 1) / BN;
-  const int tile = blockIdx.y;
-  const int tm0 = (tile / tiles_n) * BM;
-  const int tn0 = (tile % tiles_n) * BN;
-  if (mode == OUT_UPPER && tm0 > tn0) return;  // strictly-lower tiles hold no output
+  int ti = (int)blockIdx.y / tiles_n, tj = (int)blockIdx.y % tiles_n;
+  if (mode == OUT_UPPER) {
+    // Square tiles; blockIdx.y enumerates the tiles ti <= tj row by row.
+    int u = (int)blockIdx.y;
+    ti = 0;
+    while (u >= tiles_n - ti) u -= tiles_n - ti++;
+    tj = ti + u;
+  }
+  const int tm0 = ti * BM;
+  const int tn0 = tj * BN;
   const int e0 = blockIdx.x * EG;
   const int split = blockIdx.z;
   const int kbeg = split * k_per_split;
   const int kend = min(K, kbeg + k_per_split);
+  const int nchunks = kend > kbeg ? (kend - kbeg + KC - 1) / KC : 0;
 
   const int t = threadIdx.x;
   const int eg = t & 7;
-  const int tn = (t >> 3) & 3;
-  const int tm = t >> 5;
+  const int tm = (t >> 3) % TMG;
+  const int tn = (t >> 3) / TMG;
+
+  // Copy chunk c (K steps kbeg + 16c ..) into stage c % STAGES as 8-byte
+  // pieces, one half row per warp; rows past M / N and steps past kend are
+  // zero-filled.
+  auto issue = [&](int c) {
+    uint32_t* st = emm_smem + (c % STAGES) * SW;
+    const int k0 = kbeg + c * KC;
+#pragma unroll
+    for (int i = 0; i < (BM + BN) / 4; ++i) {
+      const int u = t + kEmmThreads * i;  // (row, kk, quarter)
+      const int quarter = u & 3;
+      const int kk = (u >> 2) & (KC - 1);
+      const int row = u >> 6;
+      const int k = k0 + kk;
+      const uint32_t* src = X;
+      bool valid;
+      if (row < BM) {  // uniform per i: BM is a multiple of 4
+        const int m = tm0 + row;
+        valid = k < kend && m < M;
+        if (valid) src = X + ((size_t)m * K + k) * d + e0 + quarter * 2;
+      } else {
+        const int n = tn0 + row - BM;
+        valid = k < kend && n < N;
+        if (valid) src = Y + ((size_t)n * ldy + k) * d + e0 + quarter * 2;
+      }
+      cp_async8(st + row * RS + kk * EG + quarter * 2, src, valid ? 8u : 0u);
+    }
+  };
 
   Acc96 acc[4][8];
 #pragma unroll
@@ -67,43 +125,37 @@ __global__ void __launch_bounds__(kEmmThreads) emm_kernel(
 #pragma unroll
     for (int j = 0; j < 8; ++j) acc96_zero(acc[i][j]);
 
-  for (int k0 = kbeg; k0 < kend; k0 += KC) {
-    // Stage X[tm0 .. +32][k0 .. +16][e0 .. +8] and the same of Y.
+  // This thread's words: X rows tm*4 + i and Y rows BM + tn*8 + j, step kk,
+  // evaluation point eg.
+  const int xo = (tm * 4) * RS + eg;
+  const int yo = (BM + tn * 8) * RS + eg;
+
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int u = t + kEmmThreads * i;  // 0 .. 1023: (mm, kk, half)
-      const int half = u & 1;
-      const int kk = (u >> 1) & (KC - 1);
-      const int mm = u >> 5;
-      const int k = k0 + kk;
-      uint4 vx = make_uint4(0, 0, 0, 0), vy = make_uint4(0, 0, 0, 0);
-      if (k < kend) {
-        const int m = tm0 + mm, n = tn0 + mm;
-        if (m < M)
-          vx = *reinterpret_cast<const uint4*>(X + ((size_t)m * K + k) * d + e0 + half * 4);
-        if (n < N)
-          vy = *reinterpret_cast<const uint4*>(Y + ((size_t)n * ldy + k) * d + e0 + half * 4);
-      }
-      uint32_t* xs = Xs + (kk * EG + half * 4) * ROWX + mm;
-      uint32_t* ys = Ys + (kk * EG + half * 4) * ROWY + mm;
-      xs[0] = vx.x; xs[ROWX] = vx.y; xs[2 * ROWX] = vx.z; xs[3 * ROWX] = vx.w;
-      ys[0] = vy.x; ys[ROWY] = vy.y; ys[2 * ROWY] = vy.z; ys[3 * ROWY] = vy.w;
-    }
-    __syncthreads();
+  for (int c = 0; c < STAGES - 1; ++c) {
+    if (c < nchunks) issue(c);
+    cp_async_commit();
+  }
+  for (int c = 0; c < nchunks; ++c) {
+    cp_async_wait<STAGES - 2>();
+    __syncthreads();  // chunk c landed for every thread; stage (c - 1) % STAGES is free
+    if (c + STAGES - 1 < nchunks) issue(c + STAGES - 1);
+    cp_async_commit();
+    const uint32_t* xs = emm_smem + (c % STAGES) * SW + xo;
+    const uint32_t* ys = emm_smem + (c % STAGES) * SW + yo;
 #pragma unroll 4
     for (int kk = 0; kk < KC; ++kk) {
-      const uint4 xv = *reinterpret_cast<const uint4*>(Xs + (kk * EG + eg) * ROWX + tm * 4);
-      const uint4 y0 = *reinterpret_cast<const uint4*>(Ys + (kk * EG + eg) * ROWY + tn * 8);
-      const uint4 y1 = *reinterpret_cast<const uint4*>(Ys + (kk * EG + eg) * ROWY + tn * 8 + 4);
-      const uint32_t xr[4] = {xv.x, xv.y, xv.z, xv.w};
-      const uint32_t yr[8] = {y0.x, y0.y, y0.z, y0.w, y1.x, y1.y, y1.z, y1.w};
+      uint32_t xr[4], yr[8];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) xr[i] = xs[kk * EG + i * RS];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) yr[j] = ys[kk * EG + j * RS];
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 8; ++j) acc96_mad(acc[i][j], xr[i], yr[j]);
     }
-    __syncthreads();
   }
+  cp_async_wait<0>();
 
   const int e = e0 + eg;
   uint32_t* o = out + (size_t)split * split_stride;
@@ -137,21 +189,53 @@ __global__ void sum_splits_kernel(const uint32_t* __restrict__ part, uint32_t* _
   }
 }
 
-int choose_splits(int ctas, int K, int num_sms) {
-  // Enough CTAs for ~2 waves, but keep each split at >= 64 K steps.
-  int splits = 1;
-  while (ctas * splits < 2 * num_sms && K / (splits * 2) >= 64) splits *= 2;
-  return splits;
+// Launch geometry of one product: tile shape, tiles and the K split.
+struct EmmGeometry {
+  int tmg, tiles_m, tiles_n, tiles, splits, k_per_split;
+};
+
+// The K range is split so that all CTAs fit one wave of the resident slots
+// (2 CTAs per SM), each split a whole number of 16-step chunks and at least
+// two of them; split partials go to the workspace and are summed after.
+EmmGeometry emm_geometry(int M, int N, int K, int d, int mode, int num_sms) {
+  EmmGeometry g;
+  g.tmg = (mode == OUT_DENSE && N <= 16) ? 16 : 8;
+  const int bm = 4 * g.tmg, bn = 8 * (32 / g.tmg);
+  g.tiles_m = (M + bm - 1) / bm;
+  g.tiles_n = (N + bn - 1) / bn;
+  g.tiles = mode == OUT_UPPER ? g.tiles_m * (g.tiles_m + 1) / 2 : g.tiles_m * g.tiles_n;
+  const long long ctas = (long long)(d / EG) * g.tiles;
+  const long long slots = 2LL * num_sms;
+  const int chunks = (K + KC - 1) / KC;
+  long long want = ctas >= slots ? 1 : slots / ctas;
+  if (want > chunks / 2) want = chunks / 2 > 1 ? chunks / 2 : 1;
+  const int cps = (int)((chunks + want - 1) / want);  // chunks per split
+  g.splits = (chunks + cps - 1) / cps;
+  g.k_per_split = cps * KC;
+  return g;
+}
+
+template <int TMG>
+int launch_emm_tile(dim3 grid, const uint32_t* X, const uint32_t* Y, uint32_t* dst, int M, int N,
+                    int K, int ldy, int mode, const EmmGeometry& g, size_t stride,
+                    const grid_gpu_plan* p, cudaStream_t s) {
+  static int bps_cache[kMaxDevices] = {};
+  int bps = 0;
+  const int rc = prepare_kernel(emm_kernel<TMG>, EmmTile<TMG>::SMEM, kEmmThreads, p->device,
+                                bps_cache, &bps);
+  if (rc) return rc;
+  emm_kernel<TMG><<<grid, kEmmThreads, EmmTile<TMG>::SMEM, s>>>(
+      X, Y, dst, M, N, K, ldy, (int)p->d, mode, g.k_per_split, stride, p->f);
+  return GRID_OK;
 }
 
 }  // namespace
 
 size_t emm_workspace_words(const grid_gpu_plan* p, int M, int N, int K, int mode) {
-  const int tiles = ((M + BM - 1) / BM) * ((N + BN - 1) / BN);
-  const int ctas = (int)(p->d / EG) * tiles;
-  const int splits = choose_splits(ctas, K, p->num_sms);
+  if (M <= 0 || N <= 0 || K <= 0 || p->d % EG) return 0;
+  const EmmGeometry g = emm_geometry(M, N, K, (int)p->d, mode, p->num_sms);
   const size_t outputs = mode == OUT_UPPER ? (size_t)M * (M + 1) / 2 : (size_t)M * N;
-  return splits > 1 ? (size_t)splits * outputs * p->d : 0;
+  return g.splits > 1 ? (size_t)g.splits * outputs * p->d : 0;
 }
 
 // out_evals: dense [M][N][d] or packed-upper [M(M+1)/2][d]. work: >= emm_workspace_words.
@@ -159,18 +243,17 @@ int launch_emm(const grid_gpu_plan* p, const uint32_t* X, const uint32_t* Y, int
                int ldy, int mode, uint32_t* out_evals, uint32_t* work, cudaStream_t s) {
   if (M <= 0 || N <= 0 || K <= 0) return GRID_OK;
   if (p->d % EG) return GRID_ERR_UNSUPPORTED_DEGREE;
-  const int tiles_m = (M + BM - 1) / BM, tiles_n = (N + BN - 1) / BN;
-  const int ctas = (int)(p->d / EG) * tiles_m * tiles_n;
-  const int splits = choose_splits(ctas, K, p->num_sms);
-  int kps = (K + splits - 1) / splits;
-  kps = (kps + KC - 1) / KC * KC;
+  if (mode == OUT_UPPER && M != N) return GRID_ERR_DIMENSION_MISMATCH;
+  const EmmGeometry g = emm_geometry(M, N, K, (int)p->d, mode, p->num_sms);
+  const int splits = g.splits;
   const size_t outputs = mode == OUT_UPPER ? (size_t)M * (M + 1) / 2 : (size_t)M * N;
   const size_t stride = outputs * p->d;
-  dim3 grid(p->d / EG, tiles_m * tiles_n, splits);
+  dim3 grid(p->d / EG, g.tiles, splits);
   uint32_t* dst = splits > 1 ? work : out_evals;
   if (splits > 1 && !work) return GRID_ERR_NULL_POINTER;
-  emm_kernel<<<grid, kEmmThreads, 0, s>>>(X, Y, dst, M, N, K, ldy, (int)p->d, mode, kps, stride,
-                                          p->f);
+  int rc = g.tmg == 16 ? launch_emm_tile<16>(grid, X, Y, dst, M, N, K, ldy, mode, g, stride, p, s)
+                       : launch_emm_tile<8>(grid, X, Y, dst, M, N, K, ldy, mode, g, stride, p, s);
+  if (rc) return rc;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_status(e);
   if (splits > 1) {

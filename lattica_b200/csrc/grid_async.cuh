@@ -118,6 +118,34 @@ __device__ __forceinline__ void bulk_wait_all() {
   asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
 }
 
+// Per-thread 16-byte global -> shared copy (L2 only); src_bytes < 16 zero-fills
+// the rest (0 reads nothing). Both addresses 16-byte aligned.
+__device__ __forceinline__ void cp_async16(void* dst_smem, const void* src_gmem,
+                                           uint32_t src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_addr(dst_smem)),
+               "l"(src_gmem), "r"(src_bytes)
+               : "memory");
+}
+
+// Per-thread 8-byte global -> shared copy (through L1); src_bytes < 8 zero-fills
+// the rest. Both addresses 8-byte aligned.
+__device__ __forceinline__ void cp_async8(void* dst_smem, const void* src_gmem,
+                                          uint32_t src_bytes) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(smem_addr(dst_smem)),
+               "l"(src_gmem), "r"(src_bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+// Wait until at most N of this thread's committed copy groups are pending.
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // Order generic-proxy shared-memory accesses before later async-proxy (TMA) accesses.
 __device__ __forceinline__ void fence_proxy_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");

@@ -113,19 +113,22 @@ __device__ __forceinline__ uint32_t to_mont(uint32_t v, const FieldParams& f) {
 
 // 96-bit accumulator for sums of 64-bit products: acc += a*b.
 struct Acc96 {
-  uint64_t lo;   // bits 0..63
-  uint32_t w2;   // bits 64..95
+  uint32_t w0, w1, w2;  // bits 0..31, 32..63, 64..95
 };
 
 __device__ __forceinline__ void acc96_zero(Acc96& a) {
-  a.lo = 0;
+  a.w0 = 0;
+  a.w1 = 0;
   a.w2 = 0;
 }
 
+// One carry chain: w0 += lo(a*b), w1 += hi(a*b) + carry, w2 += carry.
 __device__ __forceinline__ void acc96_mad(Acc96& acc, uint32_t a, uint32_t b) {
-  const uint64_t p = (uint64_t)a * b;
-  acc.lo += p;
-  acc.w2 += acc.lo < p ? 1u : 0u;
+  asm("mad.lo.cc.u32 %0, %3, %4, %0;\n\t"
+      "madc.hi.cc.u32 %1, %3, %4, %1;\n\t"
+      "addc.u32 %2, %2, 0;"
+      : "+r"(acc.w0), "+r"(acc.w1), "+r"(acc.w2)
+      : "r"(a), "r"(b));
 }
 
 // Reduce V = w2*2^64 + w1*2^32 + w0 to V * 2^-32 mod q (canonical).
@@ -133,7 +136,7 @@ __device__ __forceinline__ void acc96_mad(Acc96& acc, uint32_t a, uint32_t b) {
 // sum(a_k*b_k) * 2^-32 = sum(mont_mul(a_k, b_k)) mod q.
 // Requires w2 < 2^32 (at most 2^32 products of words < 2^32).
 __device__ __forceinline__ uint32_t acc96_reduce(const Acc96& acc, const FieldParams& f) {
-  const uint32_t w0 = (uint32_t)acc.lo, w1 = (uint32_t)(acc.lo >> 32);
+  const uint32_t w0 = acc.w0, w1 = acc.w1;
   // Low 64 bits: (w1*2^32 + w0) * 2^-32 = w1 - hi(m*q) with m = w0*q^-1.
   const uint32_t m = w0 * f.qinv;
   const uint32_t u = __umulhi(m, f.q);
