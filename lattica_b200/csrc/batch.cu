@@ -50,7 +50,7 @@ struct WorkDev {
   uint32_t tile, k0, k1, eg;
 };
 
-__global__ void __launch_bounds__(kThreads, 2) batch_emm_kernel(
+__global__ void __launch_bounds__(kThreads) batch_emm_kernel(
     const WorkDev* __restrict__ work, unsigned nwork, const TileDev* __restrict__ tiles,
     const ItemDev* __restrict__ items, const MatDev* __restrict__ mats,
     const uint32_t* __restrict__ s_hat, unsigned long long* __restrict__ acc,

@@ -15,8 +15,8 @@
 // is d independent dense modular matmuls, one per evaluation point e:
 //     out_e[m][n] = sum_k X[m][k][e] * Y[n][k][e]   (mod q, Montgomery)
 // Kernel "emm": a CTA owns 8 consecutive evaluation points (one 32-byte
-// sector per (row, k)), a 32 x 32 output tile and a K range; operands are
-// staged through shared memory in 16-deep K chunks; each thread keeps a 4 x 8
+// sector per (row, k)), a 32 x 32 (or 64 x 16) output tile and a K range;
+// operands stream through shared memory in 16-deep K chunks; each thread keeps a 4 x 8
 // register tile of exact 96-bit accumulators (64-bit product added to a 64-bit
 // sum, carries counted in a third word) and reduces once at the end.
 // Partial sums of a K split are canonical residues, so splits add exactly.
@@ -46,8 +46,7 @@ struct EmmTile {
   static constexpr int TNG = 32 / TMG;
   static constexpr int BM = 4 * TMG, BN = 8 * TNG;
   static constexpr int STAGE_WORDS = (BM + BN) * RS;
-  // Three stages where two CTAs per SM still fit in shared memory, else two.
-  static constexpr int STAGES = 3 * STAGE_WORDS * 4 <= 100 * 1024 ? 3 : 2;
+  static constexpr int STAGES = 3;
   static constexpr size_t SMEM = (size_t)STAGES * STAGE_WORDS * 4;
 };
 
@@ -56,11 +55,12 @@ struct EmmTile {
 // row-major order (garbage_index).
 // With splits > 1 the CTA of split s writes to out + s * split_stride.
 // Operands stream through a cp.async ring of STAGES chunks (X rows, then Y
-// rows, each in global order: [k][e]); two CTAs per SM. A warp covers 8
+// rows, each in global order: [k][e]); one CTA per SM, so the 4 x 8 tile of
+// 96-bit accumulators stays in registers without spilling. A warp covers 8
 // evaluation points x 4 consecutive row groups of X, so its X reads hit 32
 // distinct banks and its Y reads are broadcasts.
 template <int TMG>
-__global__ void __launch_bounds__(kEmmThreads, 2) emm_kernel(
+__global__ void __launch_bounds__(kEmmThreads, 1) emm_kernel(
     const uint32_t* __restrict__ X, const uint32_t* __restrict__ Y, uint32_t* __restrict__ out,
     int M, int N, int K, int ldy, int d, int mode, int k_per_split, size_t split_stride,
     FieldParams f) {
@@ -142,7 +142,7 @@ __global__ void __launch_bounds__(kEmmThreads, 2) emm_kernel(
     cp_async_commit();
     const uint32_t* xs = emm_smem + (c % STAGES) * SW + xo;
     const uint32_t* ys = emm_smem + (c % STAGES) * SW + yo;
-#pragma unroll 4
+#pragma unroll
     for (int kk = 0; kk < KC; ++kk) {
       uint32_t xr[4], yr[8];
 #pragma unroll
@@ -195,7 +195,7 @@ struct EmmGeometry {
 };
 
 // The K range is split so that all CTAs fit one wave of the resident slots
-// (2 CTAs per SM), each split a whole number of 16-step chunks and at least
+// (one CTA per SM), each split a whole number of 16-step chunks and at least
 // two of them; split partials go to the workspace and are summed after.
 EmmGeometry emm_geometry(int M, int N, int K, int d, int mode, int num_sms) {
   EmmGeometry g;
@@ -205,7 +205,7 @@ EmmGeometry emm_geometry(int M, int N, int K, int d, int mode, int num_sms) {
   g.tiles_n = (N + bn - 1) / bn;
   g.tiles = mode == OUT_UPPER ? g.tiles_m * (g.tiles_m + 1) / 2 : g.tiles_m * g.tiles_n;
   const long long ctas = (long long)(d / EG) * g.tiles;
-  const long long slots = 2LL * num_sms;
+  const long long slots = num_sms;
   const int chunks = (K + KC - 1) / KC;
   long long want = ctas >= slots ? 1 : slots / ctas;
   if (want > chunks / 2) want = chunks / 2 > 1 ? chunks / 2 : 1;
