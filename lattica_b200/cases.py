@@ -1,0 +1,78 @@
+"""Standalone runs of the hot-path workloads at their benchmark sizes, for
+profilers and quick timing: each case builds its seeded inputs on cuda:0,
+runs the operation `--reps` times through the public Python API and prints
+the median CUDA-event time.
+
+    python -m lattica_b200.cases round --reps 24     # LaBRADOR prover round
+    python -m lattica_b200.cases gram --reps 4       # r x r Gram, r = 64, n = 2048
+    python -m lattica_b200.cases commit --reps 4     # 16 x 2048 matrix times 64 witnesses
+    python -m lattica_b200.cases ntt256 --reps 4     # d = 256 products, 2^20 polys at q'
+
+Sizes: r = 64 witness vectors of n = 2048 polys (d = 64, coefficients in
+[-2^11, 2^11], as Montgomery words), kappa = 16, JL 256 rows, base 2^8 x 4
+limbs; q = 4294966657 (q' = 4294962689 for d = 256)."""
+import argparse
+import statistics
+
+Q = 4294966657
+Q256 = 4294962689
+
+
+def _witness(torch, dev, g, q, shape):
+    coeffs = torch.randint(-2048, 2049, shape, dtype=torch.int64, device=dev, generator=g) % q
+    return ((coeffs * ((1 << 32) % q)) % q).to(torch.int32)
+
+
+def _uniform(torch, dev, g, q, shape):
+    return torch.randint(0, q, shape, dtype=torch.int64, device=dev, generator=g).to(torch.int32)
+
+
+def build(case: str):
+    """Returns a zero-argument callable that runs one instance of `case`."""
+    import torch
+    from lattica_b200 import TwistedNttPlan
+    from lattica_b200.labrador import CommitKey, compute_garbage_g, prover_round_dev
+    dev = torch.device("cuda:0")
+    g = torch.Generator(device=dev).manual_seed(5)
+    r, n, kappa = 64, 2048, 16
+    if case == "ntt256":
+        plan = TwistedNttPlan(Q256, 256)
+        a = _uniform(torch, dev, g, Q256, (1 << 20, 256))
+        b = _uniform(torch, dev, g, Q256, (1 << 20, 256))
+        return lambda: plan.ntt_mul_inverse(a, b)
+    plan = TwistedNttPlan(Q, 64)
+    wit = _witness(torch, dev, g, Q, (r, n, 64))
+    if case == "gram":
+        return lambda: compute_garbage_g(plan, wit)
+    key = CommitKey(plan, _uniform(torch, dev, g, Q, (kappa, n, 64)), kappa, n)
+    if case == "commit":
+        return lambda: key.inner_commit_slice(wit)
+    if case == "round":
+        seed = bytes(range(32))
+        return lambda: prover_round_dev(key, wit, 256, 4, 256, 4, seed, 256)
+    raise ValueError(f"unknown case {case!r}")
+
+
+def main(argv=None) -> None:
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    ap.add_argument("case", choices=["round", "gram", "commit", "ntt256"])
+    ap.add_argument("--reps", type=int, default=4)
+    args = ap.parse_args(argv)
+    import torch
+    fn = build(args.case)
+    fn()
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(args.reps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        e1.record()
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    print(f"{args.case}: {len(times)} runs, median {statistics.median(times):.4f} ms")
+
+
+if __name__ == "__main__":
+    main()

@@ -59,8 +59,9 @@ struct grid_gpu_plan {
   grid::TwiddleTable tw;
   // Device copy of the twiddle table as uint2 {w, wq}: fw[d], iw[d], {ninv}, {izeta1*ninv}.
   uint2* d_tw = nullptr;
-  // d = 64: byte planes of the Montgomery-form forward / inverse matrices for
-  // the tensor-core transform (2 x 16 KB); null selects the CUDA-core kernels.
+  // Tensor-core tables. d = 64: byte planes of the Montgomery-form forward /
+  // inverse matrices (2 x 64 KB). d = 256: the 64-point matrix (64 KB) and the
+  // twist constants of the products. Null selects the CUDA-core kernels.
   void* d_tcw = nullptr;
   int* d_err = nullptr;
   cudaStream_t stream = nullptr;   // host-buffer entry points: first pipeline stream
@@ -90,6 +91,11 @@ int launch_ntt_tc(const grid_gpu_plan* p, int mode, const uint32_t* a, const uin
                   uint32_t* out, size_t npolys, cudaStream_t s);
 void build_tc_tables(uint32_t q, uint32_t d, uint64_t psi, uint64_t ninv,
                      std::vector<unsigned char>& out);
+// ntt256_tc.cu (d = 256 products, tcgen05)
+bool ntt256_tc_available(const grid_gpu_plan* p);
+int launch_ntt256_tc(const grid_gpu_plan* p, const uint32_t* a, const uint32_t* b, uint32_t* out,
+                     size_t npolys, cudaStream_t s);
+void build_tc256_tables(uint32_t q, uint64_t psi, std::vector<unsigned char>& out);
 
 // commit.cu: out_e[m][n] = sum_k X[m][k][e] * Y[n][k][e] for every evaluation point.
 enum EmmOut : int { EMM_DENSE = 0, EMM_UPPER = 1 };

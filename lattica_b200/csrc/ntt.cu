@@ -558,6 +558,8 @@ int launch_ntt(const grid_gpu_plan* p, int mode, const uint32_t* a, const uint32
                uint32_t* out, size_t npolys, cudaStream_t s) {
   if (npolys == 0) return GRID_OK;
   if (ntt_tc_available(p)) return launch_ntt_tc(p, mode, a, b, out, npolys, s);
+  if (mode == MODE_MULINV && ntt256_tc_available(p))
+    return launch_ntt256_tc(p, a, b, out, npolys, s);
   switch (mode) {
     case MODE_FWD: return dispatch<MODE_FWD>(p, a, nullptr, out, npolys, s);
     case MODE_INV: return dispatch<MODE_INV>(p, a, nullptr, out, npolys, s);

@@ -419,9 +419,12 @@ int grid_gpu_plan_create(uint64_t q, uint64_t d, grid_gpu_plan** out) {
     if ((e = cudaMalloc(&p->d_tw, dev_tw.size() * sizeof(uint2))) != cudaSuccess) break;
     if ((e = cudaMemcpy(p->d_tw, dev_tw.data(), dev_tw.size() * sizeof(uint2),
                         cudaMemcpyHostToDevice)) != cudaSuccess) break;
-    if (d == 64 && use_tensor_cores()) {
+    if ((d == 64 || d == 256) && use_tensor_cores()) {
       std::vector<unsigned char> tcw;
-      build_tc_tables(p->q, p->d, p->psi_value, p->n_inv_value, tcw);
+      if (d == 64)
+        build_tc_tables(p->q, p->d, p->psi_value, p->n_inv_value, tcw);
+      else
+        build_tc256_tables(p->q, p->psi_value, tcw);
       if ((e = cudaMalloc(&p->d_tcw, tcw.size())) != cudaSuccess) break;
       if ((e = cudaMemcpy(p->d_tcw, tcw.data(), tcw.size(), cudaMemcpyHostToDevice)) !=
           cudaSuccess)
