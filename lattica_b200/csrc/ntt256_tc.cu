@@ -19,15 +19,16 @@
 // is the same matrix read at output column j' = -b mod 64, and
 //   out_{64 a + b} = sum_j1 zeta^(-a (2 j1 + 1)) 256^-1 psi^(-(2 j1 + 1) b) V_{j1}[b].
 // One matrix in shared memory serves both directions, which leaves room for
-// three input buffers.
+// two input buffers and a staged tile of b.
 //
 // A tile is 32 polynomials = 128 rows (row 32 j1 + p), so epilogue warp w
 // (tensor-memory lanes 32 (w % 4) ..) holds block j1 = w % 4 of every
 // polynomial. Per tile j of a CTA (one persistent CTA per SM):
-//   loader (warp 17): bulk-loads input tile j into buffer j % 3 once output
-//     tile j - 3 has been stored from it; L2 prefetch of a and b 3 tiles ahead
+//   loader (warp 17): bulk-loads input tile j into buffer j % 2 once output
+//     tile j - 2 has been stored from it, and b's tile j into padded rows once
+//     F(j-1) has read the previous one; L2 prefetch of a and b 3 tiles ahead
 //   epilogue (warps 0-15): P(j) 4-point + twist -> forward A operand;
-//     E(j-1) inverse results -> 4-point inverse in buffer (j-1) % 3 -> staged;
+//     E(j-1) inverse results -> 4-point inverse in buffer (j-1) % 2 -> staged;
 //     F(j) forward results (x) b -> inverse A operand
 //   MMA (warp 16): fwd(j) after P(j) and F(j-1) read columns 0-255;
 //     inv(j) after F(j) and E(j-1) read columns 256-511.
@@ -52,15 +53,18 @@ using namespace tcx;
 constexpr int D = 256;
 constexpr int PT = ROWS / 4;                // polys per tile
 constexpr int EPI_THREADS = EPI_WARPS * 32;
-constexpr int NX = 3;                       // natural-order tile buffers
+constexpr int NX = 2;                       // natural-order tile buffers
 constexpr uint32_t XT = PT * D * 4;         // 32 KB
+// b rows padded to 260 words: the 32 rows of one gather start 4 banks apart
+constexpr uint32_t BROW = (D + 4) * 4;
 
 // Offsets from the 1 KB-aligned base of dynamic shared memory.
 constexpr uint32_t OFF_W = 0;               // the 64-point matrix (B of both transforms)
 constexpr uint32_t OFF_AF = OFF_W + WMAT;   // forward A operand
 constexpr uint32_t OFF_AI = OFF_AF + TILE;  // inverse A operand (pointwise products)
 constexpr uint32_t OFF_X = OFF_AI + TILE;   // input tiles, then inverse results
-constexpr uint32_t OFF_BAR = OFF_X + NX * XT;
+constexpr uint32_t OFF_B = OFF_X + NX * XT;  // b's tile, padded rows
+constexpr uint32_t OFF_BAR = OFF_B + PT * BROW;
 constexpr uint32_t OFF_TADDR = OFF_BAR + 16 * 8;
 constexpr uint32_t SMEM_BYTES = OFF_TADDR + 16 + 1024;  // + alignment slack
 static_assert(SMEM_BYTES <= 232448, "shared memory budget");
@@ -77,7 +81,9 @@ constexpr size_t TABLE_BYTES = WMAT + (256 + 256 + 8) * 8;
 enum Bar : int {
   AFULL0 = 0,               // input tile landed in buffer i
   STAGED0 = AFULL0 + NX,    // output tile written into buffer i
-  PREP = STAGED0 + NX, FDONE, FREAD, PREADY, IDONE, EREAD, NBARS
+  BFULL = STAGED0 + NX,     // b's tile landed
+  BFREE,                    // F has read b's tile
+  PREP, FDONE, FREAD, PREADY, IDONE, EREAD, NBARS
 };
 static_assert(NBARS <= 16, "barrier slots");
 
@@ -128,6 +134,8 @@ __global__ void __launch_bounds__(THREADS, 1)
         mbar_init(&bars[AFULL0 + i], 1);
         mbar_init(&bars[STAGED0 + i], EPI_WARPS);
       }
+      mbar_init(&bars[BFULL], 1);
+      mbar_init(&bars[BFREE], EPI_WARPS);
       mbar_init(&bars[PREP], EPI_WARPS);
       mbar_init(&bars[FDONE], 1);
       mbar_init(&bars[FREAD], EPI_WARPS);
@@ -158,7 +166,7 @@ __global__ void __launch_bounds__(THREADS, 1)
 
   if (warp == LOAD_WARP) {
     // ------------------------------------------------------------ loader
-    uint32_t armed[NX] = {};
+    uint32_t armed[NX] = {}, barmed = 0;
     bool ok = true;
     auto prefetch = [&](uint32_t j) {
       if (lane == 0 && j < n) {
@@ -166,11 +174,11 @@ __global__ void __launch_bounds__(THREADS, 1)
         prefetch_l2(b + poly0(j) * D, tile_bytes(j));
       }
     };
-    for (uint32_t j = 0; j < (uint32_t)NX; ++j) prefetch(j);
+    for (uint32_t j = 0; j < 3; ++j) prefetch(j);
     for (uint32_t t = 0; ok && t < n + NX; ++t) {
       const uint32_t buf = t % NX;
       unsigned char* xb = sm + OFF_X + buf * XT;
-      if (t >= (uint32_t)NX) {  // store output tile t - 3, which frees the buffer
+      if (t >= (uint32_t)NX) {  // store output tile t - 2, which frees the buffer
         const uint32_t js = t - NX;
         ok = warp_wait_fast(&bars[STAGED0 + buf], (js / NX) & 1, err);
         if (ok && lane == 0) {
@@ -187,13 +195,25 @@ __global__ void __launch_bounds__(THREADS, 1)
           bulk_load(xb, a + poly0(t) * D, tile_bytes(t), &bars[AFULL0 + buf]);
         }
         __syncwarp();
+        // b's tile t, one row per lane, once F(t-1) has read tile t-1
+        if (t >= 1) ok = warp_wait_fast(&bars[BFREE], (t - 1) & 1, err);
+        if (ok) {
+          ++barmed;
+          if (lane == 0) mbar_arrive_expect_tx(&bars[BFULL], tile_bytes(t));
+          __syncwarp();
+          if ((uint32_t)lane * D * 4 < tile_bytes(t))
+            bulk_load(sm + OFF_B + lane * BROW, b + (poly0(t) + lane) * D, D * 4, &bars[BFULL]);
+          __syncwarp();
+        }
       }
-      prefetch(t + NX);
+      prefetch(t + 3);
     }
     if (lane == 0) bulk_wait_all();
-    if (!ok)
+    if (!ok) {
       for (int i = 0; i < NX; ++i)
         if (armed[i]) mbar_wait_sleep(&bars[AFULL0 + i], (armed[i] - 1) & 1, err);
+      if (barmed) mbar_wait_sleep(&bars[BFULL], (barmed - 1) & 1, err);
+    }
   } else if (warp == MMA_WARP) {
     // ------------------------------------------------------------ MMA issue
     uint32_t armed[NBARS] = {};
@@ -233,29 +253,27 @@ __global__ void __launch_bounds__(THREADS, 1)
     const int tid = threadIdx.x;  // 0 .. 511
     const uint32_t q = k.q;
     bool ok = true;
-    uint32_t bv[16];
+    // The 4-point steps give this thread coefficient / slot index bb = tid % 64
+    // of polynomials tid / 64 + 8 it: its twists are fixed. Montgomery words
+    // only; the Shoup companions are recomputed at use.
+    const uint32_t bb = tid & 63;
+    uint32_t twf[4], twi[4];
+#pragma unroll
+    for (int j1 = 0; j1 < 4; ++j1) {
+      twf[j1] = tw[TW_F + 64 * j1 + bb].x;
+      twi[j1] = tw[TW_I + 64 * j1 + bb].x;
+    }
+    const uint2 ci = tw[TW_C + 0], cz = tw[TW_C + 1], cz3 = tw[TW_C + 2];
+    const uint2 czi1 = tw[TW_C + 3], czi2 = tw[TW_C + 4], czi3 = tw[TW_C + 5];
+    auto mulw = [&](uint32_t x, uint32_t w) { return mont_c(x, w, w * k.qinv, q); };
 
-    // b at slots 4 (16 cq + t) + wl of this row's polynomial of tile j
-    auto load_b = [&](uint32_t j) {
-      const unsigned long long r = j < n ? poly0(j) + p : npolys;
-      if (r < npolys) {
-        const uint32_t* src = b + r * D + 64 * cq + wl;
-#pragma unroll
-        for (int t = 0; t < 16; ++t) bv[t] = __ldg(src + 4 * t);
-      } else {
-#pragma unroll
-        for (int t = 0; t < 16; ++t) bv[t] = 0;
-      }
-    };
-    // P(j): Y_{j1}[b] for 4 (polynomial, b) items per thread, into the forward A operand
+    // P(j): Y_{j1}[bb] for 4 polynomials per thread, into the forward A operand
     auto prep = [&](uint32_t j) {
       const uint32_t* x = reinterpret_cast<const uint32_t*>(sm + OFF_X + (j % NX) * XT);
       unsigned char* af = sm + OFF_AF;
-      const uint2 ci = tw[TW_C + 0], cz = tw[TW_C + 1], cz3 = tw[TW_C + 2];
 #pragma unroll
       for (int it = 0; it < 4; ++it) {
-        const int u = it * EPI_THREADS + tid;
-        const uint32_t bb = u & 63, pp = u >> 6;
+        const uint32_t pp = (it * EPI_THREADS + tid) >> 6;
         const uint32_t* xr = x + pp * D + bb;
         const uint32_t x0 = xr[0], x1 = xr[64], x2 = xr[128], x3 = xr[192];
         const uint32_t t2 = mulc(x2, ci, q), t3 = mulc(x3, ci, q);  // zeta^2 x2, zeta^2 x3
@@ -269,7 +287,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         z[3] = sub_lazy(e1, s1, q);   // j1 = 3: zeta^(7a)
 #pragma unroll
         for (int j1 = 0; j1 < 4; ++j1) {
-          const uint32_t y = mulc(z[j1], __ldg(tw + TW_F + 64 * j1 + bb), q);
+          const uint32_t y = mulw(z[j1], twf[j1]);
           *reinterpret_cast<uint32_t*>(af + sw128(32 * j1 + pp, bb >> 5, (bb & 31) >> 2, BOX) +
                                        4 * (bb & 3)) = y;
         }
@@ -277,13 +295,22 @@ __global__ void __launch_bounds__(THREADS, 1)
     };
     // F(j): forward results (x) b -> inverse A operand
     auto forward_out = [&](uint32_t j) -> bool {
-      if (!epi_all(warp_wait_fast(&bars[FDONE], j & 1, err))) return false;
+      bool got = warp_wait_fast(&bars[FDONE], j & 1, err);
+      got = got && warp_wait_fast(&bars[BFULL], j & 1, err);
+      if (!epi_all(got)) return false;
       tc::fence_after_sync();
       uint32_t res[16];
       reduce16(R0 + lane_off, k, res);
       tc::fence_before_sync();
       __syncwarp();
       if (lane == 0) mbar_arrive(&bars[FREAD]);  // columns 0-255 free for fwd(j+1)
+      // b at slots 4 (16 cq + t) + wl of polynomial p
+      const uint32_t* brow = reinterpret_cast<const uint32_t*>(sm + OFF_B + p * BROW) + 64 * cq + wl;
+      uint32_t bv[16];
+#pragma unroll
+      for (int t = 0; t < 16; ++t) bv[t] = brow[4 * t];
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&bars[BFREE]);
 #pragma unroll
       for (int t = 0; t < 16; ++t) res[t] = redc64(mad_wide(res[t], bv[t], 0ull), q, k.qinv);
       unsigned char* ai = sm + OFF_AI;
@@ -306,25 +333,22 @@ __global__ void __launch_bounds__(THREADS, 1)
       __syncwarp();
       if (lane == 0) mbar_arrive(&bars[EREAD]);  // columns 256-511 free for inv(j+1)
       uint32_t* x = reinterpret_cast<uint32_t*>(sm + OFF_X + (j % NX) * XT);
-      // column 16 cq + t is V_{wl}[b] with b = -(16 cq + t) mod 64; word 64 wl + b of
+      // column 16 cq + t is V_{wl}[c] with c = -(16 cq + t) mod 64; word 64 wl + c of
       // polynomial p, its low 5 bits XORed with p (the 32 lanes hit 32 banks)
 #pragma unroll
       for (int t = 0; t < 16; ++t) {
-        const uint32_t bb = (64u - (16u * cq + t)) & 63u;
-        x[p * D + ((64 * wl + bb) ^ p)] = res[t];
+        const uint32_t c = (64u - (16u * cq + t)) & 63u;
+        x[p * D + ((64 * wl + c) ^ p)] = res[t];
       }
       epi_sync();
-      const uint2 czi1 = tw[TW_C + 3], czi2 = tw[TW_C + 4], czi3 = tw[TW_C + 5];
       uint32_t o[4][4];
 #pragma unroll
       for (int it = 0; it < 4; ++it) {
-        const int u = it * EPI_THREADS + tid;
-        const uint32_t bb = u & 63, pp = u >> 6;
+        const uint32_t pp = (it * EPI_THREADS + tid) >> 6;
         const uint32_t* xr = x + pp * D;
         uint32_t v[4];
 #pragma unroll
-        for (int j1 = 0; j1 < 4; ++j1)
-          v[j1] = mulc(xr[(64 * j1 + bb) ^ pp], __ldg(tw + TW_I + 64 * j1 + bb), q);
+        for (int j1 = 0; j1 < 4; ++j1) v[j1] = mulw(xr[(64 * j1 + bb) ^ pp], twi[j1]);
         const uint32_t p0 = add_canon(v[0], v[2], q), q0 = sub_lazy(v[0], v[2], q);
         const uint32_t p1 = add_canon(v[1], v[3], q), q1 = sub_lazy(v[1], v[3], q);
         const uint32_t tq = mulc(q1, czi2, q);
@@ -336,8 +360,7 @@ __global__ void __launch_bounds__(THREADS, 1)
       epi_sync();  // every swizzled word read before the tile is rewritten in order
 #pragma unroll
       for (int it = 0; it < 4; ++it) {
-        const int u = it * EPI_THREADS + tid;
-        const uint32_t bb = u & 63, pp = u >> 6;
+        const uint32_t pp = (it * EPI_THREADS + tid) >> 6;
 #pragma unroll
         for (int aa = 0; aa < 4; ++aa) x[pp * D + 64 * aa + bb] = o[it][aa];
       }
@@ -347,7 +370,6 @@ __global__ void __launch_bounds__(THREADS, 1)
       return true;
     };
 
-    if (n > 0) load_b(0);
     for (uint32_t j = 0; ok && j < n; ++j) {
       ok = epi_all(warp_wait_fast(&bars[AFULL0 + j % NX], (j / NX) & 1, err));
       if (!ok) break;
@@ -357,7 +379,6 @@ __global__ void __launch_bounds__(THREADS, 1)
       if (lane == 0) mbar_arrive(&bars[PREP]);
       if (j >= 1 && !(ok = inverse_out(j - 1))) break;  // also frees the inverse A operand
       if (!(ok = forward_out(j))) break;
-      load_b(j + 1);
     }
     if (ok && n > 0) inverse_out(n - 1);
   }
