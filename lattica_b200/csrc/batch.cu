@@ -5,7 +5,8 @@
 // columns of its matrix, e.g. one matrix per rank m) run as one sequence:
 //   1. one NTT of every witness polynomial (packed s buffer -> s_hat),
 //   2. a persistent grouped evaluation-domain matmul: instances are grouped by
-//      matrix and sorted by length into tiles of 32; a work item is (tile,
+//      matrix and sorted by length into tiles (32 to 128 instances, by the
+//      matrix's rows); a work item is (tile,
 //      8 evaluation points, K range); CTAs pull work items from an atomic
 //      counter and add canonical partial sums into 64-bit accumulators,
 //   3. a fold of the accumulators mod q and one INTT of every output.
@@ -25,15 +26,33 @@
 #include <tuple>
 #include <vector>
 
+#include "grid_async.cuh"
 #include "grid_field.cuh"
 #include "grid_internal.h"
 
 namespace grid {
 namespace {
 
-constexpr int TM = 32, TN = 32, EG = 8, KC = 16, PAD = 4;
-constexpr int ROW = TM + PAD;
+constexpr int TN = 32, EG = 8, KC = 16;
+constexpr int RS = KC * EG + 2;  // words per staged row (padded: rows 4 apart, 8 banks apart)
 constexpr int kThreads = 256;
+
+// Tile shapes: TMG groups of 4 instances by (32 / TMG) groups of 8 matrix
+// rows, for 8 evaluation points; each thread keeps one evaluation point of a
+// 4 x 8 sub-tile. A matrix of <= 8 rows takes 128-instance tiles, <= 16 rows
+// 64-instance tiles, up to 32 rows 32-instance tiles, so no tile multiplies
+// padding rows of a short matrix.
+template <int TMG>
+struct BTile {
+  static constexpr int BM = 4 * TMG, BN = 8 * (32 / TMG);
+  static constexpr int ROWS = BM + BN;
+  static constexpr int STAGES = ROWS <= 80 ? 3 : 2;
+  static constexpr size_t SMEM = (size_t)STAGES * ROWS * RS * 4;
+};
+constexpr int kMaxTileInstances = BTile<32>::BM;
+constexpr size_t kBatchSmem = std::max({BTile<8>::SMEM, BTile<16>::SMEM, BTile<32>::SMEM});
+
+__host__ __device__ constexpr int tile_tmg(uint32_t rows) { return rows <= 8 ? 32 : rows <= 16 ? 16 : 8; }
 
 struct MatDev {
   const uint32_t* evals;
@@ -44,23 +63,113 @@ struct ItemDev {
   uint32_t n, pad;
 };
 struct TileDev {
-  uint32_t first, count, matrix, kmax;
+  uint32_t first, count, matrix, kmax;  // count <= 4 * tile_tmg(rows of the matrix)
 };
 struct WorkDev {
   uint32_t tile, k0, k1, eg;
 };
 
-__global__ void __launch_bounds__(kThreads) batch_emm_kernel(
+// One work item (a tile, evaluation points 8 eg .. + 7, K steps k0 .. k1) with
+// tile shape TMG: operands stream through a cp.async ring (instances' witness
+// evaluations, then the matrix rows, each row 16 K steps x 8 points in global
+// order), 96-bit accumulators, canonical partial sums added into acc.
+template <int TMG>
+__device__ __forceinline__ void batch_item(const WorkDev& wk, const TileDev& tile,
+                                           const MatDev& mat, const ItemDev* sitems,
+                                           const uint32_t* __restrict__ s_hat,
+                                           unsigned long long* __restrict__ acc, int d,
+                                           const FieldParams& f, uint32_t* smem) {
+  using Tl = BTile<TMG>;
+  constexpr int BM = Tl::BM, BN = Tl::BN, STAGES = Tl::STAGES, SW = Tl::ROWS * RS;
+  const int t = threadIdx.x;
+  const int eg = t & 7, tm = (t >> 3) % TMG, tn = (t >> 3) / TMG;
+  const int e0 = wk.eg * EG;
+  const int nchunks = (int)((wk.k1 - wk.k0 + KC - 1) / KC);
+  // this thread copies quarter t & 3 of step (t >> 2) & 15 of rows (t >> 6) + 4i
+  const int cq = t & 3, ck = (t >> 2) & (KC - 1), cr = t >> 6;
+  const int cdst = cr * RS + ck * EG + 2 * cq;
+
+  auto issue = [&](int c) {
+    uint32_t* st = smem + (c % STAGES) * SW + cdst;
+    const uint32_t k = wk.k0 + (uint32_t)(c * KC + ck);
+    const bool kval = k < wk.k1;
+#pragma unroll
+    for (int i = 0; i < BM / 4; ++i) {
+      const int row = cr + 4 * i;
+      const ItemDev& it = sitems[row];
+      const bool valid = kval && (uint32_t)row < tile.count && k < it.n;
+      const uint32_t* src = valid ? s_hat + (it.s_off + k) * d + e0 + 2 * cq : s_hat;
+      cp_async8(st + 4 * i * RS, src, valid ? 8u : 0u);
+    }
+#pragma unroll
+    for (int i = 0; i < BN / 4; ++i) {
+      const int r = cr + 4 * i;
+      const bool valid = kval && (uint32_t)r < mat.rows;
+      const uint32_t* src =
+          valid ? mat.evals + ((size_t)r * mat.ld + k) * d + e0 + 2 * cq : mat.evals;
+      cp_async8(st + (BM + 4 * i) * RS, src, valid ? 8u : 0u);
+    }
+  };
+
+  Acc96 a[4][8];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc96_zero(a[i][j]);
+  const int xo = (tm * 4) * RS + eg;
+  const int yo = (BM + tn * 8) * RS + eg;
+#pragma unroll
+  for (int c = 0; c < STAGES - 1; ++c) {
+    if (c < nchunks) issue(c);
+    cp_async_commit();
+  }
+  for (int c = 0; c < nchunks; ++c) {
+    cp_async_wait<STAGES - 2>();
+    __syncthreads();  // chunk c landed for every thread; stage (c - 1) % STAGES is free
+    if (c + STAGES - 1 < nchunks) issue(c + STAGES - 1);
+    cp_async_commit();
+    const uint32_t* xs = smem + (c % STAGES) * SW + xo;
+    const uint32_t* ys = smem + (c % STAGES) * SW + yo;
+#pragma unroll
+    for (int kk = 0; kk < KC; ++kk) {
+      uint32_t xr[4], yr[8];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) xr[i] = xs[kk * EG + i * RS];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) yr[j] = ys[kk * EG + j * RS];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc96_mad(a[i][j], xr[i], yr[j]);
+    }
+  }
+  cp_async_wait<0>();
+  const int e = e0 + eg;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int m = tm * 4 + i;
+    if ((uint32_t)m >= tile.count) continue;
+    const unsigned long long t_off = sitems[m].t_off;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int row = tn * 8 + j;
+      if ((uint32_t)row >= mat.rows) continue;
+      atomicAdd(&acc[(t_off + row) * d + e], (unsigned long long)acc96_reduce(a[i][j], f));
+    }
+  }
+}
+
+// Persistent: CTAs pull work items from an atomic counter (longest K ranges
+// first); one CTA per SM keeps the accumulators in registers.
+__global__ void __launch_bounds__(kThreads, 1) batch_emm_kernel(
     const WorkDev* __restrict__ work, unsigned nwork, const TileDev* __restrict__ tiles,
     const ItemDev* __restrict__ items, const MatDev* __restrict__ mats,
     const uint32_t* __restrict__ s_hat, unsigned long long* __restrict__ acc,
     unsigned* __restrict__ counter, int d, FieldParams f) {
-  __shared__ __align__(16) uint32_t Xs[KC * EG * ROW];
-  __shared__ __align__(16) uint32_t Ys[KC * EG * ROW];
-  __shared__ ItemDev sitems[TM];
+  extern __shared__ __align__(16) uint32_t batch_smem[];
+  __shared__ ItemDev sitems[kMaxTileInstances];
   __shared__ unsigned widx;
   const int t = threadIdx.x;
-  const int eg = t & 7, tn = (t >> 3) & 3, tm = t >> 5;
 
   for (;;) {
     if (t == 0) widx = atomicAdd(counter, 1u);
@@ -70,71 +179,18 @@ __global__ void __launch_bounds__(kThreads) batch_emm_kernel(
     const WorkDev wk = work[w];
     const TileDev tile = tiles[wk.tile];
     const MatDev mat = mats[tile.matrix];
-    if (t < TM) {
+    for (int i = t; i < kMaxTileInstances; i += kThreads) {
       ItemDev it = {0, 0, 0, 0};
-      if ((uint32_t)t < tile.count) it = items[tile.first + t];
-      sitems[t] = it;
+      if ((uint32_t)i < tile.count) it = items[tile.first + i];
+      sitems[i] = it;
     }
     __syncthreads();
-    const int e0 = wk.eg * EG;
-
-    Acc96 a[4][8];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-      for (int j = 0; j < 8; ++j) acc96_zero(a[i][j]);
-
-    for (uint32_t k0 = wk.k0; k0 < wk.k1; k0 += KC) {
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const int u = t + kThreads * i;  // (mm, kk, half)
-        const int half = u & 1;
-        const int kk = (u >> 1) & (KC - 1);
-        const int mm = u >> 5;
-        const uint32_t k = k0 + kk;
-        uint4 vx = make_uint4(0, 0, 0, 0), vy = make_uint4(0, 0, 0, 0);
-        if (k < wk.k1) {
-          const ItemDev& it = sitems[mm];
-          if (k < it.n)
-            vx = *reinterpret_cast<const uint4*>(s_hat + (it.s_off + k) * d + e0 + half * 4);
-          if ((uint32_t)mm < mat.rows)
-            vy = *reinterpret_cast<const uint4*>(mat.evals + ((size_t)mm * mat.ld + k) * d + e0 +
-                                                 half * 4);
-        }
-        uint32_t* xs = Xs + (kk * EG + half * 4) * ROW + mm;
-        uint32_t* ys = Ys + (kk * EG + half * 4) * ROW + mm;
-        xs[0] = vx.x; xs[ROW] = vx.y; xs[2 * ROW] = vx.z; xs[3 * ROW] = vx.w;
-        ys[0] = vy.x; ys[ROW] = vy.y; ys[2 * ROW] = vy.z; ys[3 * ROW] = vy.w;
-      }
-      __syncthreads();
-#pragma unroll 4
-      for (int kk = 0; kk < KC; ++kk) {
-        const uint4 xv = *reinterpret_cast<const uint4*>(Xs + (kk * EG + eg) * ROW + tm * 4);
-        const uint4 y0 = *reinterpret_cast<const uint4*>(Ys + (kk * EG + eg) * ROW + tn * 8);
-        const uint4 y1 = *reinterpret_cast<const uint4*>(Ys + (kk * EG + eg) * ROW + tn * 8 + 4);
-        const uint32_t xr[4] = {xv.x, xv.y, xv.z, xv.w};
-        const uint32_t yr[8] = {y0.x, y0.y, y0.z, y0.w, y1.x, y1.y, y1.z, y1.w};
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-          for (int j = 0; j < 8; ++j) acc96_mad(a[i][j], xr[i], yr[j]);
-      }
-      __syncthreads();
+    switch (tile_tmg(mat.rows)) {
+      case 32: batch_item<32>(wk, tile, mat, sitems, s_hat, acc, d, f, batch_smem); break;
+      case 16: batch_item<16>(wk, tile, mat, sitems, s_hat, acc, d, f, batch_smem); break;
+      default: batch_item<8>(wk, tile, mat, sitems, s_hat, acc, d, f, batch_smem); break;
     }
-    const int e = e0 + eg;
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const int m = tm * 4 + i;
-      if ((uint32_t)m >= tile.count) continue;
-      const unsigned long long t_off = sitems[m].t_off;
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const int row = tn * 8 + j;
-        if ((uint32_t)row >= mat.rows) continue;
-        atomicAdd(&acc[(t_off + row) * d + e], (unsigned long long)acc96_reduce(a[i][j], f));
-      }
-    }
-    __syncthreads();  // sitems / widx are rewritten by the next work item
+    __syncthreads();  // stages, sitems and widx are rewritten by the next work item
   }
 }
 
@@ -183,7 +239,7 @@ std::vector<WorkDev> make_work(const std::vector<TileDev>& tiles, uint32_t group
       for (uint32_t g = 0; g < groups; ++g) work.push_back(WorkDev{ti, k0, k1, g});
     }
   }
-  // Longest K ranges first (every tile carries up to 32 x 32 outputs per K step).
+  // Longest K ranges first (every tile shape carries 1024 outputs per K step).
   std::stable_sort(work.begin(), work.end(), [](const WorkDev& x, const WorkDev& y) {
     return (x.k1 - x.k0) > (y.k1 - y.k0);
   });
@@ -228,10 +284,10 @@ int run_core(const grid_gpu_plan* p, const MatDev* d_mats, const ItemDev* d_item
   if (nwork) {
     static int bps_cache[kMaxDevices] = {};
     int bps = 0;
-    rc = prepare_kernel(batch_emm_kernel, 0, kThreads, p->device, bps_cache, &bps);
+    rc = prepare_kernel(batch_emm_kernel, kBatchSmem, kThreads, p->device, bps_cache, &bps);
     if (rc) return rc;
     const unsigned grid = std::min<unsigned>(nwork, (unsigned)(p->num_sms * bps));
-    batch_emm_kernel<<<grid, kThreads, 0, st>>>(d_work, nwork, d_tiles, d_items, d_mats, s_hat,
+    batch_emm_kernel<<<grid, kThreads, kBatchSmem, st>>>(d_work, nwork, d_tiles, d_items, d_mats, s_hat,
                                                  acc, counter, (int)d, p->f);
     if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(e);
   }
@@ -274,7 +330,8 @@ uint32_t auto_k_split(const std::vector<TileDev>& tiles, uint32_t groups, int nu
   return (uint32_t)(per * KC);
 }
 
-// Group items by matrix, longest first, into tiles of TM; then cut every tile
+// Group items by matrix, longest first, into tiles of 32, 64 or 128 instances
+// (by the matrix's rows, tile_tmg); then cut every tile
 // into (K range, evaluation group) work items, longest K ranges first.
 int build_tables(const grid_gpu_plan* plan, grid_gpu_matrix* const* mats, size_t nmats,
                  const grid_gpu_batch_item* items, size_t nitems, uint32_t k_split,
@@ -306,7 +363,8 @@ int build_tables(const grid_gpu_plan* plan, grid_gpu_matrix* const* mats, size_t
     const uint32_t m = order[i].first;
     size_t j = i;
     TileDev tl{(uint32_t)tb.sorted.size(), 0, m, 0};
-    while (j < order.size() && order[j].first == m && j - i < (size_t)TM) {
+    const size_t cap = 4 * (size_t)tile_tmg(tb.mats[m].rows);  // instances per tile
+    while (j < order.size() && order[j].first == m && j - i < cap) {
       const grid_gpu_batch_item& it = items[order[j].second];
       tb.sorted.push_back(ItemDev{it.s_offset, it.t_offset, it.n, 0});
       tl.kmax = std::max(tl.kmax, it.n);
