@@ -22,6 +22,8 @@
 // 64-bit global row sums with atomics; a final kernel reduces them mod q.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "grid_async.cuh"
 #include "grid_field.cuh"
 #include "grid_internal.h"
@@ -429,6 +431,22 @@ int launch_jl_project(const FieldParams& f, const uint8_t seed[32], size_t rows,
                                       &bps)
                      : prepare_kernel(jl_tc_kernel<false>, kTcSmem, kTcThreads, dev, tc_bps_part,
                                       &bps)) == GRID_OK;
+  // Resident CTAs per SM: the occupancy query has reported 1 for this kernel
+  // where shared memory admits 3 (measured 20 % slower), so take the larger of
+  // it and what the SM's shared memory holds. The grid-stride chunk loop makes
+  // any count correct.
+  static int smem_bps[kMaxDevices] = {};
+  if (use_tc && smem_bps[dev] == 0) {
+    int per_sm = 0, reserved = 0;
+    if (cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) !=
+            cudaSuccess ||
+        cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev) !=
+            cudaSuccess)
+      per_sm = 0;
+    const int fit = per_sm / (int)(kTcSmem + (uint32_t)reserved);
+    smem_bps[dev] = std::max(1, std::min(fit, 2048 / kTcThreads));
+  }
+  if (use_tc) bps = std::max(bps, smem_bps[dev]);
   unsigned long long tc_grid = (unsigned long long)num_sms * (unsigned long long)(bps > 0 ? bps : 1);
   if (tc_grid > tc_chunks) tc_grid = tc_chunks;
   // exactness bound of the int32 accumulators: columns per CTA
