@@ -387,7 +387,11 @@ def measure_serve(dev, rates=(1000, 2000, 5000, 10000, 20000, 50000), seconds=0.
            "rates": {}}
     for mode in ("continuous", "plain"):
         with RingServer(plan, mats, key, pool, mode=mode) as srv:
-            run_load(srv, schedule(1, 300, 3000.0))           # warm-up
+            # warm-up at a sparse and a dense rate: the first sparse-traffic
+            # requests of a process pay a one-time host-side cost (tens of ms)
+            # that dense traffic does not trigger
+            run_load(srv, schedule(2, 200, 1000.0))
+            run_load(srv, schedule(1, 300, 3000.0))
             for lam in rates:
                 res = run_load(srv, schedule(100 + lam, max(200, int(lam * seconds)), float(lam)))
                 out["rates"].setdefault(str(lam), {})[mode] = res
