@@ -290,8 +290,21 @@ def measure_round(dev, reps=50):
         if i >= 2:
             e2e.append((time.perf_counter() - t0) * 1e3)
     d2h = sum(x.numel() * x.element_size() for x in outs_host)
+    # the round's neighbours at the same size: garbage h (aggregated phis of
+    # the witness shape) and the amortized witness z = sum_i c_i s_i
+    from lattica_b200.labrador import amortize_witness, compute_garbage_h
+    phis = torch.randint(0, q, (r, n, d), dtype=torch.int64, device=dev, generator=g).to(torch.int32)
+    chal = torch.randint(0, q, (r, d), dtype=torch.int64, device=dev, generator=g).to(torch.int32)
+    for _ in range(3):
+        compute_garbage_h(plan, wit, phis)
+        amortize_witness(plan, wit, chal)
+    torch.cuda.synchronize()
+    times_h = _events_ms(lambda: compute_garbage_h(plan, wit, phis), max(5, reps // 5), stream)
+    times_z = _events_ms(lambda: amortize_witness(plan, wit, chal), max(5, reps // 5), stream)
+    del phis
     return {"workload": "LaBRADOR round: r=64, n=2048, d=64, kappa=16, JL 256 rows, base 2^8 x4 limbs",
             "round_ms_p50": _pct(times, 50), "round_ms_p99": _pct(times, 99),
+            "garbage_h_ms_p50": _pct(times_h, 50), "amortize_ms_p50": _pct(times_z, 50),
             "round_with_jl_extraction_ms_p50": _pct(times_x, 50),
             "e2e_round_ms_p50": _pct(e2e, 50), "e2e_round_ms_p99": _pct(e2e, 99),
             "e2e_h2d_bytes": hw.numel() * 4, "e2e_d2h_bytes": d2h, "rounds": reps}

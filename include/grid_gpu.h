@@ -172,6 +172,27 @@ int grid_gpu_gram_dev(const grid_gpu_plan* plan, const uint32_t* S, size_t r, si
                       uint32_t* G, void* workspace, size_t workspace_bytes, void* stream);
 int grid_gpu_gram(grid_gpu_plan* plan, const uint32_t* S, size_t r, size_t n, uint32_t* G);
 
+/* ---- garbage h: compute_garbage_h (labrador/src/main_protocol/garbage.rs:101-133)
+ *      H[idx(i,j)] = (<phi_i, s_j> + <phi_j, s_i>) * 2^-1 for i <= j, row-major upper
+ *      triangle (garbage_index, main_protocol/mod.rs:664-670). S, Phi: r x n polys. */
+int grid_gpu_garbage_h_workspace(const grid_gpu_plan* plan, size_t r, size_t n, size_t* bytes);
+int grid_gpu_garbage_h_dev(const grid_gpu_plan* plan, const uint32_t* S, const uint32_t* Phi,
+                           size_t r, size_t n, uint32_t* H, void* workspace,
+                           size_t workspace_bytes, void* stream);
+int grid_gpu_garbage_h(grid_gpu_plan* plan, const uint32_t* S, const uint32_t* Phi, size_t r,
+                       size_t n, uint32_t* H);
+
+/* ---- amortized witness: compute_amortized_witness
+ *      (labrador/src/main_protocol/amortization.rs:61-84) without the challenge
+ *      sampling, which stays with the transcript on the host:
+ *      z[k] = sum_i c_i * s_i[k]. S: r x n polys, c: r polys, z: n polys. */
+int grid_gpu_amortize_workspace(const grid_gpu_plan* plan, size_t r, size_t n, size_t* bytes);
+int grid_gpu_amortize_dev(const grid_gpu_plan* plan, const uint32_t* S, const uint32_t* c,
+                          size_t r, size_t n, uint32_t* z, void* workspace,
+                          size_t workspace_bytes, void* stream);
+int grid_gpu_amortize(grid_gpu_plan* plan, const uint32_t* S, const uint32_t* c, size_t r,
+                      size_t n, uint32_t* z);
+
 /* ---- JL projection: JLMatrix::project_and_extract_jl_rows (labrador/src/jl.rs:267-303)
  *      seed: 32 bytes; parts: num_parts x cols words; rows <= 256; p_out: rows words;
  *      flat_out (optional, NULL to skip): rows*num_parts*cols int8 in the

@@ -73,6 +73,16 @@ SIGNATURES = {
     "grid_gpu_gram_workspace": (C.c_int, [_vp, C.c_size_t, C.c_size_t, C.POINTER(C.c_size_t)]),
     "grid_gpu_gram_dev": (C.c_int, [_vp, _vp, C.c_size_t, C.c_size_t, _vp, _vp, C.c_size_t, _vp]),
     "grid_gpu_gram": (C.c_int, [_vp, _vp, C.c_size_t, C.c_size_t, _vp]),
+    "grid_gpu_garbage_h_workspace": (C.c_int, [_vp, C.c_size_t, C.c_size_t,
+                                               C.POINTER(C.c_size_t)]),
+    "grid_gpu_garbage_h_dev": (C.c_int, [_vp, _vp, _vp, C.c_size_t, C.c_size_t, _vp, _vp,
+                                         C.c_size_t, _vp]),
+    "grid_gpu_garbage_h": (C.c_int, [_vp, _vp, _vp, C.c_size_t, C.c_size_t, _vp]),
+    "grid_gpu_amortize_workspace": (C.c_int, [_vp, C.c_size_t, C.c_size_t,
+                                              C.POINTER(C.c_size_t)]),
+    "grid_gpu_amortize_dev": (C.c_int, [_vp, _vp, _vp, C.c_size_t, C.c_size_t, _vp, _vp,
+                                        C.c_size_t, _vp]),
+    "grid_gpu_amortize": (C.c_int, [_vp, _vp, _vp, C.c_size_t, C.c_size_t, _vp]),
     "grid_gpu_jl_workspace": (C.c_int, [C.c_size_t, C.POINTER(C.c_size_t)]),
     "grid_gpu_jl_project_dev": (C.c_int, [_vp, _vp, C.c_size_t, _vp, C.c_size_t, C.c_size_t,
                                           C.c_size_t, _vp, _vp, _vp, C.c_size_t, _vp]),

@@ -6,6 +6,8 @@ the median CUDA-event time.
     python -m lattica_b200.cases round --reps 24     # LaBRADOR prover round
     python -m lattica_b200.cases gram --reps 4       # r x r Gram, r = 64, n = 2048
     python -m lattica_b200.cases commit --reps 4     # 16 x 2048 matrix times 64 witnesses
+    python -m lattica_b200.cases garbage_h --reps 4  # h = sym(Phi S^T) / 2, r = 64, n = 2048
+    python -m lattica_b200.cases amortize --reps 4   # z = sum_i c_i s_i, r = 64, n = 2048
     python -m lattica_b200.cases ntt256 --reps 4     # d = 256 products, 2^20 polys at q'
 
 Sizes: r = 64 witness vectors of n = 2048 polys (d = 64, coefficients in
@@ -31,7 +33,8 @@ def build(case: str):
     """Returns a zero-argument callable that runs one instance of `case`."""
     import torch
     from lattica_b200 import TwistedNttPlan
-    from lattica_b200.labrador import CommitKey, compute_garbage_g, prover_round_dev
+    from lattica_b200.labrador import (CommitKey, amortize_witness, compute_garbage_g,
+                                       compute_garbage_h, prover_round_dev)
     dev = torch.device("cuda:0")
     g = torch.Generator(device=dev).manual_seed(5)
     r, n, kappa = 64, 2048, 16
@@ -44,6 +47,12 @@ def build(case: str):
     wit = _witness(torch, dev, g, Q, (r, n, 64))
     if case == "gram":
         return lambda: compute_garbage_g(plan, wit)
+    if case == "garbage_h":
+        phis = _uniform(torch, dev, g, Q, (r, n, 64))
+        return lambda: compute_garbage_h(plan, wit, phis)
+    if case == "amortize":
+        chal = _uniform(torch, dev, g, Q, (r, 64))
+        return lambda: amortize_witness(plan, wit, chal)
     key = CommitKey(plan, _uniform(torch, dev, g, Q, (kappa, n, 64)), kappa, n)
     if case == "commit":
         return lambda: key.inner_commit_slice(wit)
@@ -55,7 +64,7 @@ def build(case: str):
 
 def main(argv=None) -> None:
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
-    ap.add_argument("case", choices=["round", "gram", "commit", "ntt256"])
+    ap.add_argument("case", choices=["round", "gram", "garbage_h", "amortize", "commit", "ntt256"])
     ap.add_argument("--reps", type=int, default=4)
     args = ap.parse_args(argv)
     import torch

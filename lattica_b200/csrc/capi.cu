@@ -47,6 +47,15 @@ size_t gram_ws_bytes(const grid_gpu_plan* p, size_t r, size_t n) {
                                                                        EMM_UPPER));
 }
 
+size_t garbage_h_ws_bytes(const grid_gpu_plan* p, size_t r, size_t n) {
+  return 2 * words_bytes(r * n * p->d) + words_bytes(r * r * p->d) +
+         words_bytes(emm_workspace_words(p, (int)r, (int)r, (int)n, EMM_DENSE));
+}
+
+size_t amortize_ws_bytes(const grid_gpu_plan* p, size_t r, size_t n) {
+  return words_bytes(r * n * p->d) + words_bytes(r * p->d);
+}
+
 bool dims_ok(size_t a, size_t b, size_t c) {
   // all kernels index rows/cols/K with int
   return a > 0 && b > 0 && c > 0 && a < (1u << 30) && b < (1u << 30) && c < (1u << 30);
@@ -289,6 +298,116 @@ int grid_gpu_gram(grid_gpu_plan* p, const uint32_t* S, size_t r, size_t n, uint3
                            static_cast<uint32_t*>(p->scratch[7].ptr), p->scratch[8].ptr, ws, st);
   if (!rc)
     rc = cuda_status(cudaMemcpyAsync(G, p->scratch[7].ptr, g_bytes, cudaMemcpyDeviceToHost, st));
+  const int fin = finish_host_call(p, st);
+  return rc ? rc : fin;
+}
+
+/* ---- garbage h and the amortized witness -------------------------------- */
+
+int grid_gpu_garbage_h_workspace(const grid_gpu_plan* p, size_t r, size_t n, size_t* bytes) {
+  if (!p || !bytes) return GRID_ERR_NULL_POINTER;
+  *bytes = garbage_h_ws_bytes(p, r, n);
+  return GRID_OK;
+}
+
+int grid_gpu_garbage_h_dev(const grid_gpu_plan* p, const uint32_t* S, const uint32_t* Phi,
+                           size_t r, size_t n, uint32_t* H, void* workspace,
+                           size_t workspace_bytes, void* stream) {
+  if (!p || !S || !Phi || !H) return GRID_ERR_NULL_POINTER;
+  if (!dims_ok(r, n, 1)) return GRID_ERR_INVALID_PARAMETERS;
+  if (!aligned16(S) || !aligned16(Phi) || !aligned16(H) || !aligned16(workspace))
+    return GRID_ERR_MISALIGNED;
+  cudaStream_t st = (cudaStream_t)stream;
+  Carver cv(workspace, workspace_bytes);
+  uint32_t* s_hat = cv.take<uint32_t>(r * n * p->d);
+  uint32_t* phi_hat = cv.take<uint32_t>(r * n * p->d);
+  uint32_t* cross = cv.take<uint32_t>(r * r * p->d);
+  const size_t ew = emm_workspace_words(p, (int)r, (int)r, (int)n, EMM_DENSE);
+  uint32_t* work = ew ? cv.take<uint32_t>(ew) : nullptr;
+  if (!cv.ok) return GRID_ERR_INVALID_PARAMETERS;
+  int rc = launch_ntt(p, MODE_FWD, S, nullptr, s_hat, r * n, st);
+  if (!rc) rc = launch_ntt(p, MODE_FWD, Phi, nullptr, phi_hat, r * n, st);
+  // cross[i][j] = <phi_i, s_j>
+  if (!rc)
+    rc = launch_emm(p, phi_hat, s_hat, (int)r, (int)r, (int)n, (int)n, EMM_DENSE, cross, work, st);
+  if (!rc) rc = launch_symmetrize_half(p, cross, (int)r, H, st);
+  if (rc) return rc;
+  return launch_ntt(p, MODE_INV, H, nullptr, H, r * (r + 1) / 2, st);
+}
+
+int grid_gpu_garbage_h(grid_gpu_plan* p, const uint32_t* S, const uint32_t* Phi, size_t r,
+                       size_t n, uint32_t* H) {
+  if (!p || !S || !Phi || !H) return GRID_ERR_NULL_POINTER;
+  if (!dims_ok(r, n, 1)) return GRID_ERR_INVALID_PARAMETERS;
+  std::lock_guard<std::mutex> lk(p->mu);
+  const size_t s_bytes = r * n * p->d * 4, h_bytes = r * (r + 1) / 2 * p->d * 4;
+  const size_t ws = garbage_h_ws_bytes(p, r, n);
+  int rc;
+  if ((rc = ensure_scratch(p, 6, s_bytes)) || (rc = ensure_scratch(p, 9, s_bytes)) ||
+      (rc = ensure_scratch(p, 7, h_bytes)) || (rc = ensure_scratch(p, 8, ws)))
+    return rc;
+  cudaStream_t st = p->stream;
+  rc = cuda_status(cudaMemcpyAsync(p->scratch[6].ptr, S, s_bytes, cudaMemcpyHostToDevice, st));
+  if (!rc)
+    rc = cuda_status(cudaMemcpyAsync(p->scratch[9].ptr, Phi, s_bytes, cudaMemcpyHostToDevice, st));
+  if (!rc)
+    rc = grid_gpu_garbage_h_dev(p, static_cast<uint32_t*>(p->scratch[6].ptr),
+                                static_cast<uint32_t*>(p->scratch[9].ptr), r, n,
+                                static_cast<uint32_t*>(p->scratch[7].ptr), p->scratch[8].ptr, ws,
+                                st);
+  if (!rc)
+    rc = cuda_status(cudaMemcpyAsync(H, p->scratch[7].ptr, h_bytes, cudaMemcpyDeviceToHost, st));
+  const int fin = finish_host_call(p, st);
+  return rc ? rc : fin;
+}
+
+int grid_gpu_amortize_workspace(const grid_gpu_plan* p, size_t r, size_t n, size_t* bytes) {
+  if (!p || !bytes) return GRID_ERR_NULL_POINTER;
+  *bytes = amortize_ws_bytes(p, r, n);
+  return GRID_OK;
+}
+
+int grid_gpu_amortize_dev(const grid_gpu_plan* p, const uint32_t* S, const uint32_t* c, size_t r,
+                          size_t n, uint32_t* z, void* workspace, size_t workspace_bytes,
+                          void* stream) {
+  if (!p || !S || !c || !z) return GRID_ERR_NULL_POINTER;
+  if (!dims_ok(r, n, 1)) return GRID_ERR_INVALID_PARAMETERS;
+  if (!aligned16(S) || !aligned16(c) || !aligned16(z) || !aligned16(workspace))
+    return GRID_ERR_MISALIGNED;
+  cudaStream_t st = (cudaStream_t)stream;
+  Carver cv(workspace, workspace_bytes);
+  uint32_t* s_hat = cv.take<uint32_t>(r * n * p->d);
+  uint32_t* c_hat = cv.take<uint32_t>(r * p->d);
+  if (!cv.ok) return GRID_ERR_INVALID_PARAMETERS;
+  int rc = launch_ntt(p, MODE_FWD, S, nullptr, s_hat, r * n, st);
+  if (!rc) rc = launch_ntt(p, MODE_FWD, c, nullptr, c_hat, r, st);
+  if (!rc) rc = launch_amortize(p, c_hat, s_hat, (int)r, n, z, st);
+  if (rc) return rc;
+  return launch_ntt(p, MODE_INV, z, nullptr, z, n, st);
+}
+
+int grid_gpu_amortize(grid_gpu_plan* p, const uint32_t* S, const uint32_t* c, size_t r, size_t n,
+                      uint32_t* z) {
+  if (!p || !S || !c || !z) return GRID_ERR_NULL_POINTER;
+  if (!dims_ok(r, n, 1)) return GRID_ERR_INVALID_PARAMETERS;
+  std::lock_guard<std::mutex> lk(p->mu);
+  const size_t s_bytes = r * n * p->d * 4, c_bytes = r * p->d * 4, z_bytes = n * p->d * 4;
+  const size_t ws = amortize_ws_bytes(p, r, n);
+  int rc;
+  if ((rc = ensure_scratch(p, 6, s_bytes)) || (rc = ensure_scratch(p, 9, c_bytes)) ||
+      (rc = ensure_scratch(p, 7, z_bytes)) || (rc = ensure_scratch(p, 8, ws)))
+    return rc;
+  cudaStream_t st = p->stream;
+  rc = cuda_status(cudaMemcpyAsync(p->scratch[6].ptr, S, s_bytes, cudaMemcpyHostToDevice, st));
+  if (!rc)
+    rc = cuda_status(cudaMemcpyAsync(p->scratch[9].ptr, c, c_bytes, cudaMemcpyHostToDevice, st));
+  if (!rc)
+    rc = grid_gpu_amortize_dev(p, static_cast<uint32_t*>(p->scratch[6].ptr),
+                               static_cast<uint32_t*>(p->scratch[9].ptr), r, n,
+                               static_cast<uint32_t*>(p->scratch[7].ptr), p->scratch[8].ptr, ws,
+                               st);
+  if (!rc)
+    rc = cuda_status(cudaMemcpyAsync(z, p->scratch[7].ptr, z_bytes, cudaMemcpyDeviceToHost, st));
   const int fin = finish_host_call(p, st);
   return rc ? rc : fin;
 }

@@ -104,6 +104,11 @@ int launch_emm(const grid_gpu_plan* p, const uint32_t* X, const uint32_t* Y, int
                int ldy, int mode, uint32_t* out_evals, uint32_t* work, cudaStream_t s);
 int launch_pointwise(const grid_gpu_plan* p, uint32_t* dst, const uint32_t* rhs, size_t words,
                      cudaStream_t s);
+// garbage.cu: (C_ij + C_ji) * 2^-1 on the upper triangle; z_hat = sum_i c_hat_i (.) s_hat_i.
+int launch_symmetrize_half(const grid_gpu_plan* p, const uint32_t* C, int r, uint32_t* H,
+                           cudaStream_t s);
+int launch_amortize(const grid_gpu_plan* p, const uint32_t* c_hat, const uint32_t* s_hat, int r,
+                    size_t n, uint32_t* z_hat, cudaStream_t s);
 int launch_add(const grid_gpu_plan* p, uint32_t* dst, const uint32_t* rhs, size_t words,
                cudaStream_t s);
 

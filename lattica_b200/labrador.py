@@ -72,6 +72,62 @@ def compute_garbage_g(plan: TwistedNttPlan, witness):
     return g
 
 
+def compute_garbage_h(plan: TwistedNttPlan, witness, aggregated_phis):
+    """h_ij = (<phi_i, s_j> + <phi_j, s_i>) * 2^-1 for i <= j in garbage_index
+    order (garbage.rs:101-133). witness, aggregated_phis: (r, n, d) numpy
+    uint32 or CUDA tensors (both the same kind)."""
+    r, n, d = (int(x) for x in witness.shape)
+    if d != plan.d or tuple(aggregated_phis.shape) != (r, n, d):
+        raise ValueError("witness and phis must both be (r, n, d) with the plan's d")
+    lib = _lib.load()
+    if _is_torch(witness):
+        import torch
+        h = torch.empty((garbage_count(r), d), dtype=witness.dtype, device=witness.device)
+        nb = C.c_size_t()
+        raise_status(lib.grid_gpu_garbage_h_workspace(plan.handle, r, n, C.byref(nb)),
+                     "garbage_h_ws")
+        ws = torch.empty(max(16, nb.value), dtype=torch.uint8, device=witness.device)
+        st = lib.grid_gpu_garbage_h_dev(plan.handle, witness.data_ptr(),
+                                        aggregated_phis.data_ptr(), r, n, h.data_ptr(),
+                                        ws.data_ptr(), ws.numel(), _stream_ptr(witness))
+    else:
+        w = np.ascontiguousarray(witness, dtype=np.uint32)
+        ph = np.ascontiguousarray(aggregated_phis, dtype=np.uint32)
+        h = np.empty((garbage_count(r), d), dtype=np.uint32)
+        st = lib.grid_gpu_garbage_h(plan.handle, w.ctypes.data, ph.ctypes.data, r, n,
+                                    h.ctypes.data)
+    raise_status(st, "grid_gpu_garbage_h")
+    return h
+
+
+def amortize_witness(plan: TwistedNttPlan, witness, challenges):
+    """z[k] = sum_i c_i * s_i[k], the product part of compute_amortized_witness
+    (amortization.rs:61-84); the challenges c_i (r polys) come from the
+    caller's transcript. witness: (r, n, d), challenges: (r, d), numpy uint32
+    or CUDA tensors (both the same kind). Returns z: (n, d)."""
+    r, n, d = (int(x) for x in witness.shape)
+    if d != plan.d or tuple(challenges.shape) != (r, d):
+        raise ValueError("witness must be (r, n, d) and challenges (r, d) with the plan's d")
+    lib = _lib.load()
+    if _is_torch(witness):
+        import torch
+        z = torch.empty((n, d), dtype=witness.dtype, device=witness.device)
+        nb = C.c_size_t()
+        raise_status(lib.grid_gpu_amortize_workspace(plan.handle, r, n, C.byref(nb)),
+                     "amortize_ws")
+        ws = torch.empty(max(16, nb.value), dtype=torch.uint8, device=witness.device)
+        st = lib.grid_gpu_amortize_dev(plan.handle, witness.data_ptr(), challenges.data_ptr(),
+                                       r, n, z.data_ptr(), ws.data_ptr(), ws.numel(),
+                                       _stream_ptr(witness))
+    else:
+        w = np.ascontiguousarray(witness, dtype=np.uint32)
+        c = np.ascontiguousarray(challenges, dtype=np.uint32)
+        z = np.empty((n, d), dtype=np.uint32)
+        st = lib.grid_gpu_amortize(plan.handle, w.ctypes.data, c.ctypes.data, r, n, z.ctypes.data)
+    raise_status(st, "grid_gpu_amortize")
+    return z
+
+
 class CommitKey:
     """The inner-commitment matrix A (kappa x n) of a LaBRADOR CommitKey
     (labrador/src/crs.rs:111-216), kept resident on the device."""

@@ -535,6 +535,61 @@ int orc_gram_naive(const orc_plan *p, const uint32_t *S, size_t r, size_t n, uin
     return ORC_OK;
 }
 
+/* compute_garbage_h, garbage.rs:101-133:
+ * h_ij = (<phi_i, s_j> + <phi_j, s_i>) * 2^-1, i <= j in garbage_index order.
+ * 2^-1 is the field element (q + 1) / 2 (R::from_u64(q / 2 + 1)), applied to
+ * every coefficient; the dot products are ring inner products, evaluated here
+ * in the twisted domain (exact field arithmetic, the same words). */
+int orc_garbage_h(const orc_plan *p, const uint32_t *S, const uint32_t *Phi, size_t r, size_t n,
+                  uint32_t *H) {
+    const uint32_t d = p->n;
+    const size_t total = r * n * d;
+    uint32_t *sh = (uint32_t *)malloc(sizeof(uint32_t) * total);
+    uint32_t *ph = (uint32_t *)malloc(sizeof(uint32_t) * total);
+    uint32_t *tmp = (uint32_t *)malloc(sizeof(uint32_t) * d);
+    if (!sh || !ph || !tmp) { free(sh); free(ph); free(tmp); return ORC_ERR_OOM; }
+    memcpy(sh, S, sizeof(uint32_t) * total);
+    memcpy(ph, Phi, sizeof(uint32_t) * total);
+    orc_twisted_forward(p, sh, r * n);
+    orc_twisted_forward(p, ph, r * n);
+    const uint32_t two_inv = orc_to_mont(&p->f, (uint64_t)p->f.q / 2 + 1);
+    size_t idx = 0;
+    for (size_t i = 0; i < r; i++)
+        for (size_t j = i; j < r; j++, idx++) {
+            uint32_t *out = H + idx * d;
+            eval_dot(&p->f, d, ph + i * n * d, d, sh + j * n * d, d, n, out);
+            eval_dot(&p->f, d, ph + j * n * d, d, sh + i * n * d, d, n, tmp);
+            for (uint32_t e = 0; e < d; e++) out[e] = orc_add(&p->f, out[e], tmp[e]);
+            orc_twisted_inverse(p, out, 1);
+            for (uint32_t e = 0; e < d; e++) out[e] = orc_mul(&p->f, out[e], two_inv);
+        }
+    free(sh); free(ph); free(tmp);
+    return ORC_OK;
+}
+
+/* compute_amortized_witness, amortization.rs:61-84 (the challenge sampling
+ * from the transcript stays with the caller): z[k] = sum_i c_i * s_i[k], ring
+ * products evaluated in the twisted domain. */
+int orc_amortize(const orc_plan *p, const uint32_t *S, const uint32_t *c, size_t r, size_t n,
+                 uint32_t *Z) {
+    const uint32_t d = p->n;
+    uint32_t *sh = (uint32_t *)malloc(sizeof(uint32_t) * r * n * d);
+    uint32_t *ch = (uint32_t *)malloc(sizeof(uint32_t) * r * d);
+    if (!sh || !ch) { free(sh); free(ch); return ORC_ERR_OOM; }
+    memcpy(sh, S, sizeof(uint32_t) * r * n * d);
+    memcpy(ch, c, sizeof(uint32_t) * r * d);
+    orc_twisted_forward(p, sh, r * n);
+    orc_twisted_forward(p, ch, r);
+    for (size_t k = 0; k < n; k++) {
+        uint32_t *out = Z + k * d;
+        /* sum over i of c_hat[i] (stride d) times s_hat[i][k] (stride n * d) */
+        eval_dot(&p->f, d, ch, d, sh + k * d, n * d, r, out);
+        orc_twisted_inverse(p, out, 1);
+    }
+    free(sh); free(ch);
+    return ORC_OK;
+}
+
 /* ------------------------------------------------------------------------ */
 /* Decompositions                                                            */
 /* ------------------------------------------------------------------------ */

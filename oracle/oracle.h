@@ -104,6 +104,10 @@ int orc_linear_commit(const orc_plan *p, const uint32_t *a_msg, size_t rows, siz
 /* Gram g_ij = <s_i, s_j>, i <= j, row-major upper triangle
  * (labrador/src/main_protocol/garbage.rs:76-93, mod.rs:664-670). */
 int orc_gram(const orc_plan *p, const uint32_t *S, size_t r, size_t n, uint32_t *G, int threads);
+int orc_garbage_h(const orc_plan *p, const uint32_t *S, const uint32_t *Phi, size_t r, size_t n,
+                  uint32_t *H);
+int orc_amortize(const orc_plan *p, const uint32_t *S, const uint32_t *c, size_t r, size_t n,
+                 uint32_t *Z);
 /* Slow faithful path: one full negacyclic product per term (poly/ring.rs:111-129). */
 int orc_gram_naive(const orc_plan *p, const uint32_t *S, size_t r, size_t n, uint32_t *G);
 size_t orc_garbage_index(size_t r, size_t i, size_t j);

@@ -75,6 +75,8 @@ def lib():
                                             C.c_size_t, _u32p, _u32p, _u32p]),
             "orc_gram": (C.c_int, [pp, _u32p, C.c_size_t, C.c_size_t, _u32p, C.c_int]),
             "orc_gram_naive": (C.c_int, [pp, _u32p, C.c_size_t, C.c_size_t, _u32p]),
+            "orc_garbage_h": (C.c_int, [pp, _u32p, _u32p, C.c_size_t, C.c_size_t, _u32p]),
+            "orc_amortize": (C.c_int, [pp, _u32p, _u32p, C.c_size_t, C.c_size_t, _u32p]),
             "orc_garbage_index": (C.c_size_t, [C.c_size_t, C.c_size_t, C.c_size_t]),
             "orc_decompose_coeff_balanced": (None, [C.c_uint64, C.c_uint64, C.c_size_t,
                                                     C.c_uint64, _i64p]),
@@ -253,6 +255,27 @@ class Plan:
         if st:
             raise OracleError(st)
         return G
+
+
+    def garbage_h(self, S, Phi, r, n):
+        """h_ij = (<phi_i, s_j> + <phi_j, s_i>) 2^-1, i <= j (garbage.rs:101-133)."""
+        S, pS = _u32(S)
+        Phi, pP = _u32(Phi)
+        H = np.empty(r * (r + 1) // 2 * self.n, dtype=np.uint32)
+        st = lib().orc_garbage_h(self._ref(), pS, pP, r, n, H.ctypes.data_as(_u32p))
+        if st:
+            raise OracleError(st)
+        return H
+
+    def amortize(self, S, c, r, n):
+        """z[k] = sum_i c_i s_i[k] (amortization.rs:75-81); c: r challenge polys."""
+        S, pS = _u32(S)
+        c, pc = _u32(c)
+        Z = np.empty(n * self.n, dtype=np.uint32)
+        st = lib().orc_amortize(self._ref(), pS, pc, r, n, Z.ctypes.data_as(_u32p))
+        if st:
+            raise OracleError(st)
+        return Z
 
 
 def decompose_coeff_balanced(c: int, base: int, num_limbs: int, q: int):
