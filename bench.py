@@ -302,9 +302,28 @@ def measure_round(dev, reps=50):
     times_h = _events_ms(lambda: compute_garbage_h(plan, wit, phis), max(5, reps // 5), stream)
     times_z = _events_ms(lambda: amortize_witness(plan, wit, chal), max(5, reps // 5), stream)
     del phis
+    # outer commitments of the round's limbs (kappa1 = kappa2 = 16): u1 = B t + C g
+    # over t (r * 4 * kappa = 4096 polys) and g (4 * 2080 = 8320), u2 = D h (8320)
+    from lattica_b200.commit import BdlopCommitmentKey
+    from lattica_b200.labrador import OuterCommitKey
+    k1, t_len, g_len = 16, r * 4 * kappa, 4 * (r * (r + 1) // 2)
+    rnd = lambda *shape: torch.randint(0, q, shape, dtype=torch.int64, device=dev,
+                                       generator=g).to(torch.int32)
+    outer = OuterCommitKey(plan, rnd(k1, t_len, d), rnd(k1, g_len, d), rnd(k1, g_len, d), k1, k1,
+                           t_len, g_len, g_len)
+    tv, gv = rnd(t_len, d), rnd(g_len, d)
+    times_u1 = _events_ms(lambda: outer.outer_commit_u1_slice(tv, gv), max(5, reps // 5), stream)
+    times_u2 = _events_ms(lambda: outer.outer_commit_u2_slice(gv), max(5, reps // 5), stream)
+    del outer
+    # BDLOP parts at the plain-commit shape: 8 x 64 matrices, a batch of 64
+    bd = BdlopCommitmentKey(plan, rnd(8, 64, d), rnd(8, 64, d), rnd(8, 64, d), 8, 64, 64)
+    bm, br = rnd(64, 64, d), rnd(64, 64, d)
+    times_bd = _events_ms(lambda: bd.recompute_parts(bm, br), max(5, reps // 5), stream)
     return {"workload": "LaBRADOR round: r=64, n=2048, d=64, kappa=16, JL 256 rows, base 2^8 x4 limbs",
             "round_ms_p50": _pct(times, 50), "round_ms_p99": _pct(times, 99),
             "garbage_h_ms_p50": _pct(times_h, 50), "amortize_ms_p50": _pct(times_z, 50),
+            "outer_u1_ms_p50": _pct(times_u1, 50), "outer_u2_ms_p50": _pct(times_u2, 50),
+            "bdlop_batch64_ms_p50": _pct(times_bd, 50),
             "round_with_jl_extraction_ms_p50": _pct(times_x, 50),
             "e2e_round_ms_p50": _pct(e2e, 50), "e2e_round_ms_p99": _pct(e2e, 99),
             "e2e_h2d_bytes": hw.numel() * 4, "e2e_d2h_bytes": d2h, "rounds": reps}

@@ -162,6 +162,24 @@ int grid_gpu_commit(grid_gpu_matrix* A, const uint32_t* s, size_t batch, uint32_
  * (commit/src/linear.rs:476-506). Ajtai with a zero opening is grid_gpu_commit. */
 int grid_gpu_linear_commit(grid_gpu_matrix* A_msg, grid_gpu_matrix* A_open, const uint32_t* m,
                            const uint32_t* r, size_t batch, uint32_t* t);
+int grid_gpu_linear_commit_workspace(const grid_gpu_matrix* A_msg, const grid_gpu_matrix* A_open,
+                                     size_t batch, size_t* bytes);
+int grid_gpu_linear_commit_dev(const grid_gpu_matrix* A_msg, const grid_gpu_matrix* A_open,
+                               const uint32_t* m, const uint32_t* r, size_t batch, uint32_t* t,
+                               void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---- BDLOP parts: recompute_bdlop_parts_runtime (commit/src/linear.rs:552-573,
+ *      800-938): u = A_mask * r and v = A_msg * m + A_open * r per batch entry
+ *      (A_mask and A_open share the randomness: equal column counts). ------- */
+int grid_gpu_bdlop_workspace(const grid_gpu_matrix* A_mask, const grid_gpu_matrix* A_msg,
+                             const grid_gpu_matrix* A_open, size_t batch, size_t* bytes);
+int grid_gpu_bdlop_commit_dev(const grid_gpu_matrix* A_mask, const grid_gpu_matrix* A_msg,
+                              const grid_gpu_matrix* A_open, const uint32_t* m, const uint32_t* r,
+                              size_t batch, uint32_t* u, uint32_t* v, void* workspace,
+                              size_t workspace_bytes, void* stream);
+int grid_gpu_bdlop_commit(grid_gpu_matrix* A_mask, grid_gpu_matrix* A_msg, grid_gpu_matrix* A_open,
+                          const uint32_t* m, const uint32_t* r, size_t batch, uint32_t* u,
+                          uint32_t* v);
 
 /* ---- Gram matrix: compute_garbage_g (labrador/src/main_protocol/garbage.rs:76-93)
  *      G[idx(i,j)] = <s_i, s_j> for i <= j, row-major upper triangle

@@ -73,6 +73,14 @@ SIGNATURES = {
     "grid_gpu_gram_workspace": (C.c_int, [_vp, C.c_size_t, C.c_size_t, C.POINTER(C.c_size_t)]),
     "grid_gpu_gram_dev": (C.c_int, [_vp, _vp, C.c_size_t, C.c_size_t, _vp, _vp, C.c_size_t, _vp]),
     "grid_gpu_gram": (C.c_int, [_vp, _vp, C.c_size_t, C.c_size_t, _vp]),
+    "grid_gpu_linear_commit_workspace": (C.c_int, [_vp, _vp, C.c_size_t,
+                                                   C.POINTER(C.c_size_t)]),
+    "grid_gpu_linear_commit_dev": (C.c_int, [_vp, _vp, _vp, _vp, C.c_size_t, _vp, _vp,
+                                             C.c_size_t, _vp]),
+    "grid_gpu_bdlop_workspace": (C.c_int, [_vp, _vp, _vp, C.c_size_t, C.POINTER(C.c_size_t)]),
+    "grid_gpu_bdlop_commit_dev": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_size_t, _vp, _vp, _vp,
+                                            C.c_size_t, _vp]),
+    "grid_gpu_bdlop_commit": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_size_t, _vp, _vp]),
     "grid_gpu_garbage_h_workspace": (C.c_int, [_vp, C.c_size_t, C.c_size_t,
                                                C.POINTER(C.c_size_t)]),
     "grid_gpu_garbage_h_dev": (C.c_int, [_vp, _vp, _vp, C.c_size_t, C.c_size_t, _vp, _vp,

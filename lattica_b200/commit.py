@@ -104,10 +104,13 @@ class LinearCommitmentKey:
     def __init__(self, plan: TwistedNttPlan, a_msg, a_open, dims: CommitmentDimensions):
         dims.validate()
         d = plan.d
-        a_msg = np.ascontiguousarray(a_msg, dtype=np.uint32)
-        a_open = np.ascontiguousarray(a_open, dtype=np.uint32)
-        if (a_msg.size != dims.commitment_len * dims.message_len * d
-                or a_open.size != dims.commitment_len * dims.opening_len * d):
+        if not _is_torch(a_msg):
+            a_msg = np.ascontiguousarray(a_msg, dtype=np.uint32)
+        if not _is_torch(a_open):
+            a_open = np.ascontiguousarray(a_open, dtype=np.uint32)
+        size = lambda a: a.numel() if _is_torch(a) else a.size
+        if (size(a_msg) != dims.commitment_len * dims.message_len * d
+                or size(a_open) != dims.commitment_len * dims.opening_len * d):
             raise CommitmentError("DimensionMismatch")  # validate_linear_matrices
         self.plan, self.dims = plan, dims
         self.a_msg = PreparedMatrix(plan, a_msg, dims.commitment_len, dims.message_len)
@@ -115,23 +118,101 @@ class LinearCommitmentKey:
 
     def recompute(self, message, randomness):
         """t = A_msg * m + A_open * r (recompute_linear_commitment_parts_trusted,
-        commit/src/linear.rs:476-506); message (batch?, message_len, d)."""
+        commit/src/linear.rs:476-506); message (batch?, message_len, d),
+        randomness (batch?, opening_len, d): numpy uint32 or CUDA tensors."""
         d = self.plan.d
+        if tuple(message.shape[-2:]) != (self.dims.message_len, d):
+            raise CommitmentError("DimensionMismatch")  # validate_message
+        if tuple(randomness.shape[-2:]) != (self.dims.opening_len, d):
+            raise CommitmentError("DimensionMismatch")  # validate_opening_randomness
+        batch = int(np.prod(message.shape[:-2])) if len(message.shape) > 2 else 1
+        if (int(np.prod(randomness.shape[:-2])) if len(randomness.shape) > 2 else 1) != batch:
+            raise CommitmentError("DimensionMismatch")
+        if _is_torch(message):
+            import torch
+            lib = _lib.load()
+            t = torch.empty((*message.shape[:-2], self.dims.commitment_len, d),
+                            dtype=message.dtype, device=message.device)
+            nb = C.c_size_t()
+            raise_status(lib.grid_gpu_linear_commit_workspace(self.a_msg.handle,
+                                                              self.a_open.handle, batch,
+                                                              C.byref(nb)),
+                         "grid_gpu_linear_commit_workspace")
+            ws = torch.empty(max(16, nb.value), dtype=torch.uint8, device=message.device)
+            st = lib.grid_gpu_linear_commit_dev(self.a_msg.handle, self.a_open.handle,
+                                                message.data_ptr(), randomness.data_ptr(), batch,
+                                                t.data_ptr(), ws.data_ptr(), ws.numel(),
+                                                _stream_ptr(message))
+            raise_status(st, "grid_gpu_linear_commit_dev")
+            return t
         m = np.ascontiguousarray(message, dtype=np.uint32)
         r = np.ascontiguousarray(randomness, dtype=np.uint32)
-        if m.shape[-2:] != (self.dims.message_len, d):
-            raise CommitmentError("DimensionMismatch")  # validate_message
-        if r.shape[-2:] != (self.dims.opening_len, d):
-            raise CommitmentError("DimensionMismatch")  # validate_opening_randomness
-        batch = int(np.prod(m.shape[:-2])) if m.ndim > 2 else 1
-        if (int(np.prod(r.shape[:-2])) if r.ndim > 2 else 1) != batch:
-            raise CommitmentError("DimensionMismatch")
         t = np.empty((*m.shape[:-2], self.dims.commitment_len, d), dtype=np.uint32)
         st = _lib.load().grid_gpu_linear_commit(self.a_msg.handle, self.a_open.handle,
                                                 m.ctypes.data, r.ctypes.data, batch,
                                                 t.ctypes.data)
         raise_status(st, "grid_gpu_linear_commit")
         return t
+
+
+class BdlopCommitmentKey:
+    """BdlopCommitmentKey (commit/src/bdlop/params.rs:90-135) with its three
+    matrices prepared on the device: A_mask (rows x opening_len), A_msg
+    (rows x message_len), A_open (rows x opening_len)."""
+
+    def __init__(self, plan: TwistedNttPlan, a_mask, a_msg, a_open, rows: int,
+                 message_len: int, opening_len: int):
+        d = plan.d
+        mats = []
+        for a, cols in ((a_mask, opening_len), (a_msg, message_len), (a_open, opening_len)):
+            if not _is_torch(a):
+                a = np.ascontiguousarray(a, dtype=np.uint32)
+            if rows == 0 or cols == 0 or (a.numel() if _is_torch(a) else a.size) != rows * cols * d:
+                raise CommitmentError("DimensionMismatch")  # BdlopCommitmentKey::is_valid
+            mats.append(PreparedMatrix(plan, a, rows, cols))
+        self.plan, self.rows = plan, rows
+        self.message_len, self.opening_len = message_len, opening_len
+        self.a_mask, self.a_msg, self.a_open = mats
+
+    def recompute_parts(self, message, randomness):
+        """(u, v) = (A_mask r, A_msg m + A_open r) per batch entry
+        (recompute_bdlop_parts_runtime, commit/src/linear.rs:552-573, 800-938).
+        message (batch?, message_len, d), randomness (batch?, opening_len, d):
+        numpy uint32 or CUDA tensors (both the same kind)."""
+        d = self.plan.d
+        if tuple(message.shape[-2:]) != (self.message_len, d):
+            raise CommitmentError("DimensionMismatch")
+        if tuple(randomness.shape[-2:]) != (self.opening_len, d):
+            raise CommitmentError("DimensionMismatch")
+        batch = int(np.prod(message.shape[:-2])) if len(message.shape) > 2 else 1
+        if (int(np.prod(randomness.shape[:-2])) if len(randomness.shape) > 2 else 1) != batch:
+            raise CommitmentError("DimensionMismatch")
+        lib = _lib.load()
+        shape = (*message.shape[:-2], self.rows, d)
+        if _is_torch(message):
+            import torch
+            u = torch.empty(shape, dtype=message.dtype, device=message.device)
+            v = torch.empty(shape, dtype=message.dtype, device=message.device)
+            nb = C.c_size_t()
+            raise_status(lib.grid_gpu_bdlop_workspace(self.a_mask.handle, self.a_msg.handle,
+                                                      self.a_open.handle, batch, C.byref(nb)),
+                         "grid_gpu_bdlop_workspace")
+            ws = torch.empty(max(16, nb.value), dtype=torch.uint8, device=message.device)
+            st = lib.grid_gpu_bdlop_commit_dev(self.a_mask.handle, self.a_msg.handle,
+                                               self.a_open.handle, message.data_ptr(),
+                                               randomness.data_ptr(), batch, u.data_ptr(),
+                                               v.data_ptr(), ws.data_ptr(), ws.numel(),
+                                               _stream_ptr(message))
+        else:
+            m = np.ascontiguousarray(message, dtype=np.uint32)
+            r = np.ascontiguousarray(randomness, dtype=np.uint32)
+            u = np.empty(shape, dtype=np.uint32)
+            v = np.empty(shape, dtype=np.uint32)
+            st = lib.grid_gpu_bdlop_commit(self.a_mask.handle, self.a_msg.handle,
+                                           self.a_open.handle, m.ctypes.data, r.ctypes.data,
+                                           batch, u.ctypes.data, v.ctypes.data)
+        raise_status(st, "grid_gpu_bdlop_commit")
+        return u, v
 
 
 class AjtaiCommitment:

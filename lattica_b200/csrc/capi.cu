@@ -218,6 +218,39 @@ int grid_gpu_commit(grid_gpu_matrix* A, const uint32_t* s, size_t batch, uint32_
   return rc ? rc : fin;
 }
 
+int grid_gpu_linear_commit_workspace(const grid_gpu_matrix* A_msg, const grid_gpu_matrix* A_open,
+                                     size_t batch, size_t* bytes) {
+  if (!A_msg || !A_open || !bytes) return GRID_ERR_NULL_POINTER;
+  const grid_gpu_plan* p = A_msg->plan;
+  *bytes = commit_ws_bytes(p, A_msg->rows, A_msg->cols, batch) +
+           commit_ws_bytes(p, A_open->rows, A_open->cols, batch) +
+           words_bytes(batch * A_open->rows * p->d);
+  return GRID_OK;
+}
+
+int grid_gpu_linear_commit_dev(const grid_gpu_matrix* A_msg, const grid_gpu_matrix* A_open,
+                               const uint32_t* m, const uint32_t* r, size_t batch, uint32_t* t,
+                               void* workspace, size_t workspace_bytes, void* stream) {
+  if (!A_msg || !A_open || ((!m || !r || !t) && batch)) return GRID_ERR_NULL_POINTER;
+  if (A_msg->plan != A_open->plan) return GRID_ERR_INVALID_PARAMETERS;
+  if (A_msg->rows != A_open->rows) return GRID_ERR_DIMENSION_MISMATCH;
+  if (batch == 0) return GRID_OK;
+  if (!dims_ok(batch, A_msg->rows, A_msg->cols) || !dims_ok(batch, A_open->rows, A_open->cols))
+    return GRID_ERR_INVALID_PARAMETERS;
+  if (!aligned16(m) || !aligned16(r) || !aligned16(t) || !aligned16(workspace))
+    return GRID_ERR_MISALIGNED;
+  const grid_gpu_plan* p = A_msg->plan;
+  cudaStream_t st = (cudaStream_t)stream;
+  Carver cv(workspace, workspace_bytes);
+  uint32_t* t2 = cv.take<uint32_t>(batch * A_open->rows * p->d);
+  if (!cv.ok) return GRID_ERR_INVALID_PARAMETERS;
+  int rc = commit_core(A_msg, m, batch, t, cv, st);
+  if (!rc) rc = commit_core(A_open, r, batch, t2, cv, st);
+  // A_msg*m + A_open*r: INTT is linear, so adding the coefficient forms is exact.
+  if (!rc) rc = launch_add(p, t, t2, batch * A_open->rows * p->d, st);
+  return rc;
+}
+
 int grid_gpu_linear_commit(grid_gpu_matrix* A_msg, grid_gpu_matrix* A_open, const uint32_t* m,
                            const uint32_t* r, size_t batch, uint32_t* t) {
   if (!A_msg || !A_open || ((!m || !r || !t) && batch)) return GRID_ERR_NULL_POINTER;
@@ -251,6 +284,88 @@ int grid_gpu_linear_commit(grid_gpu_matrix* A_msg, grid_gpu_matrix* A_open, cons
   // A_msg*m + A_open*r: INTT is linear, so adding the coefficient forms is exact.
   if (!rc) rc = launch_add(p, t1, t2, batch * rows * d, st);
   if (!rc) rc = cuda_status(cudaMemcpyAsync(t, t1, t_bytes, cudaMemcpyDeviceToHost, st));
+  const int fin = finish_host_call(p, st);
+  return rc ? rc : fin;
+}
+
+/* ---- BDLOP parts: u = A_mask * r, v = A_msg * m + A_open * r ---------- */
+
+int grid_gpu_bdlop_workspace(const grid_gpu_matrix* A_mask, const grid_gpu_matrix* A_msg,
+                             const grid_gpu_matrix* A_open, size_t batch, size_t* bytes) {
+  if (!A_mask || !A_msg || !A_open || !bytes) return GRID_ERR_NULL_POINTER;
+  const grid_gpu_plan* p = A_msg->plan;
+  *bytes = commit_ws_bytes(p, A_mask->rows, A_mask->cols, batch) +
+           commit_ws_bytes(p, A_msg->rows, A_msg->cols, batch) +
+           commit_ws_bytes(p, A_open->rows, A_open->cols, batch) +
+           words_bytes(batch * A_open->rows * p->d);
+  return GRID_OK;
+}
+
+int grid_gpu_bdlop_commit_dev(const grid_gpu_matrix* A_mask, const grid_gpu_matrix* A_msg,
+                              const grid_gpu_matrix* A_open, const uint32_t* m, const uint32_t* r,
+                              size_t batch, uint32_t* u, uint32_t* v, void* workspace,
+                              size_t workspace_bytes, void* stream) {
+  if (!A_mask || !A_msg || !A_open || ((!m || !r || !u || !v) && batch))
+    return GRID_ERR_NULL_POINTER;
+  if (A_mask->plan != A_msg->plan || A_open->plan != A_msg->plan)
+    return GRID_ERR_INVALID_PARAMETERS;
+  // the mask and the opening part multiply the same randomness
+  if (A_msg->rows != A_open->rows || A_mask->cols != A_open->cols)
+    return GRID_ERR_DIMENSION_MISMATCH;
+  if (batch == 0) return GRID_OK;
+  if (!dims_ok(batch, A_msg->rows, A_msg->cols) || !dims_ok(batch, A_mask->rows, A_mask->cols))
+    return GRID_ERR_INVALID_PARAMETERS;
+  if (!aligned16(m) || !aligned16(r) || !aligned16(u) || !aligned16(v) || !aligned16(workspace))
+    return GRID_ERR_MISALIGNED;
+  const grid_gpu_plan* p = A_msg->plan;
+  cudaStream_t st = (cudaStream_t)stream;
+  Carver cv(workspace, workspace_bytes);
+  uint32_t* t2 = cv.take<uint32_t>(batch * A_open->rows * p->d);
+  if (!cv.ok) return GRID_ERR_INVALID_PARAMETERS;
+  int rc = commit_core(A_mask, r, batch, u, cv, st);
+  if (!rc) rc = commit_core(A_msg, m, batch, v, cv, st);
+  if (!rc) rc = commit_core(A_open, r, batch, t2, cv, st);
+  // A_msg*m + A_open*r: INTT is linear, so adding the coefficient forms is exact.
+  if (!rc) rc = launch_add(p, v, t2, batch * A_open->rows * p->d, st);
+  return rc;
+}
+
+int grid_gpu_bdlop_commit(grid_gpu_matrix* A_mask, grid_gpu_matrix* A_msg, grid_gpu_matrix* A_open,
+                          const uint32_t* m, const uint32_t* r, size_t batch, uint32_t* u,
+                          uint32_t* v) {
+  if (!A_mask || !A_msg || !A_open || ((!m || !r || !u || !v) && batch))
+    return GRID_ERR_NULL_POINTER;
+  if (A_mask->plan != A_msg->plan || A_open->plan != A_msg->plan)
+    return GRID_ERR_INVALID_PARAMETERS;
+  if (A_msg->rows != A_open->rows || A_mask->cols != A_open->cols)
+    return GRID_ERR_DIMENSION_MISMATCH;
+  if (batch == 0) return GRID_OK;
+  grid_gpu_plan* p = A_msg->plan;
+  std::lock_guard<std::mutex> lk(p->mu);
+  const size_t d = p->d;
+  const size_t m_bytes = batch * A_msg->cols * d * 4, r_bytes = batch * A_open->cols * d * 4;
+  const size_t u_bytes = batch * A_mask->rows * d * 4, v_bytes = batch * A_msg->rows * d * 4;
+  size_t ws = 0;
+  int rc = grid_gpu_bdlop_workspace(A_mask, A_msg, A_open, batch, &ws);
+  if (rc || (rc = ensure_scratch(p, 6, m_bytes)) || (rc = ensure_scratch(p, 7, r_bytes)) ||
+      (rc = ensure_scratch(p, 9, v_bytes)) || (rc = ensure_scratch(p, 10, u_bytes)) ||
+      (rc = ensure_scratch(p, 8, ws)))
+    return rc;
+  cudaStream_t st = p->stream;
+  rc = cuda_status(cudaMemcpyAsync(p->scratch[6].ptr, m, m_bytes, cudaMemcpyHostToDevice, st));
+  if (!rc)
+    rc = cuda_status(cudaMemcpyAsync(p->scratch[7].ptr, r, r_bytes, cudaMemcpyHostToDevice, st));
+  if (!rc)
+    rc = grid_gpu_bdlop_commit_dev(A_mask, A_msg, A_open,
+                                   static_cast<uint32_t*>(p->scratch[6].ptr),
+                                   static_cast<uint32_t*>(p->scratch[7].ptr), batch,
+                                   static_cast<uint32_t*>(p->scratch[10].ptr),
+                                   static_cast<uint32_t*>(p->scratch[9].ptr), p->scratch[8].ptr,
+                                   ws, st);
+  if (!rc)
+    rc = cuda_status(cudaMemcpyAsync(u, p->scratch[10].ptr, u_bytes, cudaMemcpyDeviceToHost, st));
+  if (!rc)
+    rc = cuda_status(cudaMemcpyAsync(v, p->scratch[9].ptr, v_bytes, cudaMemcpyDeviceToHost, st));
   const int fin = finish_host_call(p, st);
   return rc ? rc : fin;
 }

@@ -178,6 +178,41 @@ __global__ void __launch_bounds__(kEmmThreads, 1) emm_kernel(
   }
 }
 
+constexpr int kMvMaxRows = 4;
+constexpr int kMvThreads = 256;
+
+// Products with at most four X rows (a matrix times one to four vectors, e.g.
+// an outer commitment or a single commit): one thread per (Y row n,
+// evaluation point e) keeps the M accumulators. Consecutive threads read
+// consecutive evaluation points, so Y streams through once, coalesced, and the
+// few X words are shared through L1 / L2; the tiled kernel would spend all but
+// M of its 32 or 64 tile rows on padding here.
+__global__ void __launch_bounds__(kMvThreads) emv_kernel(
+    const uint32_t* __restrict__ X, const uint32_t* __restrict__ Y, uint32_t* __restrict__ out,
+    int M, int N, int K, int ldy, int d, int k_per_split, size_t split_stride, FieldParams f) {
+  const size_t w = (size_t)blockIdx.x * kMvThreads + threadIdx.x;
+  if (w >= (size_t)N * d) return;
+  const int n = (int)(w / d), e = (int)(w % d);
+  const int kbeg = (int)blockIdx.y * k_per_split;
+  const int kend = min(K, kbeg + k_per_split);
+  Acc96 acc[kMvMaxRows];
+#pragma unroll
+  for (int m = 0; m < kMvMaxRows; ++m) acc96_zero(acc[m]);
+  const uint32_t* yp = Y + (size_t)n * ldy * d + e;
+  const uint32_t* xp = X + e;
+#pragma unroll 4
+  for (int k = kbeg; k < kend; ++k) {
+    const uint32_t y = __ldg(yp + (size_t)k * d);
+#pragma unroll
+    for (int m = 0; m < kMvMaxRows; ++m)
+      if (m < M) acc96_mad(acc[m], __ldg(xp + ((size_t)m * K + k) * d), y);
+  }
+  uint32_t* o = out + (size_t)blockIdx.y * split_stride;
+#pragma unroll
+  for (int m = 0; m < kMvMaxRows; ++m)
+    if (m < M) o[((size_t)m * N + n) * d + e] = acc96_reduce(acc[m], f);
+}
+
 // out[i] = sum_s part[s][i] mod q (exact; partials are canonical).
 __global__ void sum_splits_kernel(const uint32_t* __restrict__ part, uint32_t* __restrict__ out,
                                   size_t n, int splits, uint32_t q) {
@@ -191,6 +226,7 @@ __global__ void sum_splits_kernel(const uint32_t* __restrict__ part, uint32_t* _
 
 // Launch geometry of one product: tile shape, tiles and the K split.
 struct EmmGeometry {
+  bool mv;  // emv_kernel (dense, M <= kMvMaxRows) instead of the tiled kernel
   int tmg, tiles_m, tiles_n, tiles, splits, k_per_split;
 };
 
@@ -199,6 +235,19 @@ struct EmmGeometry {
 // two of them; split partials go to the workspace and are summed after.
 EmmGeometry emm_geometry(int M, int N, int K, int d, int mode, int num_sms) {
   EmmGeometry g;
+  g.mv = mode == OUT_DENSE && M <= kMvMaxRows;
+  if (g.mv) {
+    // memory bound: about four 256-thread CTAs per SM, at least 32 K steps each
+    const long long blocks = ((long long)N * d + kMvThreads - 1) / kMvThreads;
+    long long want = 4LL * num_sms / blocks;
+    if (want > K / 32) want = K / 32;
+    if (want < 1) want = 1;
+    g.k_per_split = (int)((K + want - 1) / want);
+    g.splits = (K + g.k_per_split - 1) / g.k_per_split;
+    g.tmg = g.tiles_m = g.tiles_n = 0;
+    g.tiles = (int)blocks;
+    return g;
+  }
   g.tmg = (mode == OUT_DENSE && N <= 16) ? 16 : 8;
   const int bm = 4 * g.tmg, bn = 8 * (32 / g.tmg);
   g.tiles_m = (M + bm - 1) / bm;
@@ -248,11 +297,17 @@ int launch_emm(const grid_gpu_plan* p, const uint32_t* X, const uint32_t* Y, int
   const int splits = g.splits;
   const size_t outputs = mode == OUT_UPPER ? (size_t)M * (M + 1) / 2 : (size_t)M * N;
   const size_t stride = outputs * p->d;
-  dim3 grid(p->d / EG, g.tiles, splits);
   uint32_t* dst = splits > 1 ? work : out_evals;
   if (splits > 1 && !work) return GRID_ERR_NULL_POINTER;
-  int rc = g.tmg == 16 ? launch_emm_tile<16>(grid, X, Y, dst, M, N, K, ldy, mode, g, stride, p, s)
-                       : launch_emm_tile<8>(grid, X, Y, dst, M, N, K, ldy, mode, g, stride, p, s);
+  int rc = GRID_OK;
+  if (g.mv) {
+    emv_kernel<<<dim3((unsigned)g.tiles, splits), kMvThreads, 0, s>>>(
+        X, Y, dst, M, N, K, ldy, (int)p->d, g.k_per_split, stride, p->f);
+  } else {
+    dim3 grid(p->d / EG, g.tiles, splits);
+    rc = g.tmg == 16 ? launch_emm_tile<16>(grid, X, Y, dst, M, N, K, ldy, mode, g, stride, p, s)
+                     : launch_emm_tile<8>(grid, X, Y, dst, M, N, K, ldy, mode, g, stride, p, s);
+  }
   if (rc) return rc;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_status(e);

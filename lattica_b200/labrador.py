@@ -146,6 +146,30 @@ class CommitKey:
         return decompose_polys(self.plan, np.asarray(t).reshape(-1, self.plan.d), b1, t1)
 
 
+class OuterCommitKey:
+    """The outer-commitment matrices of a LaBRADOR CommitKey (crs.rs:111-123):
+    B (kappa1 x t_len), C (kappa1 x g_len), D (kappa2 x h_len), prepared on the
+    device."""
+
+    def __init__(self, plan: TwistedNttPlan, b, c, d, kappa1: int, kappa2: int, t_len: int,
+                 g_len: int, h_len: int):
+        from .commit import CommitmentDimensions, LinearCommitmentKey
+        self.plan = plan
+        self.bc = LinearCommitmentKey(plan, b, c, CommitmentDimensions(t_len, g_len, kappa1))
+        if not _is_torch(d):
+            d = np.ascontiguousarray(d, dtype=np.uint32)
+        self.d = PreparedMatrix(plan, d, kappa2, h_len)
+
+    def outer_commit_u1_slice(self, t, g):
+        """u1 = B t + C g (crs.rs:272-285); t (t_len, d), g (g_len, d): numpy
+        uint32 or CUDA tensors (both the same kind)."""
+        return self.bc.recompute(t, g)
+
+    def outer_commit_u2_slice(self, h):
+        """u2 = D h (crs.rs:297-303); h (h_len, d), numpy uint32 or a CUDA tensor."""
+        return self.d.mul_vec(h)
+
+
 class JLMatrix:
     """Seeded JL projection (labrador/src/jl.rs:34-509): ChaCha20 keystream,
     key = seed, nonce = part index."""

@@ -31,6 +31,7 @@ def _host(t):
 
 @pytest.mark.parametrize("q,d,rows,cols,batch", [
     (Q, 64, 8, 64, 64),         # plain Ajtai commit shape
+    (Q, 64, 16, 3000, 1),       # one vector, long K: the matrix-vector kernel with K splits
     (Q, 64, 16, 300, 5),
     (12289, 64, 3, 5, 7),
     (17, 8, 2, 9, 3),
