@@ -190,6 +190,19 @@ int grid_gpu_gram_dev(const grid_gpu_plan* plan, const uint32_t* S, size_t r, si
                       uint32_t* G, void* workspace, size_t workspace_bytes, void* stream);
 int grid_gpu_gram(grid_gpu_plan* plan, const uint32_t* S, size_t r, size_t n, uint32_t* G);
 
+/* ---- JL evaluations, aggregation side: jl_rows_flat_to_conjugated_polys +
+ *      the jl_evals loop of prove_step (labrador/src/main_protocol/mod.rs:885-923,
+ *      step_prover.rs:185-206): evals[m] = sum_{i,j} conj(pi_{m,i,j}) * s_{i,j}
+ *      for the rows x (num_parts * cols) JL matrix of `seed`, straight from the
+ *      keystream (the int8 entries are never stored). evals: rows x d words.
+ *      Kernel shape: rows = 256, d = 64 (else GRID_ERR_UNSUPPORTED_SIZE). -- */
+int grid_gpu_jl_evals_workspace(size_t* bytes);
+int grid_gpu_jl_evals_dev(const grid_gpu_plan* plan, const uint8_t* seed, size_t rows,
+                          const uint32_t* parts, size_t num_parts, size_t cols, size_t d,
+                          uint32_t* evals, void* workspace, size_t workspace_bytes, void* stream);
+int grid_gpu_jl_evals(grid_gpu_plan* plan, const uint8_t* seed, size_t rows, const uint32_t* parts,
+                      size_t num_parts, size_t cols, size_t d, uint32_t* evals);
+
 /* ---- garbage h: compute_garbage_h (labrador/src/main_protocol/garbage.rs:101-133)
  *      H[idx(i,j)] = (<phi_i, s_j> + <phi_j, s_i>) * 2^-1 for i <= j, row-major upper
  *      triangle (garbage_index, main_protocol/mod.rs:664-670). S, Phi: r x n polys. */

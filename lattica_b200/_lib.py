@@ -73,6 +73,11 @@ SIGNATURES = {
     "grid_gpu_gram_workspace": (C.c_int, [_vp, C.c_size_t, C.c_size_t, C.POINTER(C.c_size_t)]),
     "grid_gpu_gram_dev": (C.c_int, [_vp, _vp, C.c_size_t, C.c_size_t, _vp, _vp, C.c_size_t, _vp]),
     "grid_gpu_gram": (C.c_int, [_vp, _vp, C.c_size_t, C.c_size_t, _vp]),
+    "grid_gpu_jl_evals_workspace": (C.c_int, [C.POINTER(C.c_size_t)]),
+    "grid_gpu_jl_evals_dev": (C.c_int, [_vp, _vp, C.c_size_t, _vp, C.c_size_t, C.c_size_t,
+                                        C.c_size_t, _vp, _vp, C.c_size_t, _vp]),
+    "grid_gpu_jl_evals": (C.c_int, [_vp, _vp, C.c_size_t, _vp, C.c_size_t, C.c_size_t,
+                                    C.c_size_t, _vp]),
     "grid_gpu_linear_commit_workspace": (C.c_int, [_vp, _vp, C.c_size_t,
                                                    C.POINTER(C.c_size_t)]),
     "grid_gpu_linear_commit_dev": (C.c_int, [_vp, _vp, _vp, _vp, C.c_size_t, _vp, _vp,

@@ -8,6 +8,7 @@ the median CUDA-event time.
     python -m lattica_b200.cases commit --reps 4     # 16 x 2048 matrix times 64 witnesses
     python -m lattica_b200.cases garbage_h --reps 4  # h = sym(Phi S^T) / 2, r = 64, n = 2048
     python -m lattica_b200.cases amortize --reps 4   # z = sum_i c_i s_i, r = 64, n = 2048
+    python -m lattica_b200.cases jl_evals --reps 4   # 256 conjugated JL evaluations, same witness
     python -m lattica_b200.cases ntt256 --reps 4     # d = 256 products, 2^20 polys at q'
 
 Sizes: r = 64 witness vectors of n = 2048 polys (d = 64, coefficients in
@@ -33,7 +34,7 @@ def build(case: str):
     """Returns a zero-argument callable that runs one instance of `case`."""
     import torch
     from lattica_b200 import TwistedNttPlan
-    from lattica_b200.labrador import (CommitKey, amortize_witness, compute_garbage_g,
+    from lattica_b200.labrador import (CommitKey, JLMatrix, amortize_witness, compute_garbage_g,
                                        compute_garbage_h, prover_round_dev)
     dev = torch.device("cuda:0")
     g = torch.Generator(device=dev).manual_seed(5)
@@ -50,6 +51,10 @@ def build(case: str):
     if case == "garbage_h":
         phis = _uniform(torch, dev, g, Q, (r, n, 64))
         return lambda: compute_garbage_h(plan, wit, phis)
+    if case == "jl_evals":
+        jl = JLMatrix(bytes(range(32)), 256, n * 64)
+        flat = wit.reshape(r, n * 64)
+        return lambda: jl.conjugated_evals(plan, flat, r, 64)
     if case == "amortize":
         chal = _uniform(torch, dev, g, Q, (r, 64))
         return lambda: amortize_witness(plan, wit, chal)
@@ -64,7 +69,8 @@ def build(case: str):
 
 def main(argv=None) -> None:
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
-    ap.add_argument("case", choices=["round", "gram", "garbage_h", "amortize", "commit", "ntt256"])
+    ap.add_argument("case", choices=["round", "gram", "garbage_h", "amortize", "jl_evals", "commit",
+                                       "ntt256"])
     ap.add_argument("--reps", type=int, default=4)
     args = ap.parse_args(argv)
     import torch

@@ -575,6 +575,48 @@ int grid_gpu_jl_project(grid_gpu_plan* p, const uint8_t* seed, size_t rows,
   return rc ? rc : fin;
 }
 
+/* ---- JL evaluations (aggregation side) --------------------------------- */
+
+int grid_gpu_jl_evals_workspace(size_t* bytes) {
+  if (!bytes) return GRID_ERR_NULL_POINTER;
+  *bytes = round_up(jl_evals_scratch_bytes(), 256);
+  return GRID_OK;
+}
+
+int grid_gpu_jl_evals_dev(const grid_gpu_plan* p, const uint8_t* seed, size_t rows,
+                          const uint32_t* parts, size_t num_parts, size_t cols, size_t d,
+                          uint32_t* evals, void* workspace, size_t workspace_bytes, void* stream) {
+  if (!p || !seed || !evals || !parts) return GRID_ERR_NULL_POINTER;
+  if (d != p->d) return GRID_ERR_INVALID_PARAMETERS;
+  if (!aligned16(workspace)) return GRID_ERR_MISALIGNED;
+  return launch_jl_evals(p->f, seed, rows, parts, num_parts, cols, d, evals, workspace,
+                         workspace_bytes, p->num_sms, p->d_err, (cudaStream_t)stream);
+}
+
+int grid_gpu_jl_evals(grid_gpu_plan* p, const uint8_t* seed, size_t rows, const uint32_t* parts,
+                      size_t num_parts, size_t cols, size_t d, uint32_t* evals) {
+  if (!p || !seed || !evals || !parts) return GRID_ERR_NULL_POINTER;
+  if (d != p->d || d == 0 || cols == 0 || cols % d || num_parts == 0)
+    return GRID_ERR_INVALID_PARAMETERS;
+  std::lock_guard<std::mutex> lk(p->mu);
+  const size_t in_bytes = num_parts * cols * 4, out_bytes = rows * d * 4;
+  const size_t ws = round_up(jl_evals_scratch_bytes(), 256);
+  int rc;
+  if ((rc = ensure_scratch(p, 6, in_bytes)) || (rc = ensure_scratch(p, 7, out_bytes)) ||
+      (rc = ensure_scratch(p, 8, ws)))
+    return rc;
+  cudaStream_t st = p->stream;
+  rc = cuda_status(cudaMemcpyAsync(p->scratch[6].ptr, parts, in_bytes, cudaMemcpyHostToDevice, st));
+  if (!rc)
+    rc = launch_jl_evals(p->f, seed, rows, static_cast<uint32_t*>(p->scratch[6].ptr), num_parts,
+                         cols, d, static_cast<uint32_t*>(p->scratch[7].ptr), p->scratch[8].ptr, ws,
+                         p->num_sms, p->d_err, st);
+  if (!rc)
+    rc = cuda_status(cudaMemcpyAsync(evals, p->scratch[7].ptr, out_bytes, cudaMemcpyDeviceToHost, st));
+  const int fin = finish_host_call(p, st);
+  return rc ? rc : fin;
+}
+
 /* ---- decompositions ---------------------------------------------------- */
 
 int grid_gpu_decompose_balanced_dev(const grid_gpu_plan* p, const uint32_t* polys, size_t npolys,

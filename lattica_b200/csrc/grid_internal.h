@@ -125,6 +125,12 @@ int launch_jl_project(const FieldParams& f, const uint8_t seed[32], size_t rows,
                       uint32_t* p_out, int8_t* flat_out, void* scratch, size_t scratch_bytes,
                       int num_sms, int* d_err, cudaStream_t s);
 size_t jl_scratch_bytes(size_t rows, size_t num_parts, int num_sms);
+// JL evaluations sum conj(pi_{m,i,j}) s_{i,j} (rows = 256, d = 64 only).
+size_t jl_evals_scratch_bytes();
+int launch_jl_evals(const FieldParams& f, const uint8_t seed[32], size_t rows,
+                    const uint32_t* parts, size_t num_parts, size_t cols, size_t d,
+                    uint32_t* evals, void* scratch, size_t scratch_bytes, int num_sms, int* err,
+                    cudaStream_t s);
 
 // plan.cu
 int host_pipeline(grid_gpu_plan* p, const uint32_t* const* ins, int nin, uint32_t* out,

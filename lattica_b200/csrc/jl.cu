@@ -401,6 +401,178 @@ __global__ void __launch_bounds__(kJlThreads) jl_flat_kernel(unsigned long long 
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// JL evaluations (aggregation side): evals[m] = sum_{i,j} conj(pi_{m,i,j}) s_{i,j}
+// (jl_rows_flat_to_conjugated_polys + the jl_evals loop of prove_step,
+// main_protocol/mod.rs:885-923, step_prover.rs:185-206), without the int8
+// entries ever being stored. Coefficient t of conj(pi) * s is
+// sum_u pi_u s'[u + t] with s' the negacyclic extension (s'[v] = -s[v - d] for
+// v >= d), so coefficient t of evals[m] is the JL projection of the witness
+// with every polynomial multiplied by X^-t. One keystream therefore serves all
+// d = 64 coefficients: column (j, u) of the B tile holds the 64 words
+// s'_j[u + t], t = 0 .. 63, as 256 bytes (N = 256), and D'[r][4t + i] =
+// sum_c M'[r][c] byte_i(s'[u_c + t]) accumulates in all 512 tensor-memory
+// columns (two 128-row halves). The M' = M + 1 correction
+// S[t][i] = sum_c byte_i(s'[u_c + t]) comes from per-position byte sums of each
+// coefficient and its negation: sum_{v >= t} P_i[v] + sum_{v < t} N_i[v].
+// ---------------------------------------------------------------------------
+constexpr uint32_t kEvB = 256u * kTcCols;                  // B tile: 256 bytes x 256 columns
+constexpr uint32_t kEvOffLut = kTcA + kEvB;
+constexpr uint32_t kEvOffPoly = kEvOffLut + 1024;          // the chunk's 4 polys (1 KB)
+constexpr uint32_t kEvOffSums = kEvOffPoly + 1024;         // P[64][4], N[64][4] (2 KB)
+constexpr uint32_t kEvOffS = kEvOffSums + 2048;            // S[64][4] (1 KB)
+constexpr uint32_t kEvOffBar = kEvOffS + 1024;
+constexpr uint32_t kEvSmem = kEvOffBar + 64 + 1024;        // + alignment slack
+constexpr int kEvD = 64, kEvRows = 256;
+
+__global__ void __launch_bounds__(kTcThreads, 1) jl_eval_tc_kernel(
+    const uint32_t* __restrict__ parts, unsigned long long cols, ChachaKey key,
+    unsigned long long nchunks, unsigned long long* __restrict__ gsum, uint32_t q,
+    int* __restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char sm_raw[];
+  const uint32_t raw = smem_addr(sm_raw);
+  unsigned char* sm = sm_raw + (((raw + 1023u) & ~1023u) - raw);
+  const uint32_t s0 = smem_addr(sm);
+  uint32_t* lut = reinterpret_cast<uint32_t*>(sm + kEvOffLut);
+  uint32_t* poly = reinterpret_cast<uint32_t*>(sm + kEvOffPoly);
+  uint32_t* sums = reinterpret_cast<uint32_t*>(sm + kEvOffSums);  // [0,256): P, [256,512): N
+  uint32_t* corr = reinterpret_cast<uint32_t*>(sm + kEvOffS);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kEvOffBar);
+  uint32_t* taddr_slot = reinterpret_cast<uint32_t*>(bar + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  for (int i = tid; i < 256; i += kTcThreads) lut[i] = shifted_entries_of_byte(i);
+  for (int i = tid; i < 512; i += kTcThreads) sums[i] = 0;
+  if (warp == 0) {
+    tc::tmem_alloc(taddr_slot, 512);
+    tc::tmem_relinquish();
+  }
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    fence_mbar_init();
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tbase = *taddr_slot;
+  // kind::i8, u8 x u8 -> s32, A and B MN-major, M = 128, N = 256
+  const uint32_t idesc = tc::idesc_u8(128, 256) | (1u << 15) | (1u << 16);
+
+  const unsigned long long per_part = (cols + kTcCols - 1) / kTcCols;
+  const uint32_t u = tid & (kEvD - 1);  // this thread's coefficient position in its poly
+  uint32_t psum[4] = {0, 0, 0, 0}, nsum[4] = {0, 0, 0, 0};
+  bool ok = true;
+  uint32_t it = 0;
+  for (unsigned long long ch = blockIdx.x; ch < nchunks; ch += gridDim.x, ++it) {
+    const uint32_t part = (uint32_t)(ch / per_part);
+    const unsigned long long c = (ch % per_part) * kTcCols + tid;
+    uint32_t w[16];
+    uint32_t x = 0;
+    if (c < cols) {
+      chacha20_block(key, (uint32_t)c, part, w);  // 256 rows: column c is block c
+      x = parts[(unsigned long long)part * cols + c];
+    } else {
+#pragma unroll
+      for (int i = 0; i < 16; ++i) w[i] = 0xFFFFFFFFu;  // padding column: x = 0
+    }
+    const uint32_t xn = x == 0 ? 0u : q - x;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      psum[i] += (x >> (8 * i)) & 0xFFu;
+      nsum[i] += (xn >> (8 * i)) & 0xFFu;
+    }
+    // the previous chunk's MMAs must be done reading the tiles
+    if (it > 0) ok = __syncthreads_and(mbar_wait(bar, (it - 1) & 1, err));
+    if (!ok) break;
+    poly[tid] = x;
+#pragma unroll
+    for (int g = 0; g < 16; ++g)
+      *reinterpret_cast<uint4*>(sm + jl_a_off(16 * g, tid)) =
+          make_uint4(lut[w[g] & 0xFFu], lut[(w[g] >> 8) & 0xFFu], lut[(w[g] >> 16) & 0xFFu],
+                     lut[w[g] >> 24]);
+    __syncthreads();  // the chunk's polys are staged
+    // B column tid: s'[u + t] for t = 0 .. 63, 16 bytes per group of 4 t
+    const uint32_t* pw = poly + (tid & ~(kEvD - 1));
+#pragma unroll
+    for (int g = 0; g < 16; ++g) {
+      uint32_t v4[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const uint32_t pos = u + 4 * g + k;
+        const uint32_t s = pw[pos & (kEvD - 1)];
+        v4[k] = pos < (uint32_t)kEvD ? s : (s == 0 ? 0u : q - s);
+      }
+      *reinterpret_cast<uint4*>(sm + kTcA + (tid >> 3) * 2048 + g * 128 + (tid & 7) * 16) =
+          make_uint4(v4[0], v4[1], v4[2], v4[3]);
+    }
+    tc::fence_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    if (tid == 0) {
+      tc::fence_after_sync();
+#pragma unroll
+      for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int ks = 0; ks < kTcCols / 32; ++ks)
+          tc::mma_u8(tbase + 256 * h, tc::smem_desc(s0 + h * 1024 + ks * 8192, 2048, 128),
+                     tc::smem_desc(s0 + kTcA + ks * 8192, 2048, 128), idesc,
+                     (it | (uint32_t)ks) != 0);
+      tc::mma_commit(bar);
+    }
+  }
+  if (ok && it > 0) ok = mbar_wait(bar, (it - 1) & 1, err);
+  ok = __syncthreads_and(ok);
+  // per-position byte sums of the coefficients and of their negations
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    atomicAdd(&sums[4 * u + i], psum[i]);
+    atomicAdd(&sums[256 + 4 * u + i], nsum[i]);
+  }
+  __syncthreads();
+  {
+    // S[t][i] = sum_{v >= t} P[v][i] + sum_{v < t} N[v][i], thread (t, i) = (tid / 4, tid % 4)
+    const int t = tid >> 2, i = tid & 3;
+    uint32_t acc = 0;
+    for (int v = 0; v < kEvD; ++v) acc += v >= t ? sums[4 * v + i] : sums[256 + 4 * v + i];
+    corr[tid] = acc;
+  }
+  __syncthreads();
+  tc::fence_after_sync();
+  if (ok && it > 0) {
+    const int h = warp >> 2, wl = warp & 3;
+    const int row = 128 * h + 32 * wl + lane;
+    const uint32_t base = tc::tmem_addr(tbase, 32 * wl, 256 * h);
+#pragma unroll 1
+    for (int t0 = 0; t0 < kEvD; t0 += 2) {
+      uint32_t dv[8];
+      tc::tmem_ld8(base + 4 * t0, dv);
+      tc::tmem_ld_wait();
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        const int t = t0 + k;
+        long long v = 0;
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          v += ((long long)dv[4 * k + i] - (long long)corr[4 * t + i]) << (8 * i);
+        long long r = v % (long long)q;
+        if (r < 0) r += q;
+        atomicAdd(&gsum[(size_t)row * kEvD + t], (unsigned long long)r);
+      }
+    }
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tbase, 512);
+}
+
+__global__ void jl_eval_finish_kernel(const unsigned long long* __restrict__ gsum,
+                                      uint32_t* __restrict__ evals, size_t n, uint32_t q) {
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+    evals[i] = (uint32_t)(gsum[i] % q);
+}
+
 }  // namespace
 
 size_t jl_scratch_bytes(size_t rows, size_t, int) { return 2 * rows * sizeof(unsigned long long); }
@@ -495,6 +667,48 @@ int launch_jl_project(const FieldParams& f, const uint8_t seed[32], size_t rows,
     if (e != cudaSuccess) return cuda_status(e);
   }
   return GRID_OK;
+}
+
+
+size_t jl_evals_scratch_bytes() { return (size_t)kEvRows * kEvD * sizeof(unsigned long long); }
+
+// evals: kEvRows x d words. Only the LaBRADOR shape (256 rows, d = 64) has a
+// kernel; other shapes return GRID_ERR_UNSUPPORTED_SIZE.
+int launch_jl_evals(const FieldParams& f, const uint8_t seed[32], size_t rows,
+                    const uint32_t* parts, size_t num_parts, size_t cols, size_t d,
+                    uint32_t* evals, void* scratch, size_t scratch_bytes, int num_sms, int* err,
+                    cudaStream_t s) {
+  if (rows != (size_t)kEvRows || d != (size_t)kEvD) return GRID_ERR_UNSUPPORTED_SIZE;
+  if (cols == 0 || cols % d != 0 || num_parts == 0 || num_parts > 0xFFFFFFFFull)
+    return GRID_ERR_INVALID_PARAMETERS;
+  if (scratch_bytes < jl_evals_scratch_bytes()) return GRID_ERR_INVALID_PARAMETERS;
+  ChachaKey key;
+  for (int i = 0; i < 8; ++i)
+    key.k[i] = (uint32_t)seed[4 * i] | ((uint32_t)seed[4 * i + 1] << 8) |
+               ((uint32_t)seed[4 * i + 2] << 16) | ((uint32_t)seed[4 * i + 3] << 24);
+  unsigned long long* gsum = static_cast<unsigned long long*>(scratch);
+  cudaError_t e = cudaMemsetAsync(gsum, 0, jl_evals_scratch_bytes(), s);
+  if (e != cudaSuccess) return cuda_status(e);
+  const unsigned long long nchunks = (cols + kTcCols - 1) / kTcCols * num_parts;
+  // one CTA per SM (all 512 tensor-memory columns); more CTAs only where a CTA
+  // would see more than kTcMaxColsPerCta columns (they queue for an SM)
+  unsigned long long grid = (unsigned long long)num_sms;
+  const unsigned long long need = (nchunks * kTcCols + kTcMaxColsPerCta - 1) / kTcMaxColsPerCta;
+  if (grid < need) grid = need;
+  if (grid > nchunks) grid = nchunks;
+  if (grid > 0x7FFFFFFFull) return GRID_ERR_INVALID_PARAMETERS;
+  int dev = 0;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return cuda_status(e);
+  static int bps_cache[kMaxDevices] = {};
+  int bps = 0;
+  int rc = prepare_kernel(jl_eval_tc_kernel, kEvSmem, kTcThreads, dev, bps_cache, &bps);
+  if (rc) return rc;
+  jl_eval_tc_kernel<<<(unsigned)grid, kTcThreads, kEvSmem, s>>>(parts, cols, key, nchunks, gsum,
+                                                               f.q, err);
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(e);
+  const size_t n = (size_t)kEvRows * kEvD;
+  jl_eval_finish_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(gsum, evals, n, f.q);
+  return cuda_status(cudaGetLastError());
 }
 
 }  // namespace grid

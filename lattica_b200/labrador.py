@@ -209,6 +209,38 @@ class JLMatrix:
     def project_multi(self, plan: TwistedNttPlan, parts, num_parts: int, d: int):
         return self.project_and_extract_jl_rows(plan, parts, num_parts, d, extract=False)[0]
 
+    def conjugated_evals(self, plan: TwistedNttPlan, parts, num_parts: int, d: int):
+        """jl_evals[m] = sum_{i,j} conj(pi_{m,i,j}) * s_{i,j}: the polynomials
+        prove_step builds from jl_rows_flat_to_conjugated_polys
+        (main_protocol/mod.rs:885-923, step_prover.rs:185-206), computed from
+        the keystream without the int8 entries. parts: (num_parts, cols)
+        numpy uint32 or a CUDA tensor; returns (rows, d). The kernel covers
+        rows = 256 and d = 64."""
+        if d <= 0 or self._cols % d:
+            raise ValueError(f"cols ({self._cols}) must be divisible by ring degree d ({d})")
+        lib = _lib.load()
+        seed = (C.c_uint8 * 32).from_buffer_copy(self.seed)
+        if _is_torch(parts):
+            import torch
+            if parts.numel() != num_parts * self._cols:
+                raise ValueError("parts count / length mismatch")
+            ev = torch.empty((self.rows, d), dtype=parts.dtype, device=parts.device)
+            nb = C.c_size_t()
+            raise_status(lib.grid_gpu_jl_evals_workspace(C.byref(nb)), "jl_evals_ws")
+            ws = torch.empty(max(16, nb.value), dtype=torch.uint8, device=parts.device)
+            st = lib.grid_gpu_jl_evals_dev(plan.handle, seed, self.rows, parts.data_ptr(),
+                                           num_parts, self._cols, d, ev.data_ptr(), ws.data_ptr(),
+                                           ws.numel(), _stream_ptr(parts))
+        else:
+            parts = np.ascontiguousarray(parts, dtype=np.uint32).reshape(-1)
+            if parts.size != num_parts * self._cols:
+                raise ValueError("parts count / length mismatch")
+            ev = np.empty((self.rows, d), dtype=np.uint32)
+            st = lib.grid_gpu_jl_evals(plan.handle, seed, self.rows, parts.ctypes.data,
+                                       num_parts, self._cols, d, ev.ctypes.data)
+        raise_status(st, "grid_gpu_jl_evals")
+        return ev
+
 
 @dataclass
 class RoundOutputs:

@@ -800,3 +800,36 @@ int orc_jl_project(const orc_field *f, const uint8_t seed[32], size_t rows, size
     free(partial);
     return ORC_OK;
 }
+
+/* jl_rows_flat_to_conjugated_polys (main_protocol/mod.rs:885-923) and the
+ * jl_evals loop of prove_step (step_prover.rs:185-206):
+ * evals[m] = sum_{i < num_parts} sum_j conj(pi_{m,i,j}) * s_{i,j}, where
+ * conj(pi)_0 = pi_0 and conj(pi)_k = -pi_{d-k}, each entry taken as the field
+ * element of a residue in {0, 1, q - 1} (R::from_u64). flat: the int8 entries
+ * [m][part][k][j] from orc_jl_project; parts: num_parts x (n * d) words. */
+int orc_jl_evals(const orc_plan *p, const int8_t *flat, size_t rows, const uint32_t *parts,
+                 size_t num_parts, size_t n, uint32_t *evals) {
+    const uint32_t d = p->n;
+    const uint64_t q = p->f.q;
+    uint32_t *conj = (uint32_t *)malloc(sizeof(uint32_t) * d);
+    uint32_t *prod = (uint32_t *)malloc(sizeof(uint32_t) * d);
+    if (!conj || !prod) { free(conj); free(prod); return ORC_ERR_OOM; }
+    for (size_t m = 0; m < rows; m++) {
+        uint32_t *out = evals + m * d;
+        for (uint32_t e = 0; e < d; e++) out[e] = 0;
+        for (size_t i = 0; i < num_parts; i++)
+            for (size_t j = 0; j < n; j++) {
+                for (uint32_t k = 0; k < d; k++) {
+                    const uint32_t src = k == 0 ? 0 : d - k;
+                    const int8_t v = flat[((m * num_parts + i) * d + src) * n + j];
+                    const uint64_t u = v < 0 ? q - (uint64_t)(-v) : (uint64_t)v;
+                    const uint64_t val = (k == 0 || u == 0) ? u : q - u;
+                    conj[k] = orc_to_mont(&p->f, val);
+                }
+                orc_poly_mul_ntt(p, conj, parts + (i * n + j) * d, prod);
+                for (uint32_t e = 0; e < d; e++) out[e] = orc_add(&p->f, out[e], prod[e]);
+            }
+    }
+    free(conj); free(prod);
+    return ORC_OK;
+}

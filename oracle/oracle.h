@@ -135,6 +135,11 @@ int orc_jl_project(const orc_field *f, const uint8_t seed[32], size_t rows, size
                    const uint32_t *parts, size_t num_parts, size_t d, uint32_t *p_out,
                    int8_t *flat_out, int threads);
 
+/* jl_rows_flat_to_conjugated_polys + jl_evals (main_protocol/mod.rs:885-923,
+ * step_prover.rs:185-206): evals[m] = sum conj(pi_{m,i,j}) * s_{i,j}. */
+int orc_jl_evals(const orc_plan *p, const int8_t *flat, size_t rows, const uint32_t *parts,
+                 size_t num_parts, size_t n, uint32_t *evals);
+
 #ifdef __cplusplus
 }
 #endif

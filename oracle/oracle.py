@@ -76,6 +76,8 @@ def lib():
             "orc_gram": (C.c_int, [pp, _u32p, C.c_size_t, C.c_size_t, _u32p, C.c_int]),
             "orc_gram_naive": (C.c_int, [pp, _u32p, C.c_size_t, C.c_size_t, _u32p]),
             "orc_garbage_h": (C.c_int, [pp, _u32p, _u32p, C.c_size_t, C.c_size_t, _u32p]),
+            "orc_jl_evals": (C.c_int, [pp, _i8p, C.c_size_t, _u32p, C.c_size_t, C.c_size_t,
+                                       _u32p]),
             "orc_amortize": (C.c_int, [pp, _u32p, _u32p, C.c_size_t, C.c_size_t, _u32p]),
             "orc_garbage_index": (C.c_size_t, [C.c_size_t, C.c_size_t, C.c_size_t]),
             "orc_decompose_coeff_balanced": (None, [C.c_uint64, C.c_uint64, C.c_size_t,
@@ -266,6 +268,18 @@ class Plan:
         if st:
             raise OracleError(st)
         return H
+
+    def jl_evals(self, flat, rows, parts, num_parts, n):
+        """evals[m] = sum_{i,j} conj(pi_{m,i,j}) s_{i,j} from the flat int8 JL
+        entries (mod.rs:885-923, step_prover.rs:185-206)."""
+        fl = np.ascontiguousarray(flat, dtype=np.int8)
+        pa, pp = _u32(parts)
+        out = np.empty(rows * self.n, dtype=np.uint32)
+        st = lib().orc_jl_evals(self._ref(), fl.ctypes.data_as(_i8p), rows, pp, num_parts, n,
+                                out.ctypes.data_as(_u32p))
+        if st:
+            raise OracleError(st)
+        return out
 
     def amortize(self, S, c, r, n):
         """z[k] = sum_i c_i s_i[k] (amortization.rs:75-81); c: r challenge polys."""

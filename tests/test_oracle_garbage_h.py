@@ -63,3 +63,27 @@ def test_amortize_matches_naive_products(oracle):
         assert np.array_equal(got[k], want), k
     # amortization.rs test_amortization_zero_witness
     assert not P.amortize(np.zeros_like(S), c, r, n).any()
+
+
+def test_jl_evals_are_projections_of_rotated_witnesses(oracle):
+    """Coefficient t of evals[m] = sum conj(pi_{m,i,j}) s_{i,j} (the oracle's
+    restatement of mod.rs:885-923 and step_prover.rs:185-206) equals the JL
+    projection p[m] of the witness with every polynomial multiplied by X^-t;
+    t = 0 is the projection itself (the constant-term identity LaBRADOR uses)."""
+    q = Q
+    P, F = oracle.Plan(q, D), oracle.Field(q)
+    rng = np.random.default_rng(13)
+    r, n = 2, 3
+    parts = _rand(rng, (r, n, D))
+    seed = bytes(range(32))
+    _, flat = oracle.jl_project(F, seed, 256, parts.reshape(r, n * D), r, n * D, D)
+    ev = P.jl_evals(flat, 256, parts.reshape(r, n * D), r, n).reshape(256, D)
+    for t in (0, 1, 17, 63):
+        # X^-t s: coefficient u is s[u + t] when u + t < d, else -s[u + t - d]
+        idx = np.arange(D) + t
+        rot = np.where(idx < D, parts[..., idx % D], 0).astype(np.uint32)
+        wrap = parts[..., idx % D]
+        neg = np.where(wrap == 0, 0, q - wrap.astype(np.uint64)).astype(np.uint32)
+        rot = np.where(idx < D, rot, neg)
+        p_t, _ = oracle.jl_project(F, seed, 256, rot.reshape(r, n * D), r, n * D, D, want_flat=False)
+        assert np.array_equal(ev[:, t], p_t), t
