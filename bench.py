@@ -325,12 +325,20 @@ def measure_round(dev, reps=50):
     wflat = wit.reshape(r, n * d)
     jlm.conjugated_evals(plan, wflat, r, d)
     times_ev = _events_ms(lambda: jlm.conjugated_evals(plan, wflat, r, d), max(5, reps // 5), stream)
+    # the round's commitment key expanded from a seed on the device (A, B, C, D:
+    # kappa = kappa1 = kappa2 = 16, t1 = t2 = 4; 364544 polys)
+    from lattica_b200.labrador import sample_uniform_polys
+    crs_polys = kappa * n + 16 * (r * 4 * kappa) + 2 * 16 * (4 * (r * (r + 1) // 2))
+    sample_uniform_polys(plan, seed, crs_polys, device=dev)
+    times_crs = _events_ms(lambda: sample_uniform_polys(plan, seed, crs_polys, device=dev),
+                           max(5, reps // 5), stream)
     return {"workload": "LaBRADOR round: r=64, n=2048, d=64, kappa=16, JL 256 rows, base 2^8 x4 limbs",
             "round_ms_p50": _pct(times, 50), "round_ms_p99": _pct(times, 99),
             "garbage_h_ms_p50": _pct(times_h, 50), "amortize_ms_p50": _pct(times_z, 50),
             "outer_u1_ms_p50": _pct(times_u1, 50), "outer_u2_ms_p50": _pct(times_u2, 50),
             "bdlop_batch64_ms_p50": _pct(times_bd, 50),
             "jl_evals_ms_p50": _pct(times_ev, 50),
+            "crs_expand_ms_p50": _pct(times_crs, 50),
             "round_with_jl_extraction_ms_p50": _pct(times_x, 50),
             "e2e_round_ms_p50": _pct(e2e, 50), "e2e_round_ms_p99": _pct(e2e, 99),
             "e2e_h2d_bytes": hw.numel() * 4, "e2e_d2h_bytes": d2h, "rounds": reps}

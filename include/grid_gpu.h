@@ -57,7 +57,8 @@ typedef enum grid_status {
   GRID_ERR_UNSUPPORTED_DEGREE = 12, /* valid plan, but no kernel compiled for this d */
   GRID_ERR_MISALIGNED = 13,
   GRID_ERR_NO_DEVICE = 14,
-  GRID_ERR_SCRATCH_LIMIT = 15      /* needs more than the no-alloc entry point's fixed buffer */
+  GRID_ERR_SCRATCH_LIMIT = 15,     /* needs more than the no-alloc entry point's fixed buffer */
+  GRID_ERR_SAMPLE_EXHAUSTED = 16   /* uniform sampling met more rejections than its margin */
 } grid_status;
 
 typedef struct grid_gpu_plan grid_gpu_plan;
@@ -189,6 +190,21 @@ int grid_gpu_gram_workspace(const grid_gpu_plan* plan, size_t r, size_t n, size_
 int grid_gpu_gram_dev(const grid_gpu_plan* plan, const uint32_t* S, size_t r, size_t n,
                       uint32_t* G, void* workspace, size_t workspace_bytes, void* stream);
 int grid_gpu_gram(grid_gpu_plan* plan, const uint32_t* S, size_t r, size_t n, uint32_t* G);
+
+/* ---- uniform ring elements: CommitKey::from_seed / sample_uniform_mat
+ *      (labrador/src/crs.rs:136-198, 308-326) with PrimeField::rand
+ *      (algebra/src/arith/prime.rs:730-743): npolys ring elements drawn in
+ *      order from ChaCha20Rng(seed) (rand_chacha 0.10.0), Montgomery words.
+ *      The commitment key's A, B, C, D are consecutive spans of one call.
+ *      accept_max = 0 uses the reference's rejection threshold; another value
+ *      replaces it (rejections then become frequent; for testing that path). */
+int grid_gpu_sample_uniform_polys_workspace(const grid_gpu_plan* plan, size_t npolys,
+                                            uint64_t accept_max, size_t* bytes);
+int grid_gpu_sample_uniform_polys_dev(const grid_gpu_plan* plan, const uint8_t* seed, size_t npolys,
+                                      uint64_t accept_max, uint32_t* out, void* workspace,
+                                      size_t workspace_bytes, void* stream);
+int grid_gpu_sample_uniform_polys(grid_gpu_plan* plan, const uint8_t* seed, size_t npolys,
+                                  uint64_t accept_max, uint32_t* out);
 
 /* ---- JL evaluations, aggregation side: jl_rows_flat_to_conjugated_polys +
  *      the jl_evals loop of prove_step (labrador/src/main_protocol/mod.rs:885-923,

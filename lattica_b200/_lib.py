@@ -18,6 +18,7 @@ STATUS_NAMES = {
     4: "UnsupportedTwist", 5: "InvalidParameters", 6: "DimensionMismatch",
     7: "InvalidModulus", 8: "NullPointer", 9: "OutOfMemory", 10: "Cuda", 11: "Timeout",
     12: "UnsupportedDegree", 13: "Misaligned", 14: "NoDevice", 15: "ScratchLimit",
+    16: "SampleExhausted",
 }
 
 _u32p = C.POINTER(C.c_uint32)
@@ -73,6 +74,11 @@ SIGNATURES = {
     "grid_gpu_gram_workspace": (C.c_int, [_vp, C.c_size_t, C.c_size_t, C.POINTER(C.c_size_t)]),
     "grid_gpu_gram_dev": (C.c_int, [_vp, _vp, C.c_size_t, C.c_size_t, _vp, _vp, C.c_size_t, _vp]),
     "grid_gpu_gram": (C.c_int, [_vp, _vp, C.c_size_t, C.c_size_t, _vp]),
+    "grid_gpu_sample_uniform_polys_workspace": (C.c_int, [_vp, C.c_size_t, C.c_uint64,
+                                                          C.POINTER(C.c_size_t)]),
+    "grid_gpu_sample_uniform_polys_dev": (C.c_int, [_vp, _vp, C.c_size_t, C.c_uint64, _vp, _vp,
+                                                    C.c_size_t, _vp]),
+    "grid_gpu_sample_uniform_polys": (C.c_int, [_vp, _vp, C.c_size_t, C.c_uint64, _vp]),
     "grid_gpu_jl_evals_workspace": (C.c_int, [C.POINTER(C.c_size_t)]),
     "grid_gpu_jl_evals_dev": (C.c_int, [_vp, _vp, C.c_size_t, _vp, C.c_size_t, C.c_size_t,
                                         C.c_size_t, _vp, _vp, C.c_size_t, _vp]),

@@ -617,6 +617,45 @@ int grid_gpu_jl_evals(grid_gpu_plan* p, const uint8_t* seed, size_t rows, const 
   return rc ? rc : fin;
 }
 
+/* ---- uniform ring elements (seeded commitment-key expansion) ----------- */
+
+int grid_gpu_sample_uniform_polys_workspace(const grid_gpu_plan* p, size_t npolys,
+                                            uint64_t accept_max, size_t* bytes) {
+  if (!p || !bytes) return GRID_ERR_NULL_POINTER;
+  *bytes = round_up(sample_uniform_workspace_bytes(p->f.q, (unsigned long long)npolys * p->d,
+                                                   accept_max),
+                    256);
+  return GRID_OK;
+}
+
+int grid_gpu_sample_uniform_polys_dev(const grid_gpu_plan* p, const uint8_t* seed, size_t npolys,
+                                      uint64_t accept_max, uint32_t* out, void* workspace,
+                                      size_t workspace_bytes, void* stream) {
+  if (!p || !seed || (!out && npolys)) return GRID_ERR_NULL_POINTER;
+  if (!aligned16(workspace)) return GRID_ERR_MISALIGNED;
+  return launch_sample_uniform(p, seed, (unsigned long long)npolys * p->d, accept_max, out,
+                               workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+int grid_gpu_sample_uniform_polys(grid_gpu_plan* p, const uint8_t* seed, size_t npolys,
+                                  uint64_t accept_max, uint32_t* out) {
+  if (!p || !seed || (!out && npolys)) return GRID_ERR_NULL_POINTER;
+  if (npolys == 0) return GRID_OK;
+  std::lock_guard<std::mutex> lk(p->mu);
+  const size_t out_bytes = npolys * p->d * 4;
+  const size_t ws = round_up(
+      sample_uniform_workspace_bytes(p->f.q, (unsigned long long)npolys * p->d, accept_max), 256);
+  int rc;
+  if ((rc = ensure_scratch(p, 7, out_bytes)) || (rc = ensure_scratch(p, 8, ws))) return rc;
+  cudaStream_t st = p->stream;
+  rc = launch_sample_uniform(p, seed, (unsigned long long)npolys * p->d, accept_max,
+                             static_cast<uint32_t*>(p->scratch[7].ptr), p->scratch[8].ptr, ws, st);
+  if (!rc)
+    rc = cuda_status(cudaMemcpyAsync(out, p->scratch[7].ptr, out_bytes, cudaMemcpyDeviceToHost, st));
+  const int fin = finish_host_call(p, st);
+  return rc ? rc : fin;
+}
+
 /* ---- decompositions ---------------------------------------------------- */
 
 int grid_gpu_decompose_balanced_dev(const grid_gpu_plan* p, const uint32_t* polys, size_t npolys,

@@ -12,6 +12,7 @@ constexpr uint32_t kMaxSpins = 1u << 22;
 enum DeviceError : int {
   GRID_DEV_OK = 0,
   GRID_DEV_TIMEOUT = 1,
+  GRID_DEV_SAMPLE_SHORT = 2,  // the uniform sampler ran out of candidates
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {

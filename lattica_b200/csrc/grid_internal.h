@@ -125,6 +125,13 @@ int launch_jl_project(const FieldParams& f, const uint8_t seed[32], size_t rows,
                       uint32_t* p_out, int8_t* flat_out, void* scratch, size_t scratch_bytes,
                       int num_sms, int* d_err, cudaStream_t s);
 size_t jl_scratch_bytes(size_t rows, size_t num_parts, int num_sms);
+// crs.cu: `count` uniform Montgomery words from ChaCha20Rng(seed) (accept_max 0:
+// the reference's rejection threshold).
+size_t sample_uniform_workspace_bytes(uint32_t q, unsigned long long count,
+                                      unsigned long long accept_max);
+int launch_sample_uniform(const grid_gpu_plan* p, const uint8_t seed[32], unsigned long long count,
+                          unsigned long long accept_max, uint32_t* out, void* ws, size_t ws_bytes,
+                          cudaStream_t s);
 // JL evaluations sum conj(pi_{m,i,j}) s_{i,j} (rows = 256, d = 64 only).
 size_t jl_evals_scratch_bytes();
 int launch_jl_evals(const FieldParams& f, const uint8_t seed[32], size_t rows,

@@ -27,51 +27,17 @@
 #include "grid_async.cuh"
 #include "grid_field.cuh"
 #include "grid_internal.h"
+#include "grid_chacha.cuh"
 #include "grid_tc.cuh"
 
 namespace grid {
 namespace {
 
+using chacha::ChachaKey;
+using chacha::chacha20_block;
+
 constexpr int kJlWarps = 8;
 constexpr int kJlThreads = kJlWarps * 32;
-
-struct ChachaKey {
-  uint32_t k[8];
-};
-
-__device__ __forceinline__ uint32_t rotl(uint32_t x, int r) { return __funnelshift_l(x, x, r); }
-
-#define GRID_QR(a, b, c, d)  \
-  a += b; d ^= a; d = rotl(d, 16); \
-  c += d; b ^= c; b = rotl(b, 12); \
-  a += b; d ^= a; d = rotl(d, 8);  \
-  c += d; b ^= c; b = rotl(b, 7);
-
-// RFC 8439 block function: out[16] = keystream words of block `counter`.
-__device__ __forceinline__ void chacha20_block(const ChachaKey& key, uint32_t counter,
-                                               uint32_t nonce0, uint32_t (&out)[16]) {
-  uint32_t x0 = 0x61707865u, x1 = 0x3320646eu, x2 = 0x79622d32u, x3 = 0x6b206574u;
-  uint32_t x4 = key.k[0], x5 = key.k[1], x6 = key.k[2], x7 = key.k[3];
-  uint32_t x8 = key.k[4], x9 = key.k[5], x10 = key.k[6], x11 = key.k[7];
-  uint32_t x12 = counter, x13 = nonce0, x14 = 0, x15 = 0;
-#pragma unroll
-  for (int i = 0; i < 10; ++i) {
-    GRID_QR(x0, x4, x8, x12);
-    GRID_QR(x1, x5, x9, x13);
-    GRID_QR(x2, x6, x10, x14);
-    GRID_QR(x3, x7, x11, x15);
-    GRID_QR(x0, x5, x10, x15);
-    GRID_QR(x1, x6, x11, x12);
-    GRID_QR(x2, x7, x8, x13);
-    GRID_QR(x3, x4, x9, x14);
-  }
-  out[0] = x0 + 0x61707865u; out[1] = x1 + 0x3320646eu;
-  out[2] = x2 + 0x79622d32u; out[3] = x3 + 0x6b206574u;
-  out[4] = x4 + key.k[0]; out[5] = x5 + key.k[1]; out[6] = x6 + key.k[2]; out[7] = x7 + key.k[3];
-  out[8] = x8 + key.k[4]; out[9] = x9 + key.k[5]; out[10] = x10 + key.k[6];
-  out[11] = x11 + key.k[7];
-  out[12] = x12 + counter; out[13] = x13 + nonce0; out[14] = x14; out[15] = x15;
-}
 
 // Keystream bytes [off, off + 64) of stream (key, nonce0) as 16 words
 // (unused tail bytes are whatever the next block holds; callers mask rows).

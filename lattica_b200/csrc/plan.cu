@@ -15,6 +15,7 @@
 #include <new>
 #include <vector>
 
+#include "grid_async.cuh"
 #include "grid_internal.h"
 
 namespace grid {
@@ -245,7 +246,7 @@ int finish_host_call(grid_gpu_plan* p, cudaStream_t s) {
   if (e != cudaSuccess) return cuda_status(e);
   if (derr) {
     cudaMemset(p->d_err, 0, sizeof(int));
-    return GRID_ERR_TIMEOUT;
+    return derr == GRID_DEV_SAMPLE_SHORT ? GRID_ERR_SAMPLE_EXHAUSTED : GRID_ERR_TIMEOUT;
   }
   return GRID_OK;
 }
@@ -498,7 +499,7 @@ int grid_gpu_plan_check(grid_gpu_plan* p, void* stream) {
   if (e != cudaSuccess) return cuda_status(e);
   if (derr) {
     cudaMemset(p->d_err, 0, sizeof(int));
-    return GRID_ERR_TIMEOUT;
+    return derr == GRID_DEV_SAMPLE_SHORT ? GRID_ERR_SAMPLE_EXHAUSTED : GRID_ERR_TIMEOUT;
   }
   return GRID_OK;
 }

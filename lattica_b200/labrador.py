@@ -170,6 +170,56 @@ class OuterCommitKey:
         return self.d.mul_vec(h)
 
 
+def sample_uniform_polys(plan: TwistedNttPlan, seed: bytes, npolys: int, device=None,
+                         accept_max: int = 0):
+    """npolys uniform ring elements (Montgomery words, shape (npolys, d)) drawn
+    in order from ChaCha20Rng(seed), as sample_uniform_mat does
+    (crs.rs:308-326, prime.rs:730-743). device: a CUDA device for a tensor on
+    the device, else a numpy array. accept_max 0 keeps the reference's
+    rejection threshold."""
+    if len(seed) != 32:
+        raise ValueError("seed must be 32 bytes")
+    lib = _lib.load()
+    sd = (C.c_uint8 * 32).from_buffer_copy(bytes(seed))
+    d = plan.d
+    if device is not None:
+        import torch
+        out = torch.empty((npolys, d), dtype=torch.int32, device=device)
+        nb = C.c_size_t()
+        raise_status(lib.grid_gpu_sample_uniform_polys_workspace(plan.handle, npolys, accept_max,
+                                                                 C.byref(nb)), "sample_ws")
+        ws = torch.empty(max(16, nb.value), dtype=torch.uint8, device=device)
+        st = lib.grid_gpu_sample_uniform_polys_dev(plan.handle, sd, npolys, accept_max,
+                                                   out.data_ptr(), ws.data_ptr(), ws.numel(),
+                                                   _stream_ptr(out))
+    else:
+        out = np.empty((npolys, d), dtype=np.uint32)
+        st = lib.grid_gpu_sample_uniform_polys(plan.handle, sd, npolys, accept_max,
+                                               out.ctypes.data)
+    raise_status(st, "grid_gpu_sample_uniform_polys")
+    return out
+
+
+def commit_key_from_seed(plan: TwistedNttPlan, seed: bytes, r: int, n: int, kappa: int,
+                         kappa1: int, kappa2: int, t1: int, t2: int, device):
+    """CommitKey::from_seed (crs.rs:136-198) expanded on the device: A
+    (kappa x n), B (kappa1 x r*t1*kappa), C (kappa1 x t2*g), D (kappa2 x t1*g)
+    with g = r(r+1)/2, consecutive draws of one ChaCha20Rng(seed). Returns
+    (CommitKey for A, OuterCommitKey for B, C, D)."""
+    for name, v in (("n", n), ("r", r), ("kappa", kappa), ("kappa1", kappa1),
+                    ("kappa2", kappa2), ("t1", t1), ("t2", t2)):
+        if v <= 0:
+            raise ValueError(f"CommitKey dimension {name}={v} must be positive")
+    g = r * (r + 1) // 2
+    cols_b, cols_c, cols_d = r * t1 * kappa, t2 * g, t1 * g
+    sizes = [kappa * n, kappa1 * cols_b, kappa1 * cols_c, kappa2 * cols_d]
+    polys = sample_uniform_polys(plan, seed, sum(sizes), device=device)
+    offs = np.cumsum([0] + sizes)
+    a, b, c, dm = (polys[offs[i]:offs[i + 1]] for i in range(4))
+    return (CommitKey(plan, a, kappa, n),
+            OuterCommitKey(plan, b, c, dm, kappa1, kappa2, cols_b, cols_c, cols_d))
+
+
 class JLMatrix:
     """Seeded JL projection (labrador/src/jl.rs:34-509): ChaCha20 keystream,
     key = seed, nonce = part index."""

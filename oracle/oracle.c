@@ -833,3 +833,42 @@ int orc_jl_evals(const orc_plan *p, const int8_t *flat, size_t rows, const uint3
     free(conj); free(prod);
     return ORC_OK;
 }
+
+/* CommitKey::from_seed / sample_uniform_mat (labrador/src/crs.rs:136-198,
+ * 308-326): npolys ring elements drawn in order from ChaCha20Rng(seed), each
+ * coefficient by PrimeField::rand (algebra/src/arith/prime.rs:730-743): u64
+ * rejection sampling (accept s <= u64::MAX - ((u64::MAX % q + 1) % q)), then
+ * from_u64(s % q). ChaCha20Rng is the rand_chacha 0.10.0 generator
+ * (Cargo.lock): ChaCha20 blocks with a 64-bit block counter from 0 and stream
+ * 0; rand_core 0.10.1's block RNG returns each u64 as two consecutive
+ * little-endian keystream words (low word first). accept_max = 0 selects the
+ * reference's threshold; another value replaces it (to exercise rejections). */
+int orc_sample_uniform_polys(const orc_field *f, const uint8_t seed[32], size_t npolys,
+                             uint32_t d, uint64_t accept_max, uint32_t *out) {
+    const uint64_t q = f->q;
+    const uint64_t reject = (UINT64_MAX % q + 1) % q;
+    const uint64_t upper = accept_max ? accept_max : UINT64_MAX - reject;
+    uint8_t block[64], nonce[12] = {0};
+    uint64_t blk = 0;
+    int idx = 16; /* words left in the current block: none */
+    uint32_t words[16];
+    for (size_t i = 0; i < npolys * d; i++) {
+        for (;;) {
+            if (idx >= 16) {
+                const uint32_t hi = (uint32_t)(blk >> 32);
+                for (int b = 0; b < 4; b++) nonce[b] = (uint8_t)(hi >> (8 * b));
+                orc_chacha20_block(seed, (uint32_t)blk, nonce, block);
+                for (int w = 0; w < 16; w++) words[w] = load_le32(block + 4 * w);
+                blk++;
+                idx = 0;
+            }
+            const uint64_t sample = (uint64_t)words[idx] | ((uint64_t)words[idx + 1] << 32);
+            idx += 2;
+            if (sample <= upper) {
+                out[i] = orc_to_mont(f, sample % q);
+                break;
+            }
+        }
+    }
+    return ORC_OK;
+}

@@ -140,6 +140,11 @@ int orc_jl_project(const orc_field *f, const uint8_t seed[32], size_t rows, size
 int orc_jl_evals(const orc_plan *p, const int8_t *flat, size_t rows, const uint32_t *parts,
                  size_t num_parts, size_t n, uint32_t *evals);
 
+/* Uniform ring elements from ChaCha20Rng(seed), CommitKey::from_seed order
+ * (labrador/src/crs.rs:136-198, 308-326; prime.rs:730-743). */
+int orc_sample_uniform_polys(const orc_field *f, const uint8_t seed[32], size_t npolys,
+                             uint32_t d, uint64_t accept_max, uint32_t *out);
+
 #ifdef __cplusplus
 }
 #endif

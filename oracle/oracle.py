@@ -78,6 +78,8 @@ def lib():
             "orc_garbage_h": (C.c_int, [pp, _u32p, _u32p, C.c_size_t, C.c_size_t, _u32p]),
             "orc_jl_evals": (C.c_int, [pp, _i8p, C.c_size_t, _u32p, C.c_size_t, C.c_size_t,
                                        _u32p]),
+            "orc_sample_uniform_polys": (C.c_int, [fp, _u8p, C.c_size_t, C.c_uint32, C.c_uint64,
+                                                   _u32p]),
             "orc_amortize": (C.c_int, [pp, _u32p, _u32p, C.c_size_t, C.c_size_t, _u32p]),
             "orc_garbage_index": (C.c_size_t, [C.c_size_t, C.c_size_t, C.c_size_t]),
             "orc_decompose_coeff_balanced": (None, [C.c_uint64, C.c_uint64, C.c_size_t,
@@ -290,6 +292,18 @@ class Plan:
         if st:
             raise OracleError(st)
         return Z
+
+
+def sample_uniform_polys(field: Field, seed: bytes, npolys: int, d: int, accept_max: int = 0):
+    """npolys uniform ring elements from ChaCha20Rng(seed) in CommitKey::from_seed
+    order (crs.rs:136-198, 308-326; prime.rs:730-743), Montgomery words."""
+    out = np.empty(npolys * d, dtype=np.uint32)
+    sd = (C.c_uint8 * 32).from_buffer_copy(seed)
+    st = lib().orc_sample_uniform_polys(C.byref(field.s), sd, npolys, d, accept_max,
+                                        out.ctypes.data_as(_u32p))
+    if st:
+        raise OracleError(st)
+    return out
 
 
 def decompose_coeff_balanced(c: int, base: int, num_limbs: int, q: int):
