@@ -227,7 +227,9 @@ __global__ void sum_splits_kernel(const uint32_t* __restrict__ part, uint32_t* _
 // Launch geometry of one product: tile shape, tiles and the K split.
 struct EmmGeometry {
   bool mv;  // emv_kernel (dense, M <= kMvMaxRows) instead of the tiled kernel
-  int tmg, tiles_m, tiles_n, tiles, splits, k_per_split;
+  int tmg, tiles_m, tiles_n;
+  int tiles;  // tiled kernel: output tiles; emv_kernel: 256-thread blocks over (N, d)
+  int splits, k_per_split;
 };
 
 // The K range is split so that all CTAs fit one wave of the resident slots
