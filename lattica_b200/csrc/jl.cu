@@ -384,8 +384,10 @@ __global__ void __launch_bounds__(kJlThreads) jl_flat_kernel(unsigned long long 
 // coefficient and its negation: sum_{v >= t} P_i[v] + sum_{v < t} N_i[v].
 // ---------------------------------------------------------------------------
 constexpr uint32_t kEvB = 256u * kTcCols;                  // B tile: 256 bytes x 256 columns
+// M' table in 32 bank-rotated copies (entry e of copy c at word 32 e + c; lane
+// l reads copy l), so the 32 random lookups of a warp never share a bank
 constexpr uint32_t kEvOffLut = kTcA + kEvB;
-constexpr uint32_t kEvOffPoly = kEvOffLut + 1024;          // the chunk's 4 polys (1 KB)
+constexpr uint32_t kEvOffPoly = kEvOffLut + 32 * 1024;     // the chunk's 4 polys (1 KB)
 constexpr uint32_t kEvOffSums = kEvOffPoly + 1024;         // P[64][4], N[64][4] (2 KB)
 constexpr uint32_t kEvOffS = kEvOffSums + 2048;            // S[64][4] (1 KB)
 constexpr uint32_t kEvOffBar = kEvOffS + 1024;
@@ -408,7 +410,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) jl_eval_tc_kernel(
   uint32_t* taddr_slot = reinterpret_cast<uint32_t*>(bar + 1);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
-  for (int i = tid; i < 256; i += kTcThreads) lut[i] = shifted_entries_of_byte(i);
+  for (int i = tid; i < 256 * 32; i += kTcThreads) lut[i] = shifted_entries_of_byte(i >> 5);
   for (int i = tid; i < 512; i += kTcThreads) sums[i] = 0;
   if (warp == 0) {
     tc::tmem_alloc(taddr_slot, 512);
@@ -452,11 +454,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) jl_eval_tc_kernel(
     if (it > 0) ok = __syncthreads_and(mbar_wait(bar, (it - 1) & 1, err));
     if (!ok) break;
     poly[tid] = x;
+    const uint32_t* lt = lut + lane;
 #pragma unroll
     for (int g = 0; g < 16; ++g)
       *reinterpret_cast<uint4*>(sm + jl_a_off(16 * g, tid)) =
-          make_uint4(lut[w[g] & 0xFFu], lut[(w[g] >> 8) & 0xFFu], lut[(w[g] >> 16) & 0xFFu],
-                     lut[w[g] >> 24]);
+          make_uint4(lt[(w[g] & 0xFFu) << 5], lt[((w[g] >> 8) & 0xFFu) << 5],
+                     lt[((w[g] >> 16) & 0xFFu) << 5], lt[(w[g] >> 24) << 5]);
     __syncthreads();  // the chunk's polys are staged
     // B column tid: s'[u + t] for t = 0 .. 63, 16 bytes per group of 4 t
     const uint32_t* pw = poly + (tid & ~(kEvD - 1));
