@@ -118,6 +118,24 @@ class ClockSampler:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
+def max_over_ranks(x: float, world: int, device) -> float:
+    """The largest x over the job's ranks (for times: the slowest rank sets the
+    job's time); x itself on one rank."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(units_per_rank: int, world: int, seconds_max: float) -> float:
+    """Whole-job units per second when every rank processes units_per_rank in
+    at most seconds_max (the max over ranks)."""
+    return world * units_per_rank / seconds_max
+
+
 def run_reference(args, rank, world):
     """CPU restatement of the reference path on this host's cores."""
     if rank != 0:
@@ -502,12 +520,9 @@ def run_ours(args, rank, world, local_rank):
     plan.check_device()
     elapsed_ms = t_begin.elapsed_time(t_end)
     kernel_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends)) / args.steps
-    if world > 1:
-        t = torch.tensor([elapsed_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed_ms = float(t.item())
+    elapsed_ms = max_over_ranks(elapsed_ms, world, dev)
     ms_per_step = elapsed_ms / args.steps
-    value = world * n / (ms_per_step / 1e3)
+    value = replica_throughput(n, world, ms_per_step / 1e3)
 
     # End-to-end through the host-buffer C-ABI call: pinned host inputs copied
     # in, computed, result copied out, every step.
@@ -529,10 +544,7 @@ def run_ours(args, rank, world, local_rank):
     for _ in range(e2e_steps):
         e2e_step()
     e2e_s = (time.perf_counter() - t0) / e2e_steps
-    if world > 1:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(e2e_s, world, dev)
     assert torch.equal(hout, out.cpu()), "host-buffer path disagrees with the device path"
 
     if rank != 0:
@@ -557,7 +569,7 @@ def run_ours(args, rank, world, local_rank):
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
                      "algorithmic_bytes_per_launch": bytes_per_launch,
                      "kernel_ms": kernel_ms},
-        "e2e": {"value": world * n / e2e_s, "unit": "polys/s",
+        "e2e": {"value": replica_throughput(n, world, e2e_s), "unit": "polys/s",
                 "h2d_bytes_per_step": 2 * 4 * d * n, "d2h_bytes_per_step": 4 * d * n},
         "gpu_launches": args.steps,
         "clocks": sampler.summary(),

@@ -1,0 +1,44 @@
+"""The multi-GPU bench path's cross-rank logic on CPU (gloo, 2 ranks): every
+rank sees the slowest rank's time, and the job's throughput is all ranks'
+units over that time; the reference arm runs on rank 0 only."""
+import json
+import os
+import socket
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def test_two_ranks_time_by_the_slowest_and_sum_units():
+    port = str(_free_port())
+    procs = [subprocess.Popen([sys.executable, os.path.join(HERE, "_bench_rank.py"), str(r), "2",
+                               port], stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)
+             for r in range(2)]
+    outs = []
+    for p in procs:
+        out, err = p.communicate(timeout=120)
+        assert p.returncode == 0, err
+        outs.append(json.loads(out.strip().splitlines()[-1]))
+    for o in outs:
+        assert o["slowest"] == 5.0            # rank 1 took 5 s, rank 0 took 3 s
+        assert o["value"] == 2 * 1000 / 5.0   # 2 ranks x 1000 units in 5 s
+
+
+def test_reference_arm_runs_on_rank_zero_only(capsys):
+    sys.path.insert(0, ROOT)
+    import bench
+
+    class Args:
+        workload, steps, warmup = "ntt64", 1, 3
+    assert bench.run_reference(Args(), 1, 2) is None
+    assert capsys.readouterr().out == ""
