@@ -263,7 +263,21 @@ def measure_commit_plain(dev, reps=50):
         if i >= 3:
             e2e.append((time.perf_counter() - t0) * 1e3)
     med_b, med_p, med_e = statistics.median(tb), statistics.median(tp), statistics.median(e2e)
+    # CPU beside it: the oracle's prepared commit path (NTT-domain A cached, like
+    # linear.rs:717-742) on the same inputs, one thread and all host cores
+    from oracle import oracle as O
+    P = O.Plan(q, d)
+    cpu = {}
+    for label, threads in (("1t", 1), ("all", os.cpu_count() or 1)):
+        want = P.matvec(A, rows, cols, s_host, batch, threads=threads)  # warm
+        t0 = time.perf_counter()
+        for _ in range(3):
+            P.matvec(A, rows, cols, s_host, batch, threads=threads)
+        cpu[label] = batch * 3 / (time.perf_counter() - t0)
+    assert np.array_equal(t.cpu().numpy().view(np.uint32).reshape(-1), want), "GPU != oracle"
     return {"workload": "plain Ajtai commit: A 8x64, d=64, 64 ternary witnesses per batch",
+            "cpu_oracle_commits_per_s": {"threads_1": cpu["1t"], "threads_all": cpu["all"],
+                                         "cores": os.cpu_count() or 1},
             "commits_per_s": batch / (med_b / 1e3), "batch_ms_p50": med_b,
             "per_call_commits_per_s": batch / (med_p / 1e3),
             "e2e_commits_per_s": batch / (med_e / 1e3), "e2e_batch_ms_p50": med_e,
@@ -308,6 +322,24 @@ def measure_round(dev, reps=50):
         if i >= 2:
             e2e.append((time.perf_counter() - t0) * 1e3)
     d2h = sum(x.numel() * x.element_size() for x in outs_host)
+    # CPU beside it: the oracle's round pieces (inner commitments, Gram, JL
+    # projection) at n = 128 polys per witness part, scaled by n / 128 (each
+    # piece is linear in n), on one thread and on all host cores
+    from oracle import oracle as O
+    P = O.Plan(q, d)
+    ns = 128
+    A_h = A[:, :ns].contiguous().cpu().numpy().view(np.uint32)
+    S_h = wit[:, :ns].contiguous().cpu().numpy().view(np.uint32)
+    cpu_round = {}
+    for label, threads in (("threads_1", 1), ("threads_all", os.cpu_count() or 1)):
+        t0 = time.perf_counter()
+        P.matvec(A_h, kappa, ns, S_h, r, threads=threads)
+        P.gram(S_h, r, ns, threads=threads)
+        O.jl_project(P.field, seed, 256, S_h.reshape(r, ns * d), r, ns * d, d, want_flat=False,
+                     threads=threads)
+        cpu_round[label] = (time.perf_counter() - t0) * 1e3 * (n / ns)
+    cpu_round["cores"] = os.cpu_count() or 1
+    cpu_round["sample"] = f"n = {ns} of {n} polys per part, scaled x{n // ns}"
     # the round's neighbours at the same size: garbage h (aggregated phis of
     # the witness shape) and the amortized witness z = sum_i c_i s_i
     from lattica_b200.labrador import amortize_witness, compute_garbage_h
@@ -352,6 +384,7 @@ def measure_round(dev, reps=50):
                            max(5, reps // 5), stream)
     return {"workload": "LaBRADOR round: r=64, n=2048, d=64, kappa=16, JL 256 rows, base 2^8 x4 limbs",
             "round_ms_p50": _pct(times, 50), "round_ms_p99": _pct(times, 99),
+            "cpu_oracle_round_ms": cpu_round,
             "garbage_h_ms_p50": _pct(times_h, 50), "amortize_ms_p50": _pct(times_z, 50),
             "outer_u1_ms_p50": _pct(times_u1, 50), "outer_u2_ms_p50": _pct(times_u2, 50),
             "bdlop_batch64_ms_p50": _pct(times_bd, 50),
