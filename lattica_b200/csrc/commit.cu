@@ -285,8 +285,10 @@ int launch_emm_tile(dim3 grid, const uint32_t* X, const uint32_t* Y, uint32_t* d
 size_t emm_workspace_words(const grid_gpu_plan* p, int M, int N, int K, int mode) {
   if (M <= 0 || N <= 0 || K <= 0 || p->d % EG) return 0;
   const EmmGeometry g = emm_geometry(M, N, K, (int)p->d, mode, p->num_sms);
+  EmmTcGeometry tg;
+  const int splits = !g.mv && emm_tc_geometry(p, M, N, K, mode, &tg) ? tg.splits : g.splits;
   const size_t outputs = mode == OUT_UPPER ? (size_t)M * (M + 1) / 2 : (size_t)M * N;
-  return g.splits > 1 ? (size_t)g.splits * outputs * p->d : 0;
+  return splits > 1 ? (size_t)splits * outputs * p->d : 0;
 }
 
 // out_evals: dense [M][N][d] or packed-upper [M(M+1)/2][d]. work: >= emm_workspace_words.
@@ -296,13 +298,17 @@ int launch_emm(const grid_gpu_plan* p, const uint32_t* X, const uint32_t* Y, int
   if (p->d % EG) return GRID_ERR_UNSUPPORTED_DEGREE;
   if (mode == OUT_UPPER && M != N) return GRID_ERR_DIMENSION_MISMATCH;
   const EmmGeometry g = emm_geometry(M, N, K, (int)p->d, mode, p->num_sms);
-  const int splits = g.splits;
+  EmmTcGeometry tg;
+  const bool tc = !g.mv && emm_tc_geometry(p, M, N, K, mode, &tg);
+  const int splits = tc ? tg.splits : g.splits;
   const size_t outputs = mode == OUT_UPPER ? (size_t)M * (M + 1) / 2 : (size_t)M * N;
   const size_t stride = outputs * p->d;
   uint32_t* dst = splits > 1 ? work : out_evals;
   if (splits > 1 && !work) return GRID_ERR_NULL_POINTER;
   int rc = GRID_OK;
-  if (g.mv) {
+  if (tc) {
+    rc = launch_emm_tc(p, X, Y, M, N, K, ldy, mode, dst, tg, stride, s);
+  } else if (g.mv) {
     emv_kernel<<<dim3((unsigned)g.tiles, splits), kMvThreads, 0, s>>>(
         X, Y, dst, M, N, K, ldy, (int)p->d, g.k_per_split, stride, p->f);
   } else {

@@ -63,6 +63,7 @@ struct grid_gpu_plan {
   // inverse matrices (2 x 64 KB). d = 256: the 64-point matrix (64 KB) and the
   // twist constants of the products. Null selects the CUDA-core kernels.
   void* d_tcw = nullptr;
+  bool tc_emm = false;  // evaluation-domain products on the tensor cores where the shape allows
   int* d_err = nullptr;
   cudaStream_t stream = nullptr;   // host-buffer entry points: first pipeline stream
   cudaStream_t stream2 = nullptr;  // second pipeline stream
@@ -104,6 +105,16 @@ int launch_emm(const grid_gpu_plan* p, const uint32_t* X, const uint32_t* Y, int
                int ldy, int mode, uint32_t* out_evals, uint32_t* work, cudaStream_t s);
 int launch_pointwise(const grid_gpu_plan* p, uint32_t* dst, const uint32_t* rhs, size_t words,
                      cudaStream_t s);
+// emm_tc.cu: the same products on the tensor cores (X rows <= 128, Y rows <= 64).
+struct EmmTcGeometry {
+  int np;           // Y rows padded to 16, 32, 48 or 64
+  int groups;       // CTAs along the evaluation points
+  int splits, k_per_split;
+};
+bool emm_tc_geometry(const grid_gpu_plan* p, int M, int N, int K, int mode, EmmTcGeometry* g);
+int launch_emm_tc(const grid_gpu_plan* p, const uint32_t* X, const uint32_t* Y, int M, int N,
+                  int K, int ldy, int mode, uint32_t* dst, const EmmTcGeometry& g, size_t stride,
+                  cudaStream_t s);
 // garbage.cu: (C_ij + C_ji) * 2^-1 on the upper triangle; z_hat = sum_i c_hat_i (.) s_hat_i.
 int launch_symmetrize_half(const grid_gpu_plan* p, const uint32_t* C, int r, uint32_t* H,
                            cudaStream_t s);

@@ -420,6 +420,7 @@ int grid_gpu_plan_create(uint64_t q, uint64_t d, grid_gpu_plan** out) {
     if ((e = cudaMalloc(&p->d_tw, dev_tw.size() * sizeof(uint2))) != cudaSuccess) break;
     if ((e = cudaMemcpy(p->d_tw, dev_tw.data(), dev_tw.size() * sizeof(uint2),
                         cudaMemcpyHostToDevice)) != cudaSuccess) break;
+    p->tc_emm = use_tensor_cores();
     if ((d == 64 || d == 256) && use_tensor_cores()) {
       std::vector<unsigned char> tcw;
       if (d == 64)
