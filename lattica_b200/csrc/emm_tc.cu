@@ -58,7 +58,7 @@ template <int EPC> struct EtWords;
 template <> struct EtWords<2> { using type = uint2; };
 template <> struct EtWords<4> { using type = uint4; };
 
-template <int NP>
+template <int NP, int MX>
 __global__ void __launch_bounds__(kEtThreads, 1)
     emm_tc_kernel(const uint32_t* __restrict__ X, const uint32_t* __restrict__ Y,
                   uint32_t* __restrict__ out, int M, int N, int K, int ldy, int d, int mode,
@@ -114,10 +114,12 @@ __global__ void __launch_bounds__(kEtThreads, 1)
           w[l];
   };
 
-  // Up to 16 (row, k) units per thread for X (128 rows) and 8 for Y (64 rows).
-  constexpr int kMaxUnitsX = 128 * KCH / kEtThreads, kMaxUnitsY = 64 * KCH / kEtThreads;
+  // (row, k) units per thread: X has at most MX rows, Y at most NP
+  constexpr int kUnitsX = MX * KCH / kEtThreads, kUnitsY = NP * KCH / kEtThreads;
   using Words = typename EtWords<EPC>::type;
-  uint32_t rx[kMaxUnitsX][EPC], ry[kMaxUnitsY][EPC];
+  struct Regs {
+    uint32_t x[kUnitsX][EPC], y[kUnitsY][EPC];
+  };
   auto gather_rows = [&](const uint32_t* src, int rows, int ld, int k0, auto& dst) {
     constexpr int kUnits = sizeof(dst) / sizeof(dst[0]);
 #pragma unroll
@@ -139,39 +141,40 @@ __global__ void __launch_bounds__(kEtThreads, 1)
       for (int el = 0; el < EPC; ++el) dst[it][el] = wv[el];
     }
   };
-
-  bool ok = true;
-  for (int c = 0; c < nch; ++c) {
+  // issue every load of chunk c (one vector load of the CTA's EPC adjacent
+  // evaluation points per (row, k)); nothing waits on them until put_chunk
+  auto gather_chunk = [&](int c, Regs& r) {
+    const int k0 = kbeg + c * KCH;
+    gather_rows(X, M, K, k0, r.x);
+    if (!upper) gather_rows(Y, N, ldy, k0, r.y);
+  };
+  // write chunk c's tiles into its stage, then thread 0 issues its MMAs
+  auto put_chunk = [&](int c, const Regs& r) -> bool {
     const int st = c & 1;
     unsigned char* stage = sm + st * S::STAGE;
     // the MMAs of chunk c - 2 must be done reading this stage
-    if (c >= 2) ok = __syncthreads_and(mbar_wait(&bars[st], ((c - 2) >> 1) & 1, err));
-    if (!ok) break;
-    const int k0 = kbeg + c * KCH;
-    // all of this chunk's gathers first (one vector load of the CTA's EPC
-    // adjacent evaluation points per (row, k)), then the tile writes
-    gather_rows(X, M, K, k0, rx);
-    if (!upper) gather_rows(Y, N, ldy, k0, ry);
+    if (c >= 2 && !__syncthreads_and(mbar_wait(&bars[st], ((c - 2) >> 1) & 1, err))) return false;
 #pragma unroll
-    for (int it = 0; it < kMaxUnitsX; ++it) {
+    for (int it = 0; it < kUnitsX; ++it) {
       const int u = tid + it * kEtThreads;
       if (u >= M * KCH) break;
       const int m = u >> 5, kk = u & (KCH - 1);
 #pragma unroll
       for (int el = 0; el < EPC; ++el) {
         *reinterpret_cast<uint32_t*>(stage + el * ABOX + sw128(m, 0, kk >> 2, ABOX) + 4 * (kk & 3)) =
-            rx[it][el];
-        if (upper) put_b(stage + EPC * ABOX + el * S::BBOX, m, kk, rx[it][el]);
+            r.x[it][el];
+        if (upper) put_b(stage + EPC * ABOX + el * S::BBOX, m, kk, r.x[it][el]);
       }
     }
     if (!upper) {
 #pragma unroll
-      for (int it = 0; it < kMaxUnitsY; ++it) {
+      for (int it = 0; it < kUnitsY; ++it) {
         const int u = tid + it * kEtThreads;
         if (u >= N * KCH) break;
         const int n = u >> 5, kk = u & (KCH - 1);
 #pragma unroll
-        for (int el = 0; el < EPC; ++el) put_b(stage + EPC * ABOX + el * S::BBOX, n, kk, ry[it][el]);
+        for (int el = 0; el < EPC; ++el)
+          put_b(stage + EPC * ABOX + el * S::BBOX, n, kk, r.y[it][el]);
       }
     }
     tc::fence_async_smem();
@@ -188,6 +191,19 @@ __global__ void __launch_bounds__(kEtThreads, 1)
                      desc_sw128(sa + EPC * ABOX + el * S::BBOX + 32 * s), idesc, (c | s) != 0);
       tc::mma_commit(&bars[st]);
     }
+    return true;
+  };
+
+  // two register buffers in turn: chunk c + 1's loads are in flight while
+  // chunk c is transposed into shared memory
+  bool ok = true;
+  Regs ra, rb;
+  if (nch > 0) gather_chunk(0, ra);
+  for (int c = 0; c < nch; c += 2) {
+    if (c + 1 < nch) gather_chunk(c + 1, rb);
+    if (!(ok = put_chunk(c, ra)) || c + 1 >= nch) break;
+    if (c + 2 < nch) gather_chunk(c + 2, ra);
+    if (!(ok = put_chunk(c + 1, rb))) break;
   }
   // the last commit covers every MMA issued before it
   if (ok && nch > 0) ok = mbar_wait(&bars[(nch - 1) & 1], ((nch - 1) >> 1) & 1, err);
@@ -229,14 +245,15 @@ __global__ void __launch_bounds__(kEtThreads, 1)
   }
 }
 
-template <int NP>
+template <int NP, int MX>
 int launch_np(const grid_gpu_plan* p, const uint32_t* X, const uint32_t* Y, int M, int N, int K,
               int ldy, int mode, uint32_t* dst, const EmmTcGeometry& g, size_t stride,
               cudaStream_t s) {
   using S = EtShape<NP>;
   static int bps_cache[kMaxDevices] = {};
   int bps = 0;
-  const int rc = prepare_kernel(emm_tc_kernel<NP>, S::SMEM, kEtThreads, p->device, bps_cache, &bps);
+  const int rc =
+      prepare_kernel(emm_tc_kernel<NP, MX>, S::SMEM, kEtThreads, p->device, bps_cache, &bps);
   if (rc) return rc;
   // 2^(8i) R mod q: mont_mul(y, .) = 2^(8i) y mod q
   uint32_t c[3];
@@ -249,7 +266,7 @@ int launch_np(const grid_gpu_plan* p, const uint32_t* X, const uint32_t* Y, int 
   const uintptr_t bytes = 4u * S::EPC;
   const bool vec = reinterpret_cast<uintptr_t>(X) % bytes == 0 &&
                    (mode == ET_UPPER || reinterpret_cast<uintptr_t>(Y) % bytes == 0);
-  emm_tc_kernel<NP><<<dim3(g.groups, g.splits), kEtThreads, S::SMEM, s>>>(
+  emm_tc_kernel<NP, MX><<<dim3(g.groups, g.splits), kEtThreads, S::SMEM, s>>>(
       X, Y, dst, M, N, K, ldy, (int)p->d, mode, g.k_per_split, stride,
       make_uint4(c[0], c[1], c[2], 0), k, vec, p->d_err);
   return cuda_status(cudaGetLastError());
@@ -280,11 +297,20 @@ bool emm_tc_geometry(const grid_gpu_plan* p, int M, int N, int K, int mode, EmmT
 int launch_emm_tc(const grid_gpu_plan* p, const uint32_t* X, const uint32_t* Y, int M, int N,
                   int K, int ldy, int mode, uint32_t* dst, const EmmTcGeometry& g, size_t stride,
                   cudaStream_t s) {
+  // X rows: register buffers sized for 64 or 128
+  if (M <= 64) {
+    switch (g.np) {
+      case 16: return launch_np<16, 64>(p, X, Y, M, N, K, ldy, mode, dst, g, stride, s);
+      case 32: return launch_np<32, 64>(p, X, Y, M, N, K, ldy, mode, dst, g, stride, s);
+      case 48: return launch_np<48, 64>(p, X, Y, M, N, K, ldy, mode, dst, g, stride, s);
+      default: return launch_np<64, 64>(p, X, Y, M, N, K, ldy, mode, dst, g, stride, s);
+    }
+  }
   switch (g.np) {
-    case 16: return launch_np<16>(p, X, Y, M, N, K, ldy, mode, dst, g, stride, s);
-    case 32: return launch_np<32>(p, X, Y, M, N, K, ldy, mode, dst, g, stride, s);
-    case 48: return launch_np<48>(p, X, Y, M, N, K, ldy, mode, dst, g, stride, s);
-    default: return launch_np<64>(p, X, Y, M, N, K, ldy, mode, dst, g, stride, s);
+    case 16: return launch_np<16, 128>(p, X, Y, M, N, K, ldy, mode, dst, g, stride, s);
+    case 32: return launch_np<32, 128>(p, X, Y, M, N, K, ldy, mode, dst, g, stride, s);
+    case 48: return launch_np<48, 128>(p, X, Y, M, N, K, ldy, mode, dst, g, stride, s);
+    default: return launch_np<64, 128>(p, X, Y, M, N, K, ldy, mode, dst, g, stride, s);
   }
 }
 
