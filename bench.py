@@ -19,6 +19,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import platform
 import statistics
 import subprocess
 import sys
@@ -165,11 +166,26 @@ def run_reference(args, rank, world):
         "config": {"workload": f"{args.workload}: q={q}, d={d}, {n_full} polys (sampled)",
                    "sample_polys": sample},
         "cpu_baseline": {"value": value, "unit": "polys/s", "cores": threads, "kind": "port",
-                         "sample": f"{sample} polys of the {n_full}-poly workload per step"},
+                         "sample": f"{sample} polys of the {n_full}-poly workload per step",
+                         "host": host_cpu()},
         "e2e": {"value": value, "unit": "polys/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def host_cpu():
+    """This host's CPU model and logical core count, recorded beside CPU timings."""
+    model = platform.processor() or "unknown"
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"model": model, "nproc": os.cpu_count() or 1}
 
 
 def cpu_baseline(q, d, n_full):
@@ -188,7 +204,8 @@ def cpu_baseline(q, d, n_full):
         elapsed += time.perf_counter() - t0
         reps += 1
     return {"value": sample * reps / elapsed, "unit": "polys/s", "cores": 1, "kind": "port",
-            "sample": f"{reps} x {sample} polys of the {n_full}-poly workload, 1 thread"}
+            "sample": f"{reps} x {sample} polys of the {n_full}-poly workload, 1 thread",
+            "host": host_cpu()}
 
 
 def _mont_words(q, values):
