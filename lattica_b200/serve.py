@@ -115,9 +115,39 @@ class RingServer:
         self._thread = threading.Thread(target=self._loop, name="ring-server", daemon=True)
 
     # ---------------------------------------------------------------- public
-    def start(self):
+    def start(self, prime: bool = True):
+        if prime:
+            self.prime()
         self._thread.start()
         return self
+
+    def prime(self, gram_r: int = 64, gram_n: int = 1024, round_r: int = 64):
+        """Runs one request of each kind, at its largest shape, on every stream
+        that can carry it, and waits. Each stream's memory pool then holds the
+        blocks its requests need, and every kernel is loaded. Without this, the
+        first round or Gram on a stream grows the pool in the middle of the
+        traffic, and a device-synchronising allocation stalls the work already
+        in flight on the other streams."""
+        torch = self._torch
+        polys = self.pool.shape[0]
+        m = max(self.commit_mats)
+        shapes = {"commit": (m, min(self.commit_mats[m].cols, polys)),
+                  "gramjl": (gram_r, gram_n),
+                  "round": (round_r, self.round_key.n)}
+        for slot, cls in enumerate(self._slot_class):
+            kinds = {"commit": ("commit",), "heavy": ("gramjl", "round")}.get(cls, KINDS)
+            jobs = []
+            for kind in kinds:
+                a, b = shapes[kind]
+                if kind != "commit":
+                    a = min(a, polys // b)  # r witness vectors of n polys from the pool
+                if a < 1 or b > polys:
+                    continue
+                req = Request(kind, 0, (a, b), keep=False)
+                jobs.append(self._run(kind, [req], self._streams[slot], 0))
+            for job in jobs:
+                job.event.synchronize()
+        torch.cuda.synchronize(self.device)
 
     def stop(self):
         with self._cv:
