@@ -37,6 +37,12 @@ def _host(t):
     (17, 8, 2, 9, 3),
     (Q256, 256, 4, 40, 6),
     (Q, 32, 33, 17, 2),
+    # tensor-core contraction: Y rows padded to 16 / 32 / 48 / 64, X rows <= 64 or <= 128
+    (Q, 64, 17, 40, 64),        # NP 32, X 64 rows
+    (Q, 64, 24, 50, 70),        # NP 32, X 128-row buffers
+    (Q, 64, 40, 70, 100),       # NP 48
+    (Q, 64, 49, 20, 65),        # NP 64, just past 64 X rows
+    (Q, 64, 64, 33, 128),       # NP 64, 128 X rows
 ])
 def test_commit_matches_oracle(cuda, oracle, q, d, rows, cols, batch):
     from lattica_b200 import TwistedNttPlan
@@ -104,7 +110,8 @@ def test_linear_commit_rejects_bad_shapes(cuda):
 
 @pytest.mark.parametrize("q,d,r,n", [(Q, 64, 1, 4), (Q, 64, 3, 70), (Q, 64, 5, 130),
                                      (12289, 64, 33, 9), (Q256, 256, 6, 12), (17, 8, 4, 3),
-                                     (Q, 64, 40, 1100)])
+                                     (Q, 64, 40, 1100), (Q, 64, 20, 30), (Q, 64, 64, 40),
+                                     (Q, 64, 16, 77), (Q, 64, 17, 9)])
 def test_gram_matches_oracle(cuda, oracle, q, d, r, n):
     from lattica_b200 import TwistedNttPlan
     from lattica_b200.labrador import compute_garbage_g

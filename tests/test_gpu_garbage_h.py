@@ -26,7 +26,8 @@ def _host(t):
 
 
 @pytest.mark.parametrize("q,d,r,n", [(Q, 64, 1, 5), (Q, 64, 3, 17), (Q, 64, 17, 130),
-                                     (Q, 64, 40, 33), (12289, 64, 5, 9), (Q256, 256, 6, 20)])
+                                     (Q, 64, 40, 33), (12289, 64, 5, 9), (Q256, 256, 6, 20),
+                                     (Q, 64, 64, 50), (Q, 64, 33, 40)])
 def test_garbage_h_matches_oracle(cuda, oracle, q, d, r, n):
     from lattica_b200 import TwistedNttPlan
     from lattica_b200.labrador import compute_garbage_h
