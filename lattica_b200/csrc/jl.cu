@@ -177,11 +177,20 @@ __device__ __forceinline__ uint32_t shifted_entries_of_byte(uint32_t byte) {
   return out;
 }
 
-template <bool kWholeBlocks>
+// kFlat (whole blocks, d % 8 == 0, n % 32 == 0): the kernel also writes the
+// int8 entries flat[row][part][k][j] (col = j d + k) from the words it builds
+// for the A tile, so the keystream is generated once. A chunk is then 32
+// consecutive polynomials x 8 coefficient indices: warp w takes coefficient
+// 8 kg + w and lane l polynomial 32 jg + l. For each keystream byte, the four
+// lanes of a quad swap bytes (a 4 x 4 transpose: two shuffles, two byte
+// permutes) so that lane 4 g + r holds row 4 b + r of polynomials 4 g .. 4 g + 3,
+// and the warp's stores fill whole 32-byte sectors of four rows.
+template <bool kWholeBlocks, bool kFlat = false>
 __global__ void __launch_bounds__(kTcThreads) jl_tc_kernel(
     const uint32_t* __restrict__ parts, unsigned long long cols, int rows, int packed_len,
-    ChachaKey key, unsigned long long nchunks, unsigned long long* __restrict__ gsum_pos,
-    uint32_t q, int* __restrict__ err) {
+    ChachaKey key, unsigned long long nchunks, unsigned long long per_part, int d,
+    unsigned long long plane, int8_t* __restrict__ flat,
+    unsigned long long* __restrict__ gsum_pos, uint32_t q, int* __restrict__ err) {
   extern __shared__ __align__(1024) unsigned char sm_raw[];
   const uint32_t raw = smem_addr(sm_raw);
   unsigned char* sm = sm_raw + (((raw + 1023u) & ~1023u) - raw);
@@ -209,13 +218,26 @@ __global__ void __launch_bounds__(kTcThreads) jl_tc_kernel(
   // kind::i8, u8 x u8 -> s32, A and B MN-major, M = 128, N = 16
   const uint32_t idesc = tc::idesc_u8(128, 16) | (1u << 15) | (1u << 16);
 
-  const unsigned long long per_part = (cols + kTcCols - 1) / kTcCols;
+  const unsigned long long npoly = cols / (unsigned long long)d;
+  // byte selectors of the quad transpose (step 1: lanes l, l ^ 1; step 2: l, l ^ 2)
+  const uint32_t sel1 = (lane & 1) ? 0x3715u : 0x6240u;
+  const uint32_t sel2 = (lane & 2) ? 0x3276u : 0x5410u;
   uint32_t bsum[4] = {0, 0, 0, 0};
   bool ok = true;
   uint32_t it = 0;
   for (unsigned long long ch = blockIdx.x; ch < nchunks; ch += gridDim.x, ++it) {
     const uint32_t part = (uint32_t)(ch / per_part);
-    const unsigned long long c = (ch % per_part) * kTcCols + tid;
+    const unsigned long long ci = ch % per_part;
+    unsigned long long c, jj = 0;
+    uint32_t kk = 0;
+    if constexpr (kFlat) {
+      const unsigned long long kgroups = (unsigned long long)d / 8;
+      jj = (ci / kgroups) * 32 + lane;
+      kk = (uint32_t)(ci % kgroups) * 8 + warp;
+      c = jj * d + kk;
+    } else {
+      c = ci * kTcCols + tid;
+    }
     uint32_t w[16];
     uint32_t x = 0;
     if (c < cols) {
@@ -231,11 +253,29 @@ __global__ void __launch_bounds__(kTcThreads) jl_tc_kernel(
     // the previous chunk's MMAs must be done reading the tiles
     if (it > 0) ok = __syncthreads_and(mbar_wait(bar, (it - 1) & 1, err));
     if (!ok) break;
+    // kFlat: this lane's row 4 b + (lane & 3) of polynomials jj - (lane & 3) .. + 3,
+    // keystream byte b = 0, 1, ...: one pointer advanced by 4 rows per byte
+    int8_t* rowp = nullptr;
+    if constexpr (kFlat)
+      rowp = flat + (unsigned long long)(lane & 3) * plane +
+             ((unsigned long long)part * d + kk) * npoly + (jj - (lane & 3));
+    const unsigned long long step4 = 4 * plane;
 #pragma unroll
-    for (int g = 0; g < 16; ++g)
-      *reinterpret_cast<uint4*>(sm + jl_a_off(16 * g, tid)) =
-          make_uint4(lut[w[g] & 0xFFu], lut[(w[g] >> 8) & 0xFFu], lut[(w[g] >> 16) & 0xFFu],
-                     lut[w[g] >> 24]);
+    for (int g = 0; g < 16; ++g) {
+      const uint32_t v[4] = {lut[w[g] & 0xFFu], lut[(w[g] >> 8) & 0xFFu],
+                             lut[(w[g] >> 16) & 0xFFu], lut[w[g] >> 24]};
+      *reinterpret_cast<uint4*>(sm + jl_a_off(16 * g, tid)) = make_uint4(v[0], v[1], v[2], v[3]);
+      if constexpr (kFlat) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const uint32_t m = (v[i] + 0x7F7F7F7Fu) ^ 0x80808080u;  // M = M' - 1 per byte
+          const uint32_t a = __byte_perm(m, __shfl_xor_sync(0xffffffffu, m, 1), sel1);
+          const uint32_t o = __byte_perm(a, __shfl_xor_sync(0xffffffffu, a, 2), sel2);
+          if (4 * (4 * g + i) + (lane & 3) < rows) *reinterpret_cast<uint32_t*>(rowp) = o;
+          rowp += step4;
+        }
+      }
+    }
     *reinterpret_cast<uint4*>(sm + kTcA + (tid >> 3) * 128 + (tid & 7) * 16) =
         make_uint4(x, 0, 0, 0);
 #pragma unroll
@@ -568,11 +608,21 @@ int launch_jl_project(const FieldParams& f, const uint8_t seed[32], size_t rows,
   unsigned long long* gneg = gpos + rows;
   cudaError_t e = cudaMemsetAsync(gpos, 0, 2 * rows * sizeof(unsigned long long), s);
   if (e != cudaSuccess) return cuda_status(e);
-  static int tc_bps_whole[kMaxDevices] = {}, tc_bps_part[kMaxDevices] = {};
+  static int tc_bps_whole[kMaxDevices] = {}, tc_bps_part[kMaxDevices] = {},
+             tc_bps_flat[kMaxDevices] = {};
   int dev = 0, bps = 0;
-  const unsigned long long tc_chunks = (cols + kTcCols - 1) / kTcCols * num_parts;
+  // the int8 entries come out of the projection kernel itself when the
+  // columns split into 32 polynomials x 8 coefficients and rows fill the blocks
+  const unsigned long long npoly = cols / d;
+  const bool fused_flat = flat_out && packed_len == 64 && d % 8 == 0 && npoly % 32 == 0 &&
+                          (reinterpret_cast<uintptr_t>(flat_out) & 3u) == 0;
+  const unsigned long long tc_per_part =
+      fused_flat ? npoly / 32 * (d / 8) : (cols + kTcCols - 1) / kTcCols;
+  const unsigned long long tc_chunks = tc_per_part * num_parts;
   bool use_tc = cols > 0 && cudaGetDevice(&dev) == cudaSuccess &&
-                (packed_len == 64
+                (fused_flat ? prepare_kernel(jl_tc_kernel<true, true>, kTcSmem, kTcThreads, dev,
+                                             tc_bps_flat, &bps)
+                 : packed_len == 64
                      ? prepare_kernel(jl_tc_kernel<true>, kTcSmem, kTcThreads, dev, tc_bps_whole,
                                       &bps)
                      : prepare_kernel(jl_tc_kernel<false>, kTcSmem, kTcThreads, dev, tc_bps_part,
@@ -599,13 +649,20 @@ int launch_jl_project(const FieldParams& f, const uint8_t seed[32], size_t rows,
   if (use_tc && tc_grid > 0 &&
       (tc_chunks + tc_grid - 1) / tc_grid * (unsigned long long)kTcCols > kTcMaxColsPerCta)
     use_tc = false;
+  const unsigned long long plane = (unsigned long long)num_parts * cols;  // flat bytes per row
   if (use_tc) {
-    if (packed_len == 64)
+    if (fused_flat)
+      jl_tc_kernel<true, true><<<(unsigned)tc_grid, kTcThreads, kTcSmem, s>>>(
+          parts, cols, (int)rows, packed_len, key, tc_chunks, tc_per_part, (int)d, plane,
+          flat_out, gpos, f.q, err);
+    else if (packed_len == 64)
       jl_tc_kernel<true><<<(unsigned)tc_grid, kTcThreads, kTcSmem, s>>>(
-          parts, cols, (int)rows, packed_len, key, tc_chunks, gpos, f.q, err);
+          parts, cols, (int)rows, packed_len, key, tc_chunks, tc_per_part, (int)d, plane,
+          nullptr, gpos, f.q, err);
     else
       jl_tc_kernel<false><<<(unsigned)tc_grid, kTcThreads, kTcSmem, s>>>(
-          parts, cols, (int)rows, packed_len, key, tc_chunks, gpos, f.q, err);
+          parts, cols, (int)rows, packed_len, key, tc_chunks, tc_per_part, (int)d, plane,
+          nullptr, gpos, f.q, err);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_status(e);
   } else if (cols > 0) {
@@ -625,7 +682,7 @@ int launch_jl_project(const FieldParams& f, const uint8_t seed[32], size_t rows,
   jl_finish_kernel<<<(unsigned)((rows + 255) / 256), 256, 0, s>>>(gpos, gneg, p_out, (int)rows, f.q);
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_status(e);
-  if (flat_out && cols > 0) {
+  if (flat_out && cols > 0 && !(use_tc && fused_flat)) {
     const unsigned long long n = cols / d;
     const unsigned long long work = (unsigned long long)num_parts * d * ((n + 127) / 128);
     unsigned long long blocks = (work + kJlWarps - 1) / kJlWarps;

@@ -171,11 +171,15 @@ def test_gadget_decompose_matches_oracle(cuda, oracle):
 
 
 @pytest.mark.parametrize("rows,num_parts,n,d", [(256, 3, 5, 64), (100, 2, 3, 64),
-                                                (256, 1, 130, 64), (7, 4, 2, 8)])
+                                                (256, 1, 130, 64), (7, 4, 2, 8),
+                                                # entries written by the projection kernel
+                                                # (whole blocks, n % 32 == 0, d % 8 == 0)
+                                                (256, 3, 32, 64), (253, 2, 64, 64),
+                                                (256, 2, 96, 8), (255, 1, 32, 16)])
 def test_jl_projection_matches_oracle(cuda, oracle, rows, num_parts, n, d):
     from lattica_b200 import TwistedNttPlan
     from lattica_b200.labrador import JLMatrix
-    q = Q if d == 64 else 17
+    q = 17 if d == 8 else Q
     plan = TwistedNttPlan(q, d)
     F = oracle.Field(q)
     seed = bytes((7 * i + rows) & 0xFF for i in range(32))
@@ -194,7 +198,7 @@ def test_prover_round_matches_oracle(cuda, oracle):
     import torch
     from lattica_b200 import TwistedNttPlan
     from lattica_b200.labrador import CommitKey, prover_round_dev
-    q, d, r, n, kappa = Q, 64, 6, 40, 4
+    q, d, r, n, kappa = Q, 64, 6, 64, 4  # n % 32 == 0: entries from the projection kernel
     plan = TwistedNttPlan(q, d)
     P = oracle.Plan(q, d)
     F = P.field
