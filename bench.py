@@ -326,6 +326,12 @@ def measure_round(dev, reps=50):
     times = _events_ms(lambda: prover_round_dev(key, wit, 256, 4, 256, 4, seed, 256), reps, stream)
     times_x = _events_ms(lambda: prover_round_dev(key, wit, 256, 4, 256, 4, seed, 256, extract=True),
                          max(5, reps // 5), stream)
+    # the round plus the 256 conjugated JL evaluations prove_step aggregates
+    # later; p is read from their coefficient 0 (one keystream pass)
+    prover_round_dev(key, wit, 256, 4, 256, 4, seed, 256, jl_evals=True)
+    times_ev_round = _events_ms(
+        lambda: prover_round_dev(key, wit, 256, 4, 256, 4, seed, 256, jl_evals=True),
+        max(5, reps // 5), stream)
     # end to end: witness from pinned host memory, outputs back to the host
     hw = wit.cpu().pin_memory()
     outs_host = None
@@ -408,6 +414,7 @@ def measure_round(dev, reps=50):
             "jl_evals_ms_p50": _pct(times_ev, 50),
             "crs_expand_ms_p50": _pct(times_crs, 50),
             "round_with_jl_extraction_ms_p50": _pct(times_x, 50),
+            "round_with_jl_evals_ms_p50": _pct(times_ev_round, 50),
             "e2e_round_ms_p50": _pct(e2e, 50), "e2e_round_ms_p99": _pct(e2e, 99),
             "e2e_h2d_bytes": hw.numel() * 4, "e2e_d2h_bytes": d2h, "rounds": reps}
 

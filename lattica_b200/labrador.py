@@ -299,15 +299,31 @@ class RoundOutputs:
     g_limbs: object   # (r(r+1)/2*t2, d) or None
     p: object         # (jl_rows,) or None
     jl_flat: object   # int8 or None
+    jl_evals: object = None  # (256, d) conjugated JL evaluations, or None
 
 
 def prover_round_dev(key: CommitKey, witness, b1: int, t1: int, b2: int, t2: int,
                      jl_seed: bytes | None, jl_rows: int = 256, extract: bool = False,
-                     workspace=None) -> RoundOutputs:
+                     workspace=None, jl_evals: bool = False) -> RoundOutputs:
     """The GPU hot calls of one prove_step (step_prover.rs:118-170) on a CUDA
-    witness tensor (r, n, d): inner commitments + limbs, Gram + limbs, JL."""
+    witness tensor (r, n, d): inner commitments + limbs, Gram + limbs, JL.
+
+    jl_evals=True also returns the 256 conjugated JL evaluations that
+    prove_step aggregates later (step_prover.rs:185-206). Coefficient 0 of
+    evals[m] is sum_u pi_{m,u} s[u], the projection p_m itself, so without
+    `extract` the round runs the evaluation kernel in place of the projection
+    and reads p from it: one keystream pass instead of two."""
     import torch
     r, n, d = (int(x) for x in witness.shape)
+    if jl_evals and (not jl_seed or jl_rows != 256 or d != 64):
+        raise ValueError("jl_evals needs a JL seed, 256 rows and d = 64")
+    if jl_evals and not extract:
+        out = prover_round_dev(key, witness, b1, t1, b2, t2, None, jl_rows, False, workspace)
+        jl = JLMatrix.from_seed(jl_rows, n * d, jl_seed)
+        ev = jl.conjugated_evals(key.plan, witness.reshape(r, n * d), r, d)
+        out.p = ev[:, 0].contiguous()
+        out.jl_evals = ev
+        return out
     plan = key.plan
     lib = _lib.load()
     dev = witness.device
@@ -330,7 +346,11 @@ def prover_round_dev(key: CommitKey, witness, b1: int, t1: int, b2: int, t2: int
         p.data_ptr() if p is not None else None, flat.data_ptr() if flat is not None else None,
         workspace.data_ptr(), workspace.numel(), _stream_ptr(witness))
     raise_status(st, "grid_gpu_prover_round_dev")
-    return RoundOutputs(t_limbs, g, g_limbs, p, flat)
+    out = RoundOutputs(t_limbs, g, g_limbs, p, flat)
+    if jl_evals:
+        jl = JLMatrix.from_seed(jl_rows, n * d, jl_seed)
+        out.jl_evals = jl.conjugated_evals(plan, witness.reshape(r, n * d), r, d)
+    return out
 
 
 def _canonical(words, q: int):

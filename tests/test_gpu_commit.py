@@ -220,3 +220,34 @@ def test_prover_round_matches_oracle(cuda, oracle):
     assert np.array_equal(_host(out.p), p)
     assert np.array_equal(out.jl_flat.cpu().numpy(), flat)
     plan.check_device()
+
+
+@pytest.mark.parametrize("extract", [False, True])
+def test_prover_round_with_jl_evals(cuda, oracle, extract):
+    """The round's JL evaluations; without extraction p comes from their coefficient 0."""
+    import torch
+    from lattica_b200 import TwistedNttPlan
+    from lattica_b200.labrador import CommitKey, prover_round_dev
+    q, d, r, n, kappa = Q, 64, 3, 20, 4
+    plan = TwistedNttPlan(q, d)
+    P = oracle.Plan(q, d)
+    F = P.field
+    S = _rand(q, (r, n, d), 41)
+    A = _rand(q, (kappa, n, d), 43)
+    seed = bytes((5 * i + 1) & 0xFF for i in range(32))
+    key = CommitKey(plan, A, kappa, n)
+    out = prover_round_dev(key, _dev(S, cuda), 256, 4, 256, 4, seed, 256, extract=extract,
+                           jl_evals=True)
+    torch.cuda.synchronize()
+    p, flat = oracle.jl_project(F, seed, 256, S.reshape(r, n * d), r, n * d, d)
+    assert np.array_equal(_host(out.p), p)
+    assert np.array_equal(_host(out.jl_evals),
+                          P.jl_evals(flat, 256, S.reshape(r, n * d), r, n).reshape(256, d))
+    assert (out.jl_flat is not None) == extract
+    t = P.matvec(A, kappa, n, S, r)
+    assert np.array_equal(_host(out.t_limbs),
+                          oracle.decompose_polys(F, d, t, 256, 4).reshape(-1, d))
+    assert np.array_equal(_host(out.g), P.gram(S, r, n, threads=0).reshape(-1, d))
+    with pytest.raises(ValueError):
+        prover_round_dev(key, _dev(S, cuda), 256, 4, 256, 4, None, 256, jl_evals=True)
+    plan.check_device()
