@@ -65,6 +65,8 @@ bool dims_ok(size_t a, size_t b, size_t c) {
 int commit_core(const grid_gpu_matrix* A, const uint32_t* s, size_t batch, uint32_t* t,
                 Carver& cv, cudaStream_t st) {
   const grid_gpu_plan* p = A->plan;
+  if (commit_small_fits(p, A->rows, A->cols, batch))
+    return launch_commit_small(p, A->d_evals, A->rows, A->cols, A->ld, s, batch, t, st);
   uint32_t* s_hat = cv.take<uint32_t>(batch * A->cols * p->d);
   const size_t ew = emm_workspace_words(p, (int)batch, (int)A->rows, (int)A->cols, EMM_DENSE);
   uint32_t* work = ew ? cv.take<uint32_t>(ew) : nullptr;

@@ -86,6 +86,12 @@ namespace grid {
 int launch_ntt(const grid_gpu_plan* p, int mode, const uint32_t* a, const uint32_t* b,
                uint32_t* out, size_t npolys, cudaStream_t s);
 int ntt_max_degree();
+// One-launch commitment t = A s for small shapes (d = 64, rows <= 32, cols <= 128,
+// batch <= 1024): transform, contraction and inverse in one kernel.
+bool commit_small_fits(const grid_gpu_plan* p, size_t rows, size_t cols, size_t batch);
+int launch_commit_small(const grid_gpu_plan* p, const uint32_t* A_evals, size_t rows,
+                        size_t cols, size_t ld, const uint32_t* s, size_t batch, uint32_t* t,
+                        cudaStream_t st);
 // ntt_tc.cu (d = 64, tcgen05)
 bool ntt_tc_available(const grid_gpu_plan* p);
 int launch_ntt_tc(const grid_gpu_plan* p, int mode, const uint32_t* a, const uint32_t* b,

@@ -476,6 +476,145 @@ __global__ void __launch_bounds__(kThreads, 1) nttT_kernel(const uint32_t* __res
 }
 
 // ---------------------------------------------------------------------------
+// Small commitments in one launch: t_b = A s_b for witness vectors of at most
+// kSmallMaxCols polynomials and matrices of at most kSmallMaxRows rows (the
+// plain Ajtai commitment: 8 x 64, 64 witnesses). Three separate launches
+// (transform, contraction, inverse) are latency-bound at that size. CTA b
+// takes witness b:
+//  * its polynomials go to shared memory (coalesced), one thread transforms
+//    each and writes the canonical evaluations back in slot order;
+//  * thread e accumulates evaluation point e of every output row over the
+//    columns (96-bit carry chains), reading the prepared matrix's evaluations
+//    coalesced from L2;
+//  * one thread per output row runs the inverse transform and stores it.
+// The transforms are the thread-per-polynomial stages above (bit-identical
+// to the other engines); the accumulation is the one of emm_kernel.
+// ---------------------------------------------------------------------------
+constexpr int kSmallMaxCols = 128;
+constexpr int kSmallMaxRows = 32;
+constexpr int kSmallSlots = 8;  // output-row slots: CTA = D evaluation points x 8 slots
+
+// The thread-per-polynomial stages without the per-stage CTA barriers, for
+// threads that transform alone (the barriers only keep a CTA's warps in step).
+template <int D, int LEN>
+__device__ __forceinline__ void fwd1_alone(uint32_t (&x)[D], const Tw1<D>& tw, const Consts& c) {
+#pragma unroll
+  for (int g = 0; g < D / (2 * LEN); ++g) {
+    const int k = D / (2 * LEN) + g;
+#pragma unroll
+    for (int j = g * 2 * LEN; j < g * 2 * LEN + LEN; ++j)
+      ct_bfly(x[j], x[j + LEN], tw.fw[k][0], tw.fw[k][1], c);
+  }
+  if constexpr (LEN > 1) fwd1_alone<D, LEN / 2>(x, tw, c);
+}
+
+template <int D, int LEN>
+__device__ __forceinline__ void inv1_alone(uint32_t (&x)[D], const Tw1<D>& tw, const Consts& c) {
+  if constexpr (LEN == D / 2) {
+#pragma unroll
+    for (int j = 0; j < LEN; ++j) {
+      const uint32_t s = add_canon(x[j], x[j + LEN], c.q);
+      const uint32_t d = sub_lazy(x[j], x[j + LEN], c.q);
+      x[j] = mont_c(s, tw.ninv[0], tw.ninv[1], c.q);
+      x[j + LEN] = mont_c(d, tw.iw1n[0], tw.iw1n[1], c.q);
+    }
+  } else {
+#pragma unroll
+    for (int g = 0; g < D / (2 * LEN); ++g) {
+      const int k = D / (2 * LEN) + g;
+#pragma unroll
+      for (int j = g * 2 * LEN; j < g * 2 * LEN + LEN; ++j)
+        gs_bfly(x[j], x[j + LEN], tw.iw[k][0], tw.iw[k][1], c);
+    }
+    inv1_alone<D, LEN * 2>(x, tw, c);
+  }
+}
+
+template <int D, int RPT>
+__global__ void __launch_bounds__(D * kSmallSlots) commit_small_kernel(
+    const uint32_t* __restrict__ A, int rows, int cols, int ld, const uint32_t* __restrict__ s,
+    uint32_t* __restrict__ t, const __grid_constant__ Tw1<D> tw) {
+  constexpr int LOGD = ilog2(D);
+  constexpr int PS = D + 4;  // padded row stride (words)
+  constexpr int NT = D * kSmallSlots;
+  extern __shared__ __align__(16) uint32_t small_smem[];
+  uint32_t* sh = small_smem;              // [cols][PS]: witness, then its evaluations
+  uint32_t* oh = small_smem + cols * PS;  // [rows][PS]: output evaluations
+  const int tid = threadIdx.x;
+  const Consts c = consts_of(tw.f);
+  const size_t b = blockIdx.x;
+
+  const uint4* src = reinterpret_cast<const uint4*>(s + b * (size_t)cols * D);
+  for (int i = tid; i < cols * (D / 4); i += NT)
+    *reinterpret_cast<uint4*>(sh + (i / (D / 4)) * PS + 4 * (i % (D / 4))) = src[i];
+  __syncthreads();
+
+  if (tid < cols) {  // forward transform of polynomial tid (cols <= NT)
+    uint32_t* row = sh + tid * PS;
+    uint32_t x[D];
+#pragma unroll
+    for (int cc = 0; cc < D / 4; ++cc) {
+      const uint4 v = reinterpret_cast<const uint4*>(row)[cc];
+      x[4 * cc + 0] = v.x;
+      x[4 * cc + 1] = v.y;
+      x[4 * cc + 2] = v.z;
+      x[4 * cc + 3] = v.w;
+    }
+    fwd1_alone<D, D / 2>(x, tw, c);
+#pragma unroll
+    for (int cc = 0; cc < D / 4; ++cc)  // lazy words -> canonical, slot order
+      reinterpret_cast<uint4*>(row)[cc] =
+          make_uint4(mont_v(x[brv(4 * cc + 0, LOGD)], c.r1, c.q, c.qinv),
+                     mont_v(x[brv(4 * cc + 1, LOGD)], c.r1, c.q, c.qinv),
+                     mont_v(x[brv(4 * cc + 2, LOGD)], c.r1, c.q, c.qinv),
+                     mont_v(x[brv(4 * cc + 3, LOGD)], c.r1, c.q, c.qinv));
+  }
+  __syncthreads();
+
+  // out_hat[r][e] = sum_k A[r][k][e] s_hat[k][e] * 2^-32: thread (e, slot)
+  // owns rows slot, slot + 8, ... (RPT of them), all columns; 16 matrix loads
+  // in flight per thread
+  {
+    const int e = tid % D, slot = tid / D;
+    Acc96 acc[RPT];
+#pragma unroll
+    for (int i = 0; i < RPT; ++i) acc96_zero(acc[i]);
+#pragma unroll(16 / RPT)
+    for (int k = 0; k < cols; ++k) {
+      const uint32_t sv = sh[k * PS + e];
+#pragma unroll
+      for (int i = 0; i < RPT; ++i) {
+        const int r = slot + kSmallSlots * i;
+        if (r < rows) acc96_mad(acc[i], __ldg(A + ((size_t)r * ld + k) * D + e), sv);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < RPT; ++i) {
+      const int r = slot + kSmallSlots * i;
+      if (r < rows) oh[r * PS + e] = acc96_reduce(acc[i], tw.f);
+    }
+  }
+  __syncthreads();
+
+  if (tid < rows) {  // inverse transform of output row tid
+    uint32_t x[D];
+#pragma unroll
+    for (int cc = 0; cc < D / 4; ++cc) {
+      const uint4 v = reinterpret_cast<const uint4*>(oh + tid * PS)[cc];
+      x[brv(4 * cc + 0, LOGD)] = v.x;
+      x[brv(4 * cc + 1, LOGD)] = v.y;
+      x[brv(4 * cc + 2, LOGD)] = v.z;
+      x[brv(4 * cc + 3, LOGD)] = v.w;
+    }
+    inv1_alone<D, 1>(x, tw, c);
+    uint4* dst = reinterpret_cast<uint4*>(t + (b * rows + tid) * D);
+#pragma unroll
+    for (int cc = 0; cc < D / 4; ++cc)
+      dst[cc] = make_uint4(x[4 * cc + 0], x[4 * cc + 1], x[4 * cc + 2], x[4 * cc + 3]);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Host launchers
 // ---------------------------------------------------------------------------
 template <int D>
@@ -566,6 +705,39 @@ int launch_ntt(const grid_gpu_plan* p, int mode, const uint32_t* a, const uint32
     case MODE_MULINV: return dispatch<MODE_MULINV>(p, a, b, out, npolys, s);
     default: return GRID_ERR_INVALID_PARAMETERS;
   }
+}
+
+bool commit_small_fits(const grid_gpu_plan* p, size_t rows, size_t cols, size_t batch) {
+  // one CTA per witness re-reads the matrix from L2: keep to small batches
+  return p->d == 64 && rows >= 1 && rows <= (size_t)kSmallMaxRows && cols >= 1 &&
+         cols <= (size_t)kSmallMaxCols && batch >= 1 && batch <= 1024;
+}
+
+int launch_commit_small(const grid_gpu_plan* p, const uint32_t* A_evals, size_t rows,
+                        size_t cols, size_t ld, const uint32_t* s, size_t batch, uint32_t* t,
+                        cudaStream_t st) {
+  constexpr int D = 64;
+  static_assert(kSmallMaxRows <= D * kSmallSlots && kSmallMaxCols <= D * kSmallSlots,
+                "one transform per thread");
+  static_assert(kSmallMaxRows == 4 * kSmallSlots, "rows per thread: 1, 2 or 4");
+  if (!commit_small_fits(p, rows, cols, batch)) return GRID_ERR_INVALID_PARAMETERS;
+  const size_t smem = (cols + rows) * (D + 4) * sizeof(uint32_t);
+  // the shared-memory limit is set once per device: set it for the largest shape
+  constexpr size_t kSmemMax = (size_t)(kSmallMaxCols + kSmallMaxRows) * (D + 4) * sizeof(uint32_t);
+  const Tw1<D> tw = make_tw1<D>(p);
+  // rows per thread: 1, 2 or 4
+  auto run = [&](auto kernel, int* cache) -> int {
+    int bps = 0;
+    const int rc = prepare_kernel(kernel, kSmemMax, D * kSmallSlots, p->device, cache, &bps);
+    if (rc) return rc;
+    kernel<<<(unsigned)batch, D * kSmallSlots, smem, st>>>(A_evals, (int)rows, (int)cols, (int)ld,
+                                                           s, t, tw);
+    return cuda_status(cudaGetLastError());
+  };
+  static int cache1[kMaxDevices] = {}, cache2[kMaxDevices] = {}, cache4[kMaxDevices] = {};
+  if (rows <= (size_t)kSmallSlots) return run(commit_small_kernel<D, 1>, cache1);
+  if (rows <= 2 * (size_t)kSmallSlots) return run(commit_small_kernel<D, 2>, cache2);
+  return run(commit_small_kernel<D, 4>, cache4);
 }
 
 }  // namespace grid

@@ -43,6 +43,12 @@ def _host(t):
     (Q, 64, 40, 70, 100),       # NP 48
     (Q, 64, 49, 20, 65),        # NP 64, just past 64 X rows
     (Q, 64, 64, 33, 128),       # NP 64, 128 X rows
+    # one-launch small commitments (rows <= 32, cols <= 128, batch <= 1024)
+    (Q, 64, 1, 1, 1),
+    (Q, 64, 5, 100, 2),         # a second group of 64 columns, partly filled
+    (Q, 64, 32, 128, 3),        # largest rows and cols
+    (Q, 64, 31, 65, 7),
+    (Q, 64, 8, 64, 1024),       # largest batch
 ])
 def test_commit_matches_oracle(cuda, oracle, q, d, rows, cols, batch):
     from lattica_b200 import TwistedNttPlan
