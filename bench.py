@@ -234,17 +234,20 @@ def _pct(xs, p):
 
 
 def measure_commit_plain(dev, reps=50):
-    """Plain Ajtai commit: A = 8 x 64 ring matrix (d = 64, q = 4294966657),
-    64 witnesses of 64 ternary polys; t = A s per witness."""
+    """Plain Ajtai commit: A = 8 x 64 ring matrix (d = 64, q = 4294966657)
+    expanded from a ChaCha20 seed (ChaCha20Rng, the reference's
+    sample_uniform_mat rule), 64 witnesses of 64 ternary polys; t = A s per
+    witness."""
     import ctypes as C
     import torch
     from lattica_b200 import TwistedNttPlan, _lib
     from lattica_b200.commit import PreparedMatrix
+    from lattica_b200.labrador import sample_uniform_polys
     q, d, rows, cols, batch = Q64, 64, 8, 64, 64
     lib = _lib.load()
     plan = TwistedNttPlan(q, d)
     rng = np.random.default_rng(11)
-    A = rng.integers(0, q, (rows, cols, d), dtype=np.uint64).astype(np.uint32)
+    A = sample_uniform_polys(plan, bytes(range(100, 132)), rows * cols).reshape(rows, cols, d)
     s_host = _mont_words(q, rng.integers(-1, 2, (batch, cols, d))).reshape(batch, cols, d)
     M = PreparedMatrix(plan, A, rows, cols)
     s = torch.from_numpy(s_host.view(np.int32)).to(dev)
@@ -292,7 +295,8 @@ def measure_commit_plain(dev, reps=50):
             P.matvec(A, rows, cols, s_host, batch, threads=threads)
         cpu[label] = batch * 3 / (time.perf_counter() - t0)
     assert np.array_equal(t.cpu().numpy().view(np.uint32).reshape(-1), want), "GPU != oracle"
-    return {"workload": "plain Ajtai commit: A 8x64, d=64, 64 ternary witnesses per batch",
+    return {"workload": "plain Ajtai commit: A 8x64 from a ChaCha20 seed, d=64, 64 ternary "
+                        "witnesses per batch",
             "cpu_oracle_commits_per_s": {"threads_1": cpu["1t"], "threads_all": cpu["all"],
                                          "cores": os.cpu_count() or 1},
             "commits_per_s": batch / (med_b / 1e3), "batch_ms_p50": med_b,
