@@ -10,6 +10,8 @@ the median CUDA-event time.
     python -m lattica_b200.cases amortize --reps 4   # z = sum_i c_i s_i, r = 64, n = 2048
     python -m lattica_b200.cases jl_evals --reps 4   # 256 conjugated JL evaluations, same witness
     python -m lattica_b200.cases ntt256 --reps 4     # d = 256 products, 2^20 polys at q'
+    python -m lattica_b200.cases commit_plain --reps 5  # A 8 x 64 from a seed, 64 ternary witnesses
+    python -m lattica_b200.cases jl_extract --reps 3 --parts 16  # JL p + int8 entries
 
 Sizes: r = 64 witness vectors of n = 2048 polys (d = 64, coefficients in
 [-2^11, 2^11], as Montgomery words), kappa = 16, JL 256 rows, base 2^8 x 4
@@ -30,8 +32,58 @@ def _uniform(torch, dev, g, q, shape):
     return torch.randint(0, q, shape, dtype=torch.int64, device=dev, generator=g).to(torch.int32)
 
 
-def build(case: str):
-    """Returns a zero-argument callable that runs one instance of `case`."""
+def _commit_plain(torch, dev, g, plan):
+    """The plain Ajtai commitment: A 8 x 64 expanded from a seed, 64 witnesses of
+    64 ternary polynomials, through grid_gpu_commit_dev."""
+    from lattica_b200 import _lib
+    from lattica_b200.commit import PreparedMatrix
+    from lattica_b200.labrador import sample_uniform_polys
+    rows, cols, batch = 8, 64, 64
+    lib = _lib.load()
+    A = sample_uniform_polys(plan, bytes(range(100, 132)), rows * cols).reshape(rows, cols, 64)
+    M = PreparedMatrix(plan, A, rows, cols)
+    tern = torch.randint(-1, 2, (batch * cols, 64), dtype=torch.int64, device=dev, generator=g)
+    s = ((tern % Q) * ((1 << 32) % Q) % Q).to(torch.int32)
+    t = torch.empty((batch * rows, 64), dtype=torch.int32, device=dev)
+    ws = torch.empty(max(256, M.workspace_bytes(batch)), dtype=torch.uint8, device=dev)
+
+    def run():
+        st = torch.cuda.current_stream(dev).cuda_stream
+        code = lib.grid_gpu_commit_dev(M.handle, s.data_ptr(), batch, t.data_ptr(), ws.data_ptr(),
+                                       ws.numel(), st)
+        if code:
+            raise RuntimeError(f"grid_gpu_commit_dev: {code}")
+    run.keep = (M, A)
+    return run
+
+
+def _jl_extract(torch, dev, g, plan, parts, n):
+    """JL projection of `parts` witness vectors (n polys, d = 64) by 256 rows,
+    with the int8 entries, through grid_gpu_jl_project_dev."""
+    import ctypes as C
+    from lattica_b200 import _lib
+    lib = _lib.load()
+    S = _uniform(torch, dev, g, Q, (parts, n * 64))
+    seed = (C.c_uint8 * 32)(*range(32))
+    nb = C.c_size_t()
+    lib.grid_gpu_jl_workspace(256, C.byref(nb))
+    ws = torch.empty(max(256, nb.value), dtype=torch.uint8, device=dev)
+    p = torch.empty(256, dtype=torch.int32, device=dev)
+    flat = torch.empty(256 * parts * n * 64, dtype=torch.int8, device=dev)
+
+    def run():
+        st = torch.cuda.current_stream(dev).cuda_stream
+        code = lib.grid_gpu_jl_project_dev(plan.handle, seed, 256, S.data_ptr(), parts, n * 64, 64,
+                                           p.data_ptr(), flat.data_ptr(), ws.data_ptr(),
+                                           ws.numel(), st)
+        if code:
+            raise RuntimeError(f"grid_gpu_jl_project_dev: {code}")
+    return run
+
+
+def build(case: str, parts: int = 64):
+    """Returns a zero-argument callable that runs one instance of `case`
+    (`parts`: witness vectors of the jl_extract case)."""
     import torch
     from lattica_b200 import TwistedNttPlan
     from lattica_b200.labrador import (CommitKey, JLMatrix, amortize_witness, compute_garbage_g,
@@ -45,6 +97,10 @@ def build(case: str):
         b = _uniform(torch, dev, g, Q256, (1 << 20, 256))
         return lambda: plan.ntt_mul_inverse(a, b)
     plan = TwistedNttPlan(Q, 64)
+    if case == "commit_plain":
+        return _commit_plain(torch, dev, g, plan)
+    if case == "jl_extract":
+        return _jl_extract(torch, dev, g, plan, parts, n)
     wit = _witness(torch, dev, g, Q, (r, n, 64))
     if case == "gram":
         return lambda: compute_garbage_g(plan, wit)
@@ -70,11 +126,12 @@ def build(case: str):
 def main(argv=None) -> None:
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("case", choices=["round", "gram", "garbage_h", "amortize", "jl_evals", "commit",
-                                       "ntt256"])
+                                       "ntt256", "commit_plain", "jl_extract"])
     ap.add_argument("--reps", type=int, default=4)
+    ap.add_argument("--parts", type=int, default=64, help="witness vectors (jl_extract)")
     args = ap.parse_args(argv)
     import torch
-    fn = build(args.case)
+    fn = build(args.case, args.parts)
     fn()
     torch.cuda.synchronize()
     times = []
