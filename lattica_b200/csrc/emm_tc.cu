@@ -17,9 +17,11 @@
 //    per CTA (the K range is split beyond that and the partials are summed).
 // A CTA takes EPC consecutive evaluation points and a K range; its 256 threads
 // gather the operands of each 32-word K chunk from global memory (the words of
-// one (row, k) for the CTA's evaluation points are contiguous), scale and
-// byte-transpose Y, and write both 128-byte-swizzled tiles into one of two
-// shared-memory stages; thread 0 issues 4 MMAs (M 128, N 4 NP, K 32) per
+// one (row, k) for the CTA's evaluation points are contiguous: one vector
+// load), into one of two register buffers sized for the shape (X rows <= MX,
+// Y rows <= NP), so that chunk c + 1's loads are in flight while chunk c is
+// scaled, byte-transposed and written as two 128-byte-swizzled tiles into one
+// of two shared-memory stages; thread 0 issues 4 MMAs (M 128, N 4 NP, K 32) per
 // evaluation point and commits them to the stage's mbarrier, which the
 // producers wait on before they reuse the stage. Tensor memory holds the EPC
 // accumulators (4 NP columns each); the epilogue combines the planes, reduces
