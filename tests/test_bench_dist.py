@@ -42,3 +42,22 @@ def test_reference_arm_runs_on_rank_zero_only(capsys):
         workload, steps, warmup = "ntt64", 1, 3
     assert bench.run_reference(Args(), 1, 2) is None
     assert capsys.readouterr().out == ""
+
+
+def test_reference_arm_line_keeps_the_contract(capsys):
+    """Rank 0 of the reference arm prints one JSON line with the contract's keys."""
+    sys.path.insert(0, ROOT)
+    import bench
+
+    class Args:
+        workload, steps, warmup = "ntt64", 1, 3
+    bench.run_reference(Args(), 0, 1)
+    line = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["metric"] == bench.METRIC
+    assert line["unit"] == "polys/s" and line["value"] > 0 and line["higher_is_better"] is True
+    assert line["n_gpus"] == 1 and line["steps"] == 1 and line["warmup"] >= 3
+    cb = line["cpu_baseline"]
+    assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["value"] == line["value"]
+    assert cb["host"]["nproc"] >= 1 and cb["host"]["model"]
+    assert line["e2e"] == {"value": line["value"], "unit": "polys/s", "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": 0}
