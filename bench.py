@@ -273,6 +273,41 @@ def measure_commit_plain(dev, reps=50):
         per_call()
     tb = _events_ms(batched, reps, stream)
     tp = _events_ms(per_call, max(5, reps // 5), stream)
+    # steady state: batches back to back between two events, so the GPU does
+    # not idle while the host prepares each call (the per-call times above
+    # include that launch latency)
+    steady_n = 200
+    s0 = torch.cuda.Event(enable_timing=True)
+    s1 = torch.cuda.Event(enable_timing=True)
+    s0.record(stream)
+    for _ in range(steady_n):
+        batched()
+    s1.record(stream)
+    s1.synchronize()
+    steady_ms = s0.elapsed_time(s1) / steady_n
+    # device throughput: 50 batches captured once in a CUDA graph and replayed,
+    # so the host's per-call cost is out of the timed region
+    graph_ms = None
+    try:
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            cap = torch.cuda.current_stream(dev).cuda_stream
+            for _ in range(50):
+                assert lib.grid_gpu_commit_dev(M.handle, s.data_ptr(), batch, t.data_ptr(),
+                                               ws.data_ptr(), ws.numel(), cap) == 0
+        graph.replay()
+        torch.cuda.synchronize()
+        g0 = torch.cuda.Event(enable_timing=True)
+        g1 = torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        for _ in range(4):
+            graph.replay()
+        g1.record(stream)
+        g1.synchronize()
+        graph_ms = g0.elapsed_time(g1) / 200
+        del graph
+    except Exception as exc:  # a capture failure leaves the other figures intact
+        print(f"config 0 graph timing skipped: {exc}", file=sys.stderr)
     hs = torch.from_numpy(s_host.view(np.int32).copy()).pin_memory()
     ht = torch.empty((batch, rows, d), dtype=torch.int32).pin_memory()
     e2e = []
@@ -300,6 +335,9 @@ def measure_commit_plain(dev, reps=50):
             "cpu_oracle_commits_per_s": {"threads_1": cpu["1t"], "threads_all": cpu["all"],
                                          "cores": os.cpu_count() or 1},
             "commits_per_s": batch / (med_b / 1e3), "batch_ms_p50": med_b,
+            "commits_per_s_steady": batch / (steady_ms / 1e3), "batch_ms_steady": steady_ms,
+            "commits_per_s_graph": batch / (graph_ms / 1e3) if graph_ms else None,
+            "batch_ms_graph": graph_ms,
             "per_call_commits_per_s": batch / (med_p / 1e3),
             "e2e_commits_per_s": batch / (med_e / 1e3), "e2e_batch_ms_p50": med_e,
             "e2e_h2d_bytes": s_host.nbytes, "e2e_d2h_bytes": batch * rows * d * 4}

@@ -481,95 +481,78 @@ __global__ void __launch_bounds__(kThreads, 1) nttT_kernel(const uint32_t* __res
 // plain Ajtai commitment: 8 x 64, 64 witnesses). Three separate launches
 // (transform, contraction, inverse) are latency-bound at that size. CTA b
 // takes witness b:
-//  * its polynomials go to shared memory (coalesced), one thread transforms
-//    each and writes the canonical evaluations back in slot order;
-//  * thread e accumulates evaluation point e of every output row over the
-//    columns (96-bit carry chains), reading the prepared matrix's evaluations
-//    coalesced from L2;
-//  * one thread per output row runs the inverse transform and stores it.
-// The transforms are the thread-per-polynomial stages above (bit-identical
-// to the other engines); the accumulation is the one of emm_kernel.
+//  * its polynomials go to shared memory (coalesced); eight threads transform
+//    each and write the canonical evaluations back in slot order;
+//  * thread (e, slot) accumulates evaluation point e of output rows slot,
+//    slot + 8, ... over the columns (96-bit carry chains), reading the
+//    prepared matrix's evaluations coalesced from L2;
+//  * eight threads per output row run the inverse transform and store it.
+// The transforms are the shuffle stages of the d = 128 / 256 engine
+// (fwdT_stages / invT_stages, bit-identical to the other engines); the
+// accumulation is the one of emm_kernel.
 // ---------------------------------------------------------------------------
 constexpr int kSmallMaxCols = 128;
 constexpr int kSmallMaxRows = 32;
 constexpr int kSmallSlots = 8;  // output-row slots: CTA = D evaluation points x 8 slots
 
-// The thread-per-polynomial stages without the per-stage CTA barriers, for
-// threads that transform alone (the barriers only keep a CTA's warps in step).
-template <int D, int LEN>
-__device__ __forceinline__ void fwd1_alone(uint32_t (&x)[D], const Tw1<D>& tw, const Consts& c) {
-#pragma unroll
-  for (int g = 0; g < D / (2 * LEN); ++g) {
-    const int k = D / (2 * LEN) + g;
-#pragma unroll
-    for (int j = g * 2 * LEN; j < g * 2 * LEN + LEN; ++j)
-      ct_bfly(x[j], x[j + LEN], tw.fw[k][0], tw.fw[k][1], c);
-  }
-  if constexpr (LEN > 1) fwd1_alone<D, LEN / 2>(x, tw, c);
-}
-
-template <int D, int LEN>
-__device__ __forceinline__ void inv1_alone(uint32_t (&x)[D], const Tw1<D>& tw, const Consts& c) {
-  if constexpr (LEN == D / 2) {
-#pragma unroll
-    for (int j = 0; j < LEN; ++j) {
-      const uint32_t s = add_canon(x[j], x[j + LEN], c.q);
-      const uint32_t d = sub_lazy(x[j], x[j + LEN], c.q);
-      x[j] = mont_c(s, tw.ninv[0], tw.ninv[1], c.q);
-      x[j + LEN] = mont_c(d, tw.iw1n[0], tw.iw1n[1], c.q);
-    }
-  } else {
-#pragma unroll
-    for (int g = 0; g < D / (2 * LEN); ++g) {
-      const int k = D / (2 * LEN) + g;
-#pragma unroll
-      for (int j = g * 2 * LEN; j < g * 2 * LEN + LEN; ++j)
-        gs_bfly(x[j], x[j + LEN], tw.iw[k][0], tw.iw[k][1], c);
-    }
-    inv1_alone<D, LEN * 2>(x, tw, c);
-  }
-}
+// Transforms use T = 8 threads per polynomial (the shuffle stages of the
+// d = 128 / 256 engine), so 64 polynomials occupy all 16 warps; element
+// placement as in nttT_kernel: thread t of a polynomial holds 4-word chunks
+// T m + t, evaluations go to slot brv(i) | brv(4 t).
+constexpr int kSmallT = 8;
 
 template <int D, int RPT>
 __global__ void __launch_bounds__(D * kSmallSlots) commit_small_kernel(
     const uint32_t* __restrict__ A, int rows, int cols, int ld, const uint32_t* __restrict__ s,
-    uint32_t* __restrict__ t, const __grid_constant__ Tw1<D> tw) {
+    uint32_t* __restrict__ t_out, const uint2* __restrict__ gtw, FieldParams f) {
   constexpr int LOGD = ilog2(D);
-  constexpr int PS = D + 4;  // padded row stride (words)
+  constexpr int T = kSmallT;
+  constexpr int E = D / T;            // words per thread in a transform
+  constexpr int PS = D + 4 * T;       // padded row stride (words)
   constexpr int NT = D * kSmallSlots;
+  constexpr int PPP = NT / T;         // polynomials per transform pass
+  constexpr int TWN = 2 * D + 2;      // twiddle entries (uint2)
   extern __shared__ __align__(16) uint32_t small_smem[];
-  uint32_t* sh = small_smem;              // [cols][PS]: witness, then its evaluations
-  uint32_t* oh = small_smem + cols * PS;  // [rows][PS]: output evaluations
+  uint2* tws = reinterpret_cast<uint2*>(small_smem);
+  uint32_t* sh = small_smem + 2 * TWN + 4;  // [cols][PS]: witness, then its evaluations
+  uint32_t* oh = sh + cols * PS;            // [rows][PS]: output evaluations
   const int tid = threadIdx.x;
-  const Consts c = consts_of(tw.f);
+  const int pl = tid / T, t = tid % T;
+  const int bt_t = brv(4 * t, LOGD);
+  const Consts c = consts_of(f);
   const size_t b = blockIdx.x;
 
+  for (int i = tid; i < TWN; i += NT) tws[i] = gtw[i];
   const uint4* src = reinterpret_cast<const uint4*>(s + b * (size_t)cols * D);
   for (int i = tid; i < cols * (D / 4); i += NT)
     *reinterpret_cast<uint4*>(sh + (i / (D / 4)) * PS + 4 * (i % (D / 4))) = src[i];
   __syncthreads();
 
-  if (tid < cols) {  // forward transform of polynomial tid (cols <= NT)
-    uint32_t* row = sh + tid * PS;
-    uint32_t x[D];
+  // forward transforms, PPP polynomials per pass; groups past the last
+  // polynomial transform row 0 and discard it (the stages hold CTA barriers
+  // and shuffles, so every thread runs them)
+  for (int k0 = 0; k0 < cols; k0 += PPP) {
+    const int k = k0 + pl;
+    uint32_t* row = sh + (k < cols ? k : 0) * PS;
+    uint32_t x[E];
 #pragma unroll
-    for (int cc = 0; cc < D / 4; ++cc) {
-      const uint4 v = reinterpret_cast<const uint4*>(row)[cc];
-      x[4 * cc + 0] = v.x;
-      x[4 * cc + 1] = v.y;
-      x[4 * cc + 2] = v.z;
-      x[4 * cc + 3] = v.w;
+    for (int m = 0; m < E / 4; ++m) {
+      const uint4 v = reinterpret_cast<const uint4*>(row)[T * m + t];
+      x[4 * m + 0] = v.x;
+      x[4 * m + 1] = v.y;
+      x[4 * m + 2] = v.z;
+      x[4 * m + 3] = v.w;
     }
-    fwd1_alone<D, D / 2>(x, tw, c);
+    fwdT_stages<D, T, D / 2>(x, tws, t, c);  // ends with a CTA barrier: every row read
+    if (k < cols) {
 #pragma unroll
-    for (int cc = 0; cc < D / 4; ++cc)  // lazy words -> canonical, slot order
-      reinterpret_cast<uint4*>(row)[cc] =
-          make_uint4(mont_v(x[brv(4 * cc + 0, LOGD)], c.r1, c.q, c.qinv),
-                     mont_v(x[brv(4 * cc + 1, LOGD)], c.r1, c.q, c.qinv),
-                     mont_v(x[brv(4 * cc + 2, LOGD)], c.r1, c.q, c.qinv),
-                     mont_v(x[brv(4 * cc + 3, LOGD)], c.r1, c.q, c.qinv));
+      for (int e = 0; e < E; ++e) {  // lazy words -> canonical, slot order
+        const int i = 4 * T * (e >> 2) + (e & 3);
+        row[brv(i, LOGD) | bt_t] = mont_v(x[e], c.r1, c.q, c.qinv);
+      }
+    }
+    __syncthreads();
   }
-  __syncthreads();
 
   // out_hat[r][e] = sum_k A[r][k][e] s_hat[k][e] * 2^-32: thread (e, slot)
   // owns rows slot, slot + 8, ... (RPT of them), all columns; 16 matrix loads
@@ -579,38 +562,50 @@ __global__ void __launch_bounds__(D * kSmallSlots) commit_small_kernel(
     Acc96 acc[RPT];
 #pragma unroll
     for (int i = 0; i < RPT; ++i) acc96_zero(acc[i]);
-#pragma unroll(16 / RPT)
-    for (int k = 0; k < cols; ++k) {
-      const uint32_t sv = sh[k * PS + e];
+    // 16 columns at a time: every matrix load of the group is issued before
+    // the first multiply-add uses one
+    constexpr int KB = 16;
+    for (int k0 = 0; k0 < cols; k0 += KB) {
+      uint32_t av[RPT][KB], sv[KB];
 #pragma unroll
-      for (int i = 0; i < RPT; ++i) {
-        const int r = slot + kSmallSlots * i;
-        if (r < rows) acc96_mad(acc[i], __ldg(A + ((size_t)r * ld + k) * D + e), sv);
+      for (int j = 0; j < KB; ++j) {
+        const int k = k0 + j;
+        sv[j] = k < cols ? sh[k * PS + e] : 0u;
+#pragma unroll
+        for (int i = 0; i < RPT; ++i) {
+          const int r = slot + kSmallSlots * i;
+          av[i][j] = (k < cols && r < rows) ? __ldg(A + ((size_t)r * ld + k) * D + e) : 0u;
+        }
       }
+#pragma unroll
+      for (int j = 0; j < KB; ++j)
+#pragma unroll
+        for (int i = 0; i < RPT; ++i) acc96_mad(acc[i], av[i][j], sv[j]);
     }
 #pragma unroll
     for (int i = 0; i < RPT; ++i) {
       const int r = slot + kSmallSlots * i;
-      if (r < rows) oh[r * PS + e] = acc96_reduce(acc[i], tw.f);
+      if (r < rows) oh[r * PS + e] = acc96_reduce(acc[i], f);
     }
   }
   __syncthreads();
 
-  if (tid < rows) {  // inverse transform of output row tid
-    uint32_t x[D];
+  // inverse transforms of the output rows (rows <= PPP: one pass)
+  {
+    const int r = pl < rows ? pl : 0;
+    uint32_t x[E];
 #pragma unroll
-    for (int cc = 0; cc < D / 4; ++cc) {
-      const uint4 v = reinterpret_cast<const uint4*>(oh + tid * PS)[cc];
-      x[brv(4 * cc + 0, LOGD)] = v.x;
-      x[brv(4 * cc + 1, LOGD)] = v.y;
-      x[brv(4 * cc + 2, LOGD)] = v.z;
-      x[brv(4 * cc + 3, LOGD)] = v.w;
+    for (int e = 0; e < E; ++e) {
+      const int i = 4 * T * (e >> 2) + (e & 3);
+      x[e] = oh[r * PS + (brv(i, LOGD) | bt_t)];
     }
-    inv1_alone<D, 1>(x, tw, c);
-    uint4* dst = reinterpret_cast<uint4*>(t + (b * rows + tid) * D);
+    invT_stages<D, T, 1>(x, tws, t, c);
+    if (pl < rows) {
+      uint4* dst = reinterpret_cast<uint4*>(t_out + (b * rows + pl) * D);
 #pragma unroll
-    for (int cc = 0; cc < D / 4; ++cc)
-      dst[cc] = make_uint4(x[4 * cc + 0], x[4 * cc + 1], x[4 * cc + 2], x[4 * cc + 3]);
+      for (int m = 0; m < E / 4; ++m)
+        dst[T * m + t] = make_uint4(x[4 * m + 0], x[4 * m + 1], x[4 * m + 2], x[4 * m + 3]);
+    }
   }
 }
 
@@ -717,21 +712,22 @@ int launch_commit_small(const grid_gpu_plan* p, const uint32_t* A_evals, size_t 
                         size_t cols, size_t ld, const uint32_t* s, size_t batch, uint32_t* t,
                         cudaStream_t st) {
   constexpr int D = 64;
-  static_assert(kSmallMaxRows <= D * kSmallSlots && kSmallMaxCols <= D * kSmallSlots,
-                "one transform per thread");
+  constexpr int PS = D + 4 * kSmallT, TWN = 2 * D + 2;
+  static_assert(kSmallMaxRows <= D * kSmallSlots / kSmallT, "one inverse pass");
   static_assert(kSmallMaxRows == 4 * kSmallSlots, "rows per thread: 1, 2 or 4");
   if (!commit_small_fits(p, rows, cols, batch)) return GRID_ERR_INVALID_PARAMETERS;
-  const size_t smem = (cols + rows) * (D + 4) * sizeof(uint32_t);
+  const size_t head = (2 * TWN + 4) * sizeof(uint32_t);  // twiddles
+  const size_t smem = head + (cols + rows) * PS * sizeof(uint32_t);
   // the shared-memory limit is set once per device: set it for the largest shape
-  constexpr size_t kSmemMax = (size_t)(kSmallMaxCols + kSmallMaxRows) * (D + 4) * sizeof(uint32_t);
-  const Tw1<D> tw = make_tw1<D>(p);
+  constexpr size_t kSmemMax =
+      (2 * TWN + 4) * sizeof(uint32_t) + (size_t)(kSmallMaxCols + kSmallMaxRows) * PS * 4;
   // rows per thread: 1, 2 or 4
   auto run = [&](auto kernel, int* cache) -> int {
     int bps = 0;
     const int rc = prepare_kernel(kernel, kSmemMax, D * kSmallSlots, p->device, cache, &bps);
     if (rc) return rc;
     kernel<<<(unsigned)batch, D * kSmallSlots, smem, st>>>(A_evals, (int)rows, (int)cols, (int)ld,
-                                                           s, t, tw);
+                                                           s, t, p->d_tw, p->f);
     return cuda_status(cudaGetLastError());
   };
   static int cache1[kMaxDevices] = {}, cache2[kMaxDevices] = {}, cache4[kMaxDevices] = {};
