@@ -1,0 +1,178 @@
+"""CPU models of two kernel index mappings, checked before the kernels ran on a GPU:
+
+* the element placement of the T-threads-per-polynomial transform stages
+  (`fwdT_stages` / `invT_stages` in lattica_b200/csrc/ntt.cu) at d = 64,
+  T = 8, as the one-launch commitment uses them, against the
+  one-thread-per-polynomial stages (`fwd1_stages` / `inv1_stages`);
+* the 4 x 4 byte transpose across a lane quad in the JL projection kernel
+  that writes the int8 entries (`jl_tc_kernel<true, true>` in jl.cu).
+
+The models restate the kernels' index arithmetic with exact arithmetic mod q
+and arbitrary twiddle values, so they check data movement, not the field."""
+import random
+
+Q = 4294966657
+
+
+def _brv(x, bits):
+    return int(format(x, f"0{bits}b")[::-1], 2) if bits else 0
+
+
+def _log2(x):
+    return x.bit_length() - 1
+
+
+def _one_thread_forward(inp, fw, d):
+    x = list(inp)
+    ln = d // 2
+    while ln >= 1:
+        for g in range(d // (2 * ln)):
+            k = d // (2 * ln) + g
+            for j in range(g * 2 * ln, g * 2 * ln + ln):
+                u, v = x[j], x[j + ln]
+                t = fw[k] * v % Q
+                x[j], x[j + ln] = (u + t) % Q, (u - t) % Q
+        ln //= 2
+    return {s: x[_brv(s, _log2(d))] for s in range(d)}  # slot -> value
+
+
+def _threads_forward(inp, fw, d, T):
+    E, logd = d // T, _log2(d)
+    X = [[inp[4 * (T * m + t) + s] for m in range(E // 4) for s in range(4)] for t in range(T)]
+    ln = d // 2
+    while ln >= 1:
+        l2 = _log2(2 * ln)
+        if ln >= 4 * T:
+            step = ln // T
+            for t in range(T):
+                for e in range(E):
+                    if e & step == 0:
+                        k = d // (2 * ln) + ((4 * T * (e >> 2)) >> l2)
+                        u, v = X[t][e], X[t][e + step]
+                        w = fw[k] * v % Q
+                        X[t][e], X[t][e + step] = (u + w) % Q, (u - w) % Q
+        elif ln >= 4:
+            M = ln // 4
+
+            def mine(t, e):
+                k = d // (2 * ln) + ((4 * T * (e >> 2) + 4 * t) >> l2)
+                return fw[k] * X[t][e] % Q if t & M else X[t][e]
+            X = [[(mine(t ^ M, e) - mine(t, e)) % Q if t & M else (mine(t, e) + mine(t ^ M, e)) % Q
+                  for e in range(E)] for t in range(T)]
+        else:
+            for t in range(T):
+                for e in range(E):
+                    if e & ln == 0:
+                        k = d // (2 * ln) + ((4 * T * (e >> 2) + 4 * t + (e & 3)) >> l2)
+                        u, v = X[t][e], X[t][e + ln]
+                        w = fw[k] * v % Q
+                        X[t][e], X[t][e + ln] = (u + w) % Q, (u - w) % Q
+        ln //= 2
+    out = {}
+    for t in range(T):
+        for e in range(E):
+            i = 4 * T * (e >> 2) + (e & 3)
+            out[_brv(i, logd) | _brv(4 * t, logd)] = X[t][e]
+    return out
+
+
+def _one_thread_inverse(slots, iw, ninv, iw1n, d):
+    x = [0] * d
+    for s in range(d):
+        x[_brv(s, _log2(d))] = slots[s]
+    ln = 1
+    while ln <= d // 2:
+        if ln == d // 2:
+            for j in range(ln):
+                u, v = x[j], x[j + ln]
+                x[j], x[j + ln] = (u + v) * ninv % Q, (u - v) * iw1n % Q
+        else:
+            for g in range(d // (2 * ln)):
+                k = d // (2 * ln) + g
+                for j in range(g * 2 * ln, g * 2 * ln + ln):
+                    u, v = x[j], x[j + ln]
+                    x[j], x[j + ln] = (u + v) % Q, (u - v) * iw[k] % Q
+        ln *= 2
+    return x
+
+
+def _threads_inverse(slots, iw, ninv, iw1n, d, T):
+    E, logd = d // T, _log2(d)
+    X = [[slots[_brv(4 * T * (e >> 2) + (e & 3), logd) | _brv(4 * t, logd)] for e in range(E)]
+         for t in range(T)]
+    ln = 1
+    while ln <= d // 2:
+        l2 = _log2(2 * ln)
+        if ln == d // 2:
+            step = ln // T
+            for t in range(T):
+                for e in range(E):
+                    if e & step == 0:
+                        u, v = X[t][e], X[t][e + step]
+                        X[t][e], X[t][e + step] = (u + v) * ninv % Q, (u - v) * iw1n % Q
+        elif ln >= 4 * T:
+            step = ln // T
+            for t in range(T):
+                for e in range(E):
+                    if e & step == 0:
+                        k = d // (2 * ln) + ((4 * T * (e >> 2)) >> l2)
+                        u, v = X[t][e], X[t][e + step]
+                        X[t][e], X[t][e + step] = (u + v) % Q, (u - v) * iw[k] % Q
+        elif ln >= 4:
+            M = ln // 4
+            new = [row[:] for row in X]
+            for t in range(T):
+                for e in range(E):
+                    k = d // (2 * ln) + ((4 * T * (e >> 2) + 4 * t) >> l2)
+                    other = X[t ^ M][e]
+                    s = (other - X[t][e]) % Q if t & M else (X[t][e] + other) % Q
+                    new[t][e] = s * iw[k] % Q if t & M else s
+            X = new
+        else:
+            for t in range(T):
+                for e in range(E):
+                    if e & ln == 0:
+                        k = d // (2 * ln) + ((4 * T * (e >> 2) + 4 * t + (e & 3)) >> l2)
+                        u, v = X[t][e], X[t][e + ln]
+                        X[t][e], X[t][e + ln] = (u + v) % Q, (u - v) * iw[k] % Q
+        ln *= 2
+    out = [0] * d
+    for t in range(T):
+        for m in range(E // 4):
+            for s in range(4):
+                out[4 * (T * m + t) + s] = X[t][4 * m + s]
+    return out
+
+
+def test_eight_thread_transform_places_every_value_like_one_thread():
+    rng = random.Random(3)
+    for d, T in ((64, 8), (64, 4), (128, 2), (256, 4)):
+        for _ in range(4):
+            fw = [rng.randrange(Q) for _ in range(d)]
+            iw = [rng.randrange(Q) for _ in range(d)]
+            ninv, iw1n = rng.randrange(Q), rng.randrange(Q)
+            inp = [rng.randrange(Q) for _ in range(d)]
+            assert _threads_forward(inp, fw, d, T) == _one_thread_forward(inp, fw, d), (d, T)
+            slots = [rng.randrange(Q) for _ in range(d)]
+            assert (_threads_inverse(slots, iw, ninv, iw1n, d, T) ==
+                    _one_thread_inverse(slots, iw, ninv, iw1n, d)), (d, T)
+
+
+def _byte_perm(x, y, s):
+    b = [(x >> (8 * i)) & 0xFF for i in range(4)] + [(y >> (8 * i)) & 0xFF for i in range(4)]
+    return sum(b[(s >> (4 * i)) & 7] << (8 * i) for i in range(4))
+
+
+def test_lane_quad_byte_transpose_of_jl_entries():
+    """Lane u of a quad holds rows 4b..4b+3 of polynomial u as M' = M + 1 bytes;
+    after the two exchanges lane r holds row 4b + r of polynomials 0..3 as int8 M."""
+    rng = random.Random(5)
+    for _ in range(500):
+        M = [[rng.randint(0, 2) for _ in range(4)] for _ in range(4)]  # [poly u][row r] = M'
+        words = [sum(M[u][r] << (8 * r) for r in range(4)) for u in range(4)]
+        m = [((w + 0x7F7F7F7F) & 0xFFFFFFFF) ^ 0x80808080 for w in words]
+        a = [_byte_perm(m[u], m[u ^ 1], 0x3715 if u & 1 else 0x6240) for u in range(4)]
+        o = [_byte_perm(a[u], a[u ^ 2], 0x3276 if u & 2 else 0x5410) for u in range(4)]
+        for r in range(4):
+            for u in range(4):
+                assert (o[r] >> (8 * u)) & 0xFF == (M[u][r] - 1) & 0xFF
