@@ -52,3 +52,22 @@ def test_queued_commitments_group_into_contiguous_runs():
     assert sorted(i for run in runs for i in run) == list(range(len(reqs)))
     # a larger gap joins everything into one launch
     assert len(RingServer._runs(reqs, gap=1 << 20)) == 1
+
+
+def test_uneven_batch_instances_match_the_workload():
+    """Config 3's instances: n log-uniform in [64, 8192] (mean ~1675), rank
+    uniform over {8, 16, 32}, witness and output offsets packed in order."""
+    import math
+    from lattica_b200.batch import sample_uneven_instances
+    items, s_polys, t_polys = sample_uneven_instances(4096, 7)
+    assert len(items) == 4096
+    ns = np.array([it[2] for it in items])
+    ms = np.array([(8, 16, 32)[it[3]] for it in items])
+    assert ns.min() >= 64 and ns.max() <= 8192
+    assert abs(ns.mean() - (8192 - 64) / math.log(8192 / 64)) / 1675 < 0.06
+    assert abs(np.log(ns).mean() - (math.log(64) + math.log(8192)) / 2) < 0.1
+    assert all(abs((ms == m).mean() - 1 / 3) < 0.03 for m in (8, 16, 32))
+    so = np.cumsum([0] + ns.tolist()[:-1])
+    to = np.cumsum([0] + ms.tolist()[:-1])
+    assert [it[0] for it in items] == so.tolist() and [it[1] for it in items] == to.tolist()
+    assert s_polys == ns.sum() and t_polys == ms.sum()
