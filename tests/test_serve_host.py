@@ -1,6 +1,7 @@
-"""Host-side logic of the request server, on CPU: the open-loop request
-stream (mix, arrival rate, witness offsets, determinism) and the grouping of
-queued commitments into contiguous runs for one batched launch."""
+"""Host-side logic of the batching and serving layers, on CPU: the open-loop
+request stream (mix, arrival rate, witness offsets, determinism), the
+grouping of queued commitments into contiguous runs for one batched launch,
+and the uneven-batch instance sampler."""
 import numpy as np
 import pytest
 
