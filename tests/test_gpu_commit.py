@@ -203,7 +203,7 @@ def test_prover_round_matches_oracle(cuda, oracle):
     """Fused round (commit + limbs, Gram + limbs, JL) on a small LaBRADOR witness."""
     import torch
     from lattica_b200 import TwistedNttPlan
-    from lattica_b200.labrador import CommitKey, prover_round_dev
+    from lattica_b200.labrador import CommitKey, prover_round_dev, verify_norm
     q, d, r, n, kappa = Q, 64, 6, 64, 4  # n % 32 == 0: entries from the projection kernel
     plan = TwistedNttPlan(q, d)
     P = oracle.Plan(q, d)
@@ -225,6 +225,20 @@ def test_prover_round_matches_oracle(cuda, oracle):
     p, flat = oracle.jl_project(F, seed, 256, S.reshape(r, n * d), r, n * d, d)
     assert np.array_equal(_host(out.p), p)
     assert np.array_equal(out.jl_flat.cpu().numpy(), flat)
+    # the checks verify_step applies to these outputs, on the GPU's own words:
+    # limbs reconstruct to t = A s and to g (reconstruct_from_limbs,
+    # main_protocol/mod.rs:331-359), and p passes the JL norm gate (jl.rs:533-547)
+    # for a bound above the witness norm (E ||p||^2 = 128 ||s||^2) and fails below it
+    tl, gl = _host(out.t_limbs), _host(out.g_limbs)
+    for i in range(r * kappa):
+        rec = oracle.reconstruct_from_limbs(F, d, tl[i * 4:(i + 1) * 4].reshape(-1), 256)
+        assert np.array_equal(rec, t.reshape(-1, d)[i])
+    for i in range(0, g.reshape(-1, d).shape[0], 97):
+        rec = oracle.reconstruct_from_limbs(F, d, gl[i * 4:(i + 1) * 4].reshape(-1), 256)
+        assert np.array_equal(rec, g.reshape(-1, d)[i])
+    s_norm = float(np.sqrt(np.sum(coeffs.astype(np.float64) ** 2)))
+    assert verify_norm(_host(out.p), q, 1.5 * s_norm)
+    assert not verify_norm(_host(out.p), q, 0.5 * s_norm)
     plan.check_device()
 
 
