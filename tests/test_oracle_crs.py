@@ -1,8 +1,8 @@
 """Two oracle paths against independent Python restatements of the published
 algorithms they follow. The JL projection and its int8 entries
-(labrador/src/jl.rs). The seeded commitment-key expansion: ChaCha20Rng(seed) (the RFC 8439
-block function with a 64-bit block counter in words 12-13 and stream 0 in
-words 14-15; rand_core's block RNG reads each u64 as two consecutive
+(labrador/src/jl.rs). The seeded commitment-key expansion: ChaCha20Rng(seed)
+(the RFC 8439 block function with a 64-bit block counter in words 12-13 and
+stream 0 in words 14-15; rand_core's block RNG reads each u64 as two consecutive
 little-endian words, low word first) and PrimeField::rand's u64 rejection
 (prime.rs:730-743: accept s <= u64::MAX - ((u64::MAX % q + 1) % q), value s % q).
 A lowered acceptance threshold makes rejections frequent."""
