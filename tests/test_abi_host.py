@@ -114,3 +114,13 @@ def test_plan_create_without_device_reports_no_device():
     with pytest.raises(GridGpuError) as ei:
         TwistedNttPlan(Q, 64)
     assert ei.value.name == "NoDevice"
+
+
+def test_missing_library_fails_loudly(monkeypatch, tmp_path):
+    """Without the built library every entry point refuses: there is no CPU fallback."""
+    import pytest
+    from lattica_b200 import _lib as L
+    monkeypatch.setattr(L, "_lib", None)
+    monkeypatch.setattr(L, "LIB_PATH", str(tmp_path / "libgridgpu.so"))
+    with pytest.raises(ImportError, match="no CPU fallback"):
+        L.load()
