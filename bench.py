@@ -138,7 +138,8 @@ def replica_throughput(units_per_rank: int, world: int, seconds_max: float) -> f
 
 
 def run_reference(args, rank, world):
-    """CPU restatement of the reference path on this host's cores."""
+    """CPU restatement of the reference path (the AVX2 port of its x86 NTT
+    kernels, oracle/oracle_avx2.c) on this host's cores."""
     if rank != 0:
         return
     from oracle import oracle as O
@@ -150,11 +151,11 @@ def run_reference(args, rank, world):
     a = rng.integers(0, q, (sample, d), dtype=np.uint64).astype(np.uint32)
     b = rng.integers(0, q, (sample, d), dtype=np.uint64).astype(np.uint32)
     for _ in range(max(1, args.warmup)):
-        P.ntt_mul_inverse(a[:1024], b[:1024], threads=threads)
+        P.ntt_mul_inverse(a[:1024], b[:1024], threads=threads, avx2=True)
     times = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        P.ntt_mul_inverse(a, b, threads=threads)
+        P.ntt_mul_inverse(a, b, threads=threads, avx2=True)
         times.append(time.perf_counter() - t0)
     per_step = sum(times) / len(times)
     value = sample / per_step
@@ -166,7 +167,8 @@ def run_reference(args, rank, world):
         "config": {"workload": f"{args.workload}: q={q}, d={d}, {n_full} polys (sampled)",
                    "sample_polys": sample},
         "cpu_baseline": {"value": value, "unit": "polys/s", "cores": threads, "kind": "port",
-                         "sample": f"{sample} polys of the {n_full}-poly workload per step",
+                         "sample": f"{sample} polys of the {n_full}-poly workload per step "
+                                   "(AVX2 restatement of the reference's x86 path)",
                          "host": host_cpu()},
         "e2e": {"value": value, "unit": "polys/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
@@ -189,22 +191,24 @@ def host_cpu():
 
 
 def cpu_baseline(q, d, n_full):
-    """Single-thread oracle port on a bounded sample (the reference CPU path is single-threaded)."""
+    """Single-thread AVX2 port of the reference's x86 path on a bounded sample
+    (the reference CPU path is single-threaded)."""
     from oracle import oracle as O
     P = O.Plan(q, d)
     rng = np.random.default_rng(2)
     sample = 1 << 14
     a = rng.integers(0, q, (sample, d), dtype=np.uint64).astype(np.uint32)
     b = rng.integers(0, q, (sample, d), dtype=np.uint64).astype(np.uint32)
-    P.ntt_mul_inverse(a[:256], b[:256])
+    P.ntt_mul_inverse(a[:256], b[:256], avx2=True)
     reps, elapsed = 0, 0.0
     while elapsed < 10.0 and reps < 64:
         t0 = time.perf_counter()
-        P.ntt_mul_inverse(a, b)
+        P.ntt_mul_inverse(a, b, avx2=True)
         elapsed += time.perf_counter() - t0
         reps += 1
     return {"value": sample * reps / elapsed, "unit": "polys/s", "cores": 1, "kind": "port",
-            "sample": f"{reps} x {sample} polys of the {n_full}-poly workload, 1 thread",
+            "sample": f"{reps} x {sample} polys of the {n_full}-poly workload, 1 thread "
+                      "(AVX2 restatement of the reference's x86 path)",
             "host": host_cpu()}
 
 

@@ -1,6 +1,7 @@
 """Build recipe for the CPU oracle (test infrastructure).
 
-Compiles oracle/oracle.c into oracle/_build/liboracle.so with gcc. The
+Compiles oracle/oracle.c and oracle/oracle_avx2.c into oracle/_build/liboracle.so
+with gcc. The
 reference itself is Rust and cannot be compiled here (no cargo/rustc), so
 there is no oracle/_ref build; the oracle is the C restatement only.
 """
@@ -13,7 +14,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT_DIR = os.path.join(HERE, "_build")
 LIB = os.path.join(OUT_DIR, "liboracle.so")
-SOURCES = [os.path.join(HERE, "oracle.c")]
+SOURCES = [os.path.join(HERE, "oracle.c"), os.path.join(HERE, "oracle_avx2.c")]
 
 
 def build(force: bool = False) -> str:

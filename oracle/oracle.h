@@ -83,6 +83,12 @@ void orc_ntt_mul_inverse(const orc_plan *p, const uint32_t *a, const uint32_t *b
 /* Same, split over `threads` OpenMP threads (independent polys). */
 void orc_ntt_mul_inverse_mt(const orc_plan *p, const uint32_t *a, const uint32_t *b_evals,
                             uint32_t *out, size_t count, int threads);
+/* The same product through the AVX2 restatement of the reference's x86 path
+ * (oracle_avx2.c): identical words, for the timed CPU baseline. */
+void orc_ntt_mul_inverse_avx2(const orc_plan *p, const uint32_t *a, const uint32_t *b_evals,
+                              uint32_t *out, size_t count);
+void orc_ntt_mul_inverse_avx2_mt(const orc_plan *p, const uint32_t *a, const uint32_t *b_evals,
+                                 uint32_t *out, size_t count, int threads);
 /* Negacyclic product via twisted NTT (poly/ntt.rs:110-126). */
 void orc_poly_mul_ntt(const orc_plan *p, const uint32_t *a, const uint32_t *b, uint32_t *out);
 /* Schoolbook negacyclic product (poly/ring.rs:88-105). */

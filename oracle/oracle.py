@@ -64,6 +64,9 @@ def lib():
             "orc_twisted_inverse": (None, [pp, _u32p, C.c_size_t]),
             "orc_ntt_mul_inverse": (None, [pp, _u32p, _u32p, _u32p, C.c_size_t]),
             "orc_ntt_mul_inverse_mt": (None, [pp, _u32p, _u32p, _u32p, C.c_size_t, C.c_int]),
+            "orc_ntt_mul_inverse_avx2": (None, [pp, _u32p, _u32p, _u32p, C.c_size_t]),
+            "orc_ntt_mul_inverse_avx2_mt": (None, [pp, _u32p, _u32p, _u32p, C.c_size_t,
+                                                   C.c_int]),
             "orc_poly_mul_ntt": (None, [pp, _u32p, _u32p, _u32p]),
             "orc_naive_negacyclic": (None, [fp, C.c_uint32, _u32p, _u32p, _u32p]),
             "orc_pointwise_mul": (None, [fp, _u32p, _u32p, C.c_size_t]),
@@ -197,16 +200,20 @@ class Plan:
         lib().orc_ntt_inverse(self._ref(), p)
         return a
 
-    def ntt_mul_inverse(self, a, b, threads: int = 1):
+    def ntt_mul_inverse(self, a, b, threads: int = 1, avx2: bool = False):
+        """INTT(NTT(a) * b) per polynomial; avx2 runs the AVX2 restatement of
+        the reference's x86 path (same words)."""
         a, pa = _u32(a)
         b, pb = _u32(b)
         out = np.empty_like(a)
         cnt = a.size // self.n
+        po = out.ctypes.data_as(_u32p)
         if threads == 1:
-            lib().orc_ntt_mul_inverse(self._ref(), pa, pb, out.ctypes.data_as(_u32p), cnt)
+            (lib().orc_ntt_mul_inverse_avx2 if avx2 else lib().orc_ntt_mul_inverse)(
+                self._ref(), pa, pb, po, cnt)
         else:
-            lib().orc_ntt_mul_inverse_mt(self._ref(), pa, pb, out.ctypes.data_as(_u32p), cnt,
-                                         threads)
+            (lib().orc_ntt_mul_inverse_avx2_mt if avx2 else lib().orc_ntt_mul_inverse_mt)(
+                self._ref(), pa, pb, po, cnt, threads)
         return out
 
     def poly_mul(self, a, b):
