@@ -322,22 +322,27 @@ def measure_commit_plain(dev, reps=50):
         if i >= 3:
             e2e.append((time.perf_counter() - t0) * 1e3)
     med_b, med_p, med_e = statistics.median(tb), statistics.median(tp), statistics.median(e2e)
-    # CPU beside it: the oracle's prepared commit path (NTT-domain A cached, like
-    # linear.rs:717-742) on the same inputs, one thread and all host cores
+    # CPU beside it: the prepared commit path with A_hat cached (linear.rs:717-742),
+    # through the AVX2 restatement of the reference's x86 kernels, on the same
+    # inputs, one thread and all host cores
     from oracle import oracle as O
     P = O.Plan(q, d)
+    a_hat = P.forward(np.ascontiguousarray(A).reshape(rows * cols, d)).reshape(-1)
     cpu = {}
     for label, threads in (("1t", 1), ("all", os.cpu_count() or 1)):
-        want = P.matvec(A, rows, cols, s_host, batch, threads=threads)  # warm
+        want = P.matvec(a_hat, rows, cols, s_host, batch, a_is_eval=True, threads=threads,
+                        avx2=True)  # warm
         t0 = time.perf_counter()
         for _ in range(3):
-            P.matvec(A, rows, cols, s_host, batch, threads=threads)
+            P.matvec(a_hat, rows, cols, s_host, batch, a_is_eval=True, threads=threads,
+                     avx2=True)
         cpu[label] = batch * 3 / (time.perf_counter() - t0)
     assert np.array_equal(t.cpu().numpy().view(np.uint32).reshape(-1), want), "GPU != oracle"
     return {"workload": "plain Ajtai commit: A 8x64 from a ChaCha20 seed, d=64, 64 ternary "
                         "witnesses per batch",
             "cpu_oracle_commits_per_s": {"threads_1": cpu["1t"], "threads_all": cpu["all"],
-                                         "cores": os.cpu_count() or 1},
+                                         "cores": os.cpu_count() or 1,
+                                         "kind": "AVX2 port, A_hat cached"},
             "commits_per_s": batch / (med_b / 1e3), "batch_ms_p50": med_b,
             "commits_per_s_steady": batch / (steady_ms / 1e3), "batch_ms_steady": steady_ms,
             "commits_per_s_graph": batch / (graph_ms / 1e3) if graph_ms else None,

@@ -89,6 +89,9 @@ void orc_ntt_mul_inverse_avx2(const orc_plan *p, const uint32_t *a, const uint32
                               uint32_t *out, size_t count);
 void orc_ntt_mul_inverse_avx2_mt(const orc_plan *p, const uint32_t *a, const uint32_t *b_evals,
                                  uint32_t *out, size_t count, int threads);
+/* The prepared commitment through the same AVX2 pieces (matvec's words). */
+int orc_matvec_avx2(const orc_plan *p, const uint32_t *A, size_t rows, size_t cols,
+                    int a_is_eval, const uint32_t *s, size_t batch, uint32_t *t, int threads);
 /* Negacyclic product via twisted NTT (poly/ntt.rs:110-126). */
 void orc_poly_mul_ntt(const orc_plan *p, const uint32_t *a, const uint32_t *b, uint32_t *out);
 /* Schoolbook negacyclic product (poly/ring.rs:88-105). */

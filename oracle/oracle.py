@@ -65,6 +65,8 @@ def lib():
             "orc_ntt_mul_inverse": (None, [pp, _u32p, _u32p, _u32p, C.c_size_t]),
             "orc_ntt_mul_inverse_mt": (None, [pp, _u32p, _u32p, _u32p, C.c_size_t, C.c_int]),
             "orc_ntt_mul_inverse_avx2": (None, [pp, _u32p, _u32p, _u32p, C.c_size_t]),
+            "orc_matvec_avx2": (C.c_int, [pp, _u32p, C.c_size_t, C.c_size_t, C.c_int, _u32p,
+                                          C.c_size_t, _u32p, C.c_int]),
             "orc_ntt_mul_inverse_avx2_mt": (None, [pp, _u32p, _u32p, _u32p, C.c_size_t,
                                                    C.c_int]),
             "orc_poly_mul_ntt": (None, [pp, _u32p, _u32p, _u32p]),
@@ -230,11 +232,14 @@ class Plan:
         lib().orc_naive_negacyclic(C.byref(self.s.f), self.n, pa, pb, out.ctypes.data_as(_u32p))
         return out
 
-    def matvec(self, A, rows, cols, s, batch, a_is_eval=False, threads=1):
+    def matvec(self, A, rows, cols, s, batch, a_is_eval=False, threads=1, avx2=False):
         A, pA = _u32(A)
         s, ps = _u32(s)
         t = np.empty(batch * rows * self.n, dtype=np.uint32)
-        if threads == 1:
+        if avx2:  # the AVX2 restatement of the reference's x86 path, same words
+            st = lib().orc_matvec_avx2(self._ref(), pA, rows, cols, int(a_is_eval), ps, batch,
+                                       t.ctypes.data_as(_u32p), threads)
+        elif threads == 1:
             st = lib().orc_matvec(self._ref(), pA, rows, cols, int(a_is_eval), ps, batch,
                                   t.ctypes.data_as(_u32p))
         else:

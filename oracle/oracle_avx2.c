@@ -14,6 +14,7 @@
  * on 64-bit half-lanes (even lanes, then the odd lanes shifted down), so every
  * output word equals the scalar oracle's (checked in tests/test_oracle_avx2.py). */
 #include <immintrin.h>
+#include <stdlib.h>
 #include <string.h>
 #ifdef _OPENMP
 #include <omp.h>
@@ -184,4 +185,68 @@ void orc_ntt_mul_inverse_avx2_mt(const orc_plan *p, const uint32_t *a, const uin
     (void)threads;
     orc_ntt_mul_inverse_avx2(p, a, b_evals, out, count);
 #endif
+}
+
+/* The prepared commitment t_b[row] = INTT(sum_k A_hat[row][k] * s_hat_b[k]),
+ * the reference's mul_matrix_vector_trusted over cached A_hat evaluations
+ * (commit/src/linear.rs:717-742, TwistedNttPoly::dot_product,
+ * poly/twisted_ntt.rs:378-408, whose pointwise products and additions run
+ * eight lanes at a time in the x86 backend): per witness, the twisted
+ * forward transforms of its columns, one eight-lane multiply-accumulate pass
+ * per row, the twisted inverse. a_is_eval = 0 transforms A first. */
+int orc_matvec_avx2(const orc_plan *p, const uint32_t *A, size_t rows, size_t cols,
+                    int a_is_eval, const uint32_t *s, size_t batch, uint32_t *t, int threads) {
+    const vfield v = vfield_of(&p->f);
+    const orc_field *f = &p->f;
+    const uint32_t n = p->n;
+    uint32_t *own = NULL;
+    const uint32_t *ahat = A;
+    if (!a_is_eval) {
+        own = (uint32_t *)malloc(sizeof(uint32_t) * rows * cols * n);
+        if (!own) return ORC_ERR_OOM;
+        memcpy(own, A, sizeof(uint32_t) * rows * cols * n);
+        for (size_t i = 0; i < rows * cols; i++) {
+            pointwise(f, &v, own + i * n, p->twists, n);
+            forward(p, &v, own + i * n);
+        }
+        ahat = own;
+    }
+    int err = 0;
+    const long long nb = (long long)batch;
+#ifdef _OPENMP
+    if (threads < 1) threads = omp_get_max_threads();
+#pragma omp parallel for num_threads(threads) schedule(dynamic)
+#endif
+    for (long long b = 0; b < nb; b++) {
+        uint32_t *shat = (uint32_t *)malloc(sizeof(uint32_t) * cols * n);
+        if (!shat) { err = 1; continue; }
+        memcpy(shat, s + (size_t)b * cols * n, sizeof(uint32_t) * cols * n);
+        for (size_t k = 0; k < cols; k++) {
+            pointwise(f, &v, shat + k * n, p->twists, n);
+            forward(p, &v, shat + k * n);
+        }
+        for (size_t row = 0; row < rows; row++) {
+            uint32_t *out = t + ((size_t)b * rows + row) * n;
+            const uint32_t *arow = ahat + row * cols * n;
+            uint32_t e = 0;
+            for (; e + 8 <= n; e += 8) {
+                __m256i acc = _mm256_setzero_si256();
+                for (size_t k = 0; k < cols; k++)
+                    acc = add8(&v, acc, mont8(&v, LD(arow + k * n + e), LD(shat + k * n + e)));
+                ST(out + e, acc);
+            }
+            for (; e < n; e++) {
+                uint32_t acc = 0;
+                for (size_t k = 0; k < cols; k++)
+                    acc = orc_add(f, acc, orc_mul(f, arow[k * n + e], shat[k * n + e]));
+                out[e] = acc;
+            }
+            inverse(p, &v, out);
+            pointwise(f, &v, out, p->untwists, n);
+        }
+        free(shat);
+    }
+    (void)threads;
+    free(own);
+    return err ? ORC_ERR_OOM : ORC_OK;
 }
