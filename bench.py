@@ -456,8 +456,10 @@ def measure_round(dev, reps=50):
     sample_uniform_polys(plan, seed, crs_polys, device=dev)
     times_crs = _events_ms(lambda: sample_uniform_polys(plan, seed, crs_polys, device=dev),
                            max(5, reps // 5), stream)
+    parity = check_round_parity(key, A, wit, seed, plan)
     return {"workload": "LaBRADOR round: r=64, n=2048, d=64, kappa=16, JL 256 rows, base 2^8 x4 limbs",
             "round_ms_p50": _pct(times, 50), "round_ms_p99": _pct(times, 99),
+            "parity": parity,
             "cpu_oracle_round_ms": cpu_round,
             "garbage_h_ms_p50": _pct(times_h, 50), "amortize_ms_p50": _pct(times_z, 50),
             "outer_u1_ms_p50": _pct(times_u1, 50), "outer_u2_ms_p50": _pct(times_u2, 50),
@@ -468,6 +470,39 @@ def measure_round(dev, reps=50):
             "round_with_jl_evals_ms_p50": _pct(times_ev_round, 50),
             "e2e_round_ms_p50": _pct(e2e, 50), "e2e_round_ms_p99": _pct(e2e, 99),
             "e2e_h2d_bytes": hw.numel() * 4, "e2e_d2h_bytes": d2h, "rounds": reps}
+
+
+def check_round_parity(key, A, wit, seed, plan):
+    """One round on the timed inputs, every output word compared with the
+    oracle at the round's own size (r = 64, n = 2048, kappa = 16): t limbs,
+    g, g limbs and the JL projection p. Raises on any difference."""
+    import torch
+    from lattica_b200.labrador import prover_round_dev
+    from oracle import oracle as O
+    r, n, d = (int(x) for x in wit.shape)
+    kappa = int(A.shape[0])
+    o = prover_round_dev(key, wit, 256, 4, 256, 4, seed, 256)
+    torch.cuda.synchronize()
+    got = {k: getattr(o, k).cpu().numpy().view(np.uint32).reshape(-1)
+           for k in ("t_limbs", "g", "g_limbs", "p")}
+    P = O.Plan(plan.q, d)
+    F = P.field
+    S = wit.cpu().numpy().view(np.uint32)
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    t = P.matvec(A.cpu().numpy().view(np.uint32), kappa, n, S, r, threads=threads)
+    g = P.gram(S, r, n, threads=threads)
+    p, _ = O.jl_project(F, seed, 256, S.reshape(r, n * d), r, n * d, d, want_flat=False,
+                        threads=threads)
+    want = {"t_limbs": O.decompose_polys(F, d, t, 256, 4), "g": g,
+            "g_limbs": O.decompose_polys(F, d, g, 256, 4), "p": p}
+    for k, w in want.items():
+        if not np.array_equal(got[k], w.reshape(-1)):
+            raise AssertionError(f"round {k}: {int(np.count_nonzero(got[k] != w.reshape(-1)))} "
+                                 "words differ from the oracle")
+    return {"checked": "every word of t_limbs, g, g_limbs, p vs the oracle",
+            "words": int(sum(v.size for v in got.values())),
+            "oracle_s": round(time.perf_counter() - t0, 2)}
 
 
 def measure_batch(dev, reps=10):
@@ -482,10 +517,11 @@ def measure_batch(dev, reps=10):
     q, d, ranks = Q64, 64, (8, 16, 32)
     plan = TwistedNttPlan(q, d)
     g = torch.Generator(device=dev).manual_seed(3)
-    mats = []
+    mats, mats_host = [], []
     for m in ranks:
         A = torch.randint(0, q, (m, 8192, d), dtype=torch.int64, device=dev, generator=g).to(torch.int32)
         mats.append(PreparedMatrix(plan, A, m, 8192))
+        mats_host.append(A.cpu().numpy().view(np.uint32))
         del A
     items, s_polys, t_polys = sample_uneven_instances(4096, 7)
     r1 = (1 << 32) % q
@@ -505,6 +541,23 @@ def measure_batch(dev, reps=10):
     stream = torch.cuda.current_stream(dev)
     tp = _events_ms(lambda: per_call_commit(plan, mats, items, s, t2), 3, stream)
     same = bool(torch.equal(t, t2))
+    if not same:
+        raise AssertionError("batched commits differ from the per-call path")
+    # 32 instances (the longest, the shortest and 30 spread over the batch)
+    # against the oracle
+    from oracle import oracle as O
+    P = O.Plan(q, d)
+    order = sorted(range(len(items)), key=lambda i: items[i][2])
+    pick = sorted(set([order[-1], order[0]] + order[:: max(1, len(order) // 30)][:30]))
+    for i in pick:
+        so, to, nn, m = items[i]
+        rows = ranks[m]
+        A_i = np.ascontiguousarray(mats_host[m][:, :nn, :])
+        sw = s[so:so + nn].cpu().numpy().view(np.uint32)
+        want = P.matvec(A_i, rows, nn, sw, 1).reshape(rows, d)
+        if not np.array_equal(t[to:to + rows].cpu().numpy().view(np.uint32), want):
+            raise AssertionError(f"batched commit of instance {i} (n={nn}, m={rows}) differs "
+                                 "from the oracle")
     n = len(items)
     macs = sum(ranks[m] * nn for _, _, nn, m in items) * d
     return {"workload": "uneven batched commits: 4096 instances, n log-uniform [64, 8192], "
@@ -515,6 +568,8 @@ def measure_batch(dev, reps=10):
             "per_call_ms_p50": statistics.median(tp),
             "speedup_vs_per_call": statistics.median(tp) / statistics.median(tb),
             "outputs_identical": same, "mod_macs": macs,
+            "parity": f"all outputs equal the per-call path; {len(pick)} instances "
+                      "(longest and shortest included) equal the oracle",
             "autotune": {k: v for k, v in tune.items() if k in ("k_split", "cached", "ms")},
             "schedule": batch.config()}
 
@@ -568,11 +623,66 @@ def measure_serve(dev, rates=(1000, 2000, 5000, 10000, 20000, 50000), seconds=0.
             for lam in rates:
                 res = run_load(srv, schedule(100 + lam, max(200, int(lam * seconds)), float(lam)))
                 out["rates"].setdefault(str(lam), {})[mode] = res
+        # capacity: the whole stream queued at once, so throughput is what the
+        # server sustains rather than the offered rate
+        with RingServer(plan, mats, key, pool, mode=mode) as srv:
+            run_load(srv, schedule(2, 200, 1000.0))
+            out.setdefault("saturated", {})[mode] = run_load(srv, schedule(55, 600, 1e9))
     best = {m: max(v[m]["commits_per_s"] for v in out["rates"].values())
             for m in ("continuous", "plain")}
     out["max_commits_per_s"] = best
     out["commits_per_s_ratio"] = best["continuous"] / best["plain"]
+    sat = out["saturated"]
+    out["saturated_req_per_s_ratio"] = sat["continuous"]["req_per_s"] / sat["plain"]["req_per_s"]
+    out["saturated_commits_per_s_ratio"] = (sat["continuous"]["commits_per_s"]
+                                            / sat["plain"]["commits_per_s"])
+    out["parity"] = check_serve_parity(plan, mats, key, pool, arena, pool_polys)
     return out
+
+
+def check_serve_parity(plan, mats, key, pool, arena, pool_polys, count=300, rate=20000.0):
+    """Every result of a mixed stream served continuously (batched, overlapped)
+    equals the same request served alone (the plain per-call path). Raises on
+    any difference."""
+    from lattica_b200.serve import RingServer, run_load, sample_requests
+    results = {}
+    for mode in ("continuous", "plain"):
+        sched = sample_requests(777, count, rate, commit_arena=arena, pool_polys=pool_polys)
+        with RingServer(plan, mats, key, pool, mode=mode) as srv:
+            run_load(srv, sched)
+        results[mode] = [(r.kind, r.future.result()) for _, r in sched]
+    kinds = {}
+    for (k, a), (_, b) in zip(results["continuous"], results["plain"]):
+        if len(a) != len(b) or not all(np.array_equal(x, y) for x, y in zip(a, b)):
+            raise AssertionError(f"a served {k} request differs from the same request alone")
+        kinds[k] = kinds.get(k, 0) + 1
+    return {"checked": f"{count} requests at {int(rate)} req/s: continuous == alone",
+            "by_kind": kinds}
+
+
+def measure_ntt256(dev, reps=20):
+    """The d = 256 sweep of the batched products: 2^20 polys at q' = 4294962689."""
+    import torch
+    from lattica_b200 import TwistedNttPlan, _lib
+    q, d, n = WORKLOADS["ntt256"]
+    plan = TwistedNttPlan(q, d)
+    lib = _lib.load()
+    g = torch.Generator(device=dev).manual_seed(256)
+    a = torch.randint(0, q, (n, d), dtype=torch.int64, device=dev, generator=g).to(torch.int32)
+    b = torch.randint(0, q, (n, d), dtype=torch.int64, device=dev, generator=g).to(torch.int32)
+    out = torch.empty_like(a)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        assert lib.grid_gpu_ntt_mul_inverse_dev(plan.handle, a.data_ptr(), b.data_ptr(),
+                                                out.data_ptr(), n, stream.cuda_stream) == 0
+
+    for _ in range(3):
+        step()
+    ms = statistics.median(_events_ms(step, reps, stream))
+    peak, _ = _peaks()
+    return {"polys_per_s": n / (ms / 1e3), "ms_p50": ms,
+            "frac": 3 * 4 * d * n / (ms / 1e3) / 1e9 / peak}
 
 
 def run_ours(args, rank, world, local_rank):
@@ -682,14 +792,65 @@ def run_ours(args, rank, world, local_rank):
         "gpu_launches": args.steps,
         "clocks": sampler.summary(),
     }
-    if args.secondary:
-        line["secondary"] = {"commit": measure_commit_plain(dev), "round": measure_round(dev),
-                             "batch": measure_batch(dev)}
-        if args.serve:
-            line["secondary"]["serve"] = measure_serve(dev)
     if world == 1:
         line["cpu_baseline"] = cpu_baseline(q, d, WORKLOADS[args.workload][2])
+    if args.secondary:
+        detail = {"commit": measure_commit_plain(dev), "round": measure_round(dev),
+                  "batch": measure_batch(dev), "ntt256": measure_ntt256(dev)}
+        if args.serve:
+            detail["serve"] = measure_serve(dev)
+        line["secondary"] = secondary_summary(detail)
+        path = os.environ.get("BENCH_DETAIL", os.path.join(ROOT, "gpurun_out",
+                                                           "bench_detail.json"))
+        try:
+            os.makedirs(os.path.dirname(path), exist_ok=True)
+            with open(path, "w") as fh:
+                json.dump(detail, fh, indent=1)
+            line["secondary"]["detail_file"] = os.path.relpath(path, ROOT)
+        except OSError as exc:
+            print(f"bench detail not written: {exc}", file=sys.stderr)
     print(json.dumps(line), flush=True)
+
+
+def secondary_summary(detail):
+    """The figures BASELINE's metric names, flat and short (the JSON line stays
+    a few KB): config 0 commits/s, the round's p50/p99, config 3 batched
+    commits/s, the served ratios, the d = 256 sweep; each checked in the run."""
+    def r(x, nd=3):
+        return None if x is None else round(float(x), nd)
+    c, rd, b, n2 = detail["commit"], detail["round"], detail["batch"], detail["ntt256"]
+    out = {
+        "round_ms_p50": r(rd["round_ms_p50"], 4), "round_ms_p99": r(rd["round_ms_p99"], 4),
+        "round_e2e_ms_p50": r(rd["e2e_round_ms_p50"]),
+        "round_parity": "bit-exact, every word at r=64 n=2048 kappa=16",
+        "round_cpu_oracle_ms_1t": r(rd["cpu_oracle_round_ms"]["threads_1"], 1),
+        "round_cpu_oracle_ms_all": r(rd["cpu_oracle_round_ms"]["threads_all"], 1),
+        "config0_commits_per_s": r(c["commits_per_s"], 0),
+        "config0_commits_per_s_graph": r(c["commits_per_s_graph"], 0),
+        "config0_per_call_commits_per_s": r(c["per_call_commits_per_s"], 0),
+        "config0_e2e_commits_per_s": r(c["e2e_commits_per_s"], 0),
+        "config0_cpu_commits_per_s_1t": r(c["cpu_oracle_commits_per_s"]["threads_1"], 0),
+        "config0_parity": "bit-exact vs oracle",
+        "config3_commits_per_s": r(b["batched_commits_per_s"], 0),
+        "config3_per_call_commits_per_s": r(b["per_call_commits_per_s"], 0),
+        "config3_ms_p50": r(b["batched_ms_p50"]),
+        "config3_parity": "all == per-call; 32 sampled == oracle",
+        "ntt256_polys_per_s": r(n2["polys_per_s"], 0), "ntt256_frac": r(n2["frac"]),
+        "host_cores": os.cpu_count() or 1,
+    }
+    sv = detail.get("serve")
+    if sv:
+        sat = sv["saturated"]
+        out.update({
+            "served_commits_per_s_ratio": r(sv["commits_per_s_ratio"]),
+            "served_req_per_s_ratio": r(sv["saturated_req_per_s_ratio"]),
+            "served_saturated_req_per_s": {m: sat[m]["req_per_s"] for m in sat},
+            "served_saturated_p99_ms": {m: sat[m]["p99_ms"] for m in sat},
+            "served_p99_ms_at_5k": {m: sv["rates"]["5000"][m]["p99_ms"]
+                                    for m in ("continuous", "plain")},
+            "served_parity": "continuous == alone, 300 mixed requests",
+        })
+    return out
 
 
 def main():

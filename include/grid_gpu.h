@@ -39,7 +39,7 @@ extern "C" {
 
 typedef enum grid_status {
   GRID_OK = 0,
-  /* NttError (algebra/src/arith/ntt.rs:386-395) */
+  /* NttError (algebra/src/arith/ntt.rs:40-50) */
   GRID_ERR_LENGTH_MISMATCH = 1,
   GRID_ERR_LENGTH_NOT_POW2 = 2,
   GRID_ERR_UNSUPPORTED_SIZE = 3,
@@ -88,7 +88,7 @@ uint32_t grid_gpu_max_degree(void);
 /* ---- plans: replace NttPlan::build / TwistedNttPlan::build ------------- */
 
 /* Mirrors TwistedNttPlan::build (algebra/src/poly/ntt.rs:139-154) over
- * NttPlan::build (algebra/src/arith/ntt.rs:469-500): validates q, then
+ * NttPlan::build (algebra/src/arith/ntt.rs:124-154): validates q, then
  * LengthNotPowerOfTwo, UnsupportedSize, UnsupportedTwist in that order. */
 int grid_gpu_plan_create(uint64_t q, uint64_t d, grid_gpu_plan** out);
 int grid_gpu_plan_destroy(grid_gpu_plan* plan);
@@ -104,6 +104,14 @@ int grid_gpu_plan_get_twiddles(const grid_gpu_plan* plan, uint32_t* zeta, uint32
 /* Reads and clears the plan's device error word (GRID_ERR_TIMEOUT if a
  * bounded device wait gave up since the last check). Synchronises `stream`. */
 int grid_gpu_plan_check(grid_gpu_plan* plan, void* stream);
+/* Test support for the failure path (no counterpart in the reference, whose
+ * CPU code has no device waits): one warp waits on an mbarrier that nothing
+ * arrives at, giving up after max_spins polls (1 .. 2^22) exactly as a stalled
+ * kernel's bounded wait does, which records a timeout in the plan's error
+ * word. The next grid_gpu_plan_check returns GRID_ERR_TIMEOUT and clears it;
+ * the plan stays usable. */
+int grid_gpu_selftest_wait_timeout_dev(const grid_gpu_plan* plan, uint32_t max_spins,
+                                       void* stream);
 
 /* ---- NTT: replace NTTRing::ntt_{forward,inverse}_with_plan for twisted plans
  *      (algebra/src/poly/ntt.rs:75-104, arith/prime.rs:617-637) ------------- */
@@ -124,6 +132,21 @@ int grid_gpu_poly_mul_dev(const grid_gpu_plan* plan, const uint32_t* a, const ui
 /* Ring::pointwise_mul_assign_slice (algebra/src/arith/prime.rs:433-447): dst *= rhs. */
 int grid_gpu_pointwise_mul_dev(const grid_gpu_plan* plan, uint32_t* dst, const uint32_t* rhs,
                                size_t nwords, void* stream);
+/* The other slice hooks of Ring for PrimeField (algebra/src/arith/prime.rs:433-491):
+ * add_assign_slice dst += src, sub_assign_slice dst -= src, scalar_mul_slice
+ * dst *= scalar, add_assign_scaled_slice dst += src * scalar, and dot_product
+ * (*out = sum lhs_i * rhs_i, one word in device memory). Canonical words;
+ * scalar >= q returns GRID_ERR_INVALID_PARAMETERS. */
+int grid_gpu_add_assign_dev(const grid_gpu_plan* plan, uint32_t* dst, const uint32_t* src,
+                            size_t nwords, void* stream);
+int grid_gpu_sub_assign_dev(const grid_gpu_plan* plan, uint32_t* dst, const uint32_t* src,
+                            size_t nwords, void* stream);
+int grid_gpu_scalar_mul_dev(const grid_gpu_plan* plan, uint32_t* dst, uint32_t scalar,
+                            size_t nwords, void* stream);
+int grid_gpu_add_assign_scaled_dev(const grid_gpu_plan* plan, uint32_t* dst, const uint32_t* src,
+                                   uint32_t scalar, size_t nwords, void* stream);
+int grid_gpu_dot_product_dev(const grid_gpu_plan* plan, const uint32_t* lhs, const uint32_t* rhs,
+                             size_t nwords, uint32_t* out, void* stream);
 
 int grid_gpu_ntt_forward(grid_gpu_plan* plan, uint32_t* polys, size_t npolys);
 int grid_gpu_ntt_inverse(grid_gpu_plan* plan, uint32_t* polys, size_t npolys);
@@ -327,7 +350,9 @@ int grid_gpu_batch_commit_oneshot_dev(grid_gpu_plan* plan, grid_gpu_matrix* cons
  * (grid_gpu_gram_workspace) return GRID_ERR_SCRATCH_LIMIT. The first call on a
  * device looks up the buffer's device address (cudaGetSymbolAddress); make that
  * first call before any stream capture. All calls share the buffer: calls
- * that overlap on the GPU race, so order them (for example on one stream). */
+ * that overlap on the GPU race, so order them (for example on one stream).
+ * The current device must be the plan's (else GRID_ERR_INVALID_PARAMETERS);
+ * the looked-up address does not survive cudaDeviceReset. */
 size_t grid_gpu_noalloc_scratch_bytes(void);
 int grid_gpu_gram_noalloc_dev(const grid_gpu_plan* plan, const uint32_t* S, size_t r, size_t n,
                               uint32_t* G, void* stream);

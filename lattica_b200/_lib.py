@@ -51,11 +51,17 @@ SIGNATURES = {
     "grid_gpu_plan_get_info": (C.c_int, [_vp, C.POINTER(PlanInfo)]),
     "grid_gpu_plan_get_twiddles": (C.c_int, [_vp, _vp, _vp]),
     "grid_gpu_plan_check": (C.c_int, [_vp, _vp]),
+    "grid_gpu_selftest_wait_timeout_dev": (C.c_int, [_vp, C.c_uint32, _vp]),
     "grid_gpu_ntt_forward_dev": (C.c_int, [_vp, _vp, C.c_size_t, _vp]),
     "grid_gpu_ntt_inverse_dev": (C.c_int, [_vp, _vp, C.c_size_t, _vp]),
     "grid_gpu_ntt_mul_inverse_dev": (C.c_int, [_vp, _vp, _vp, _vp, C.c_size_t, _vp]),
     "grid_gpu_poly_mul_dev": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_size_t, _vp]),
     "grid_gpu_pointwise_mul_dev": (C.c_int, [_vp, _vp, _vp, C.c_size_t, _vp]),
+    "grid_gpu_add_assign_dev": (C.c_int, [_vp, _vp, _vp, C.c_size_t, _vp]),
+    "grid_gpu_sub_assign_dev": (C.c_int, [_vp, _vp, _vp, C.c_size_t, _vp]),
+    "grid_gpu_scalar_mul_dev": (C.c_int, [_vp, _vp, C.c_uint32, C.c_size_t, _vp]),
+    "grid_gpu_add_assign_scaled_dev": (C.c_int, [_vp, _vp, _vp, C.c_uint32, C.c_size_t, _vp]),
+    "grid_gpu_dot_product_dev": (C.c_int, [_vp, _vp, _vp, C.c_size_t, _vp, _vp]),
     "grid_gpu_ntt_forward": (C.c_int, [_vp, _vp, C.c_size_t]),
     "grid_gpu_ntt_inverse": (C.c_int, [_vp, _vp, C.c_size_t]),
     "grid_gpu_ntt_mul_inverse": (C.c_int, [_vp, _vp, _vp, _vp, C.c_size_t]),

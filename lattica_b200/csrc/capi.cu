@@ -23,6 +23,10 @@ struct Carver {
   Carver(void* b, size_t c) : base(static_cast<char*>(b)), cap(c) {}
   template <typename T>
   T* take(size_t count) {
+    if (count > (cap + 1) / sizeof(T)) {  // also keeps count * sizeof(T) from wrapping
+      ok = false;
+      return nullptr;
+    }
     const size_t bytes = round_up(count * sizeof(T), 256);
     if (used + bytes > cap || !base) {
       ok = false;
@@ -59,6 +63,18 @@ size_t amortize_ws_bytes(const grid_gpu_plan* p, size_t r, size_t n) {
 bool dims_ok(size_t a, size_t b, size_t c) {
   // all kernels index rows/cols/K with int
   return a > 0 && b > 0 && c > 0 && a < (1u << 30) && b < (1u << 30) && c < (1u << 30);
+}
+
+// a * b * c words of 4 bytes stay far below SIZE_MAX (no wrap in any size sum).
+bool words_fit(size_t a, size_t b, size_t c) {
+  size_t x;
+  return !__builtin_mul_overflow(a, b, &x) && !__builtin_mul_overflow(x, c, &x) &&
+         x < (1ull << 56);
+}
+
+// r x n witness polys and the r x r products over them (Gram, garbage h, amortization).
+bool square_dims_ok(const grid_gpu_plan* p, size_t r, size_t n) {
+  return dims_ok(r, n, 1) && words_fit(r, n, p->d) && words_fit(r, r, p->d);
 }
 
 // t = A * s for `batch` vectors, into t (coefficients). ws from a Carver.
@@ -376,6 +392,7 @@ int grid_gpu_bdlop_commit(grid_gpu_matrix* A_mask, grid_gpu_matrix* A_msg, grid_
 
 int grid_gpu_gram_workspace(const grid_gpu_plan* p, size_t r, size_t n, size_t* bytes) {
   if (!p || !bytes) return GRID_ERR_NULL_POINTER;
+  if (!square_dims_ok(p, r, n)) return GRID_ERR_INVALID_PARAMETERS;
   *bytes = gram_ws_bytes(p, r, n);
   return GRID_OK;
 }
@@ -383,7 +400,7 @@ int grid_gpu_gram_workspace(const grid_gpu_plan* p, size_t r, size_t n, size_t* 
 int grid_gpu_gram_dev(const grid_gpu_plan* p, const uint32_t* S, size_t r, size_t n,
                       uint32_t* G, void* workspace, size_t workspace_bytes, void* stream) {
   if (!p || !S || !G) return GRID_ERR_NULL_POINTER;
-  if (!dims_ok(r, n, 1)) return GRID_ERR_INVALID_PARAMETERS;
+  if (!square_dims_ok(p, r, n)) return GRID_ERR_INVALID_PARAMETERS;
   if (!aligned16(S) || !aligned16(G) || !aligned16(workspace)) return GRID_ERR_MISALIGNED;
   cudaStream_t st = (cudaStream_t)stream;
   Carver cv(workspace, workspace_bytes);
@@ -400,7 +417,7 @@ int grid_gpu_gram_dev(const grid_gpu_plan* p, const uint32_t* S, size_t r, size_
 
 int grid_gpu_gram(grid_gpu_plan* p, const uint32_t* S, size_t r, size_t n, uint32_t* G) {
   if (!p || !S || !G) return GRID_ERR_NULL_POINTER;
-  if (!dims_ok(r, n, 1)) return GRID_ERR_INVALID_PARAMETERS;
+  if (!square_dims_ok(p, r, n)) return GRID_ERR_INVALID_PARAMETERS;
   std::lock_guard<std::mutex> lk(p->mu);
   const size_t s_bytes = r * n * p->d * 4, g_bytes = r * (r + 1) / 2 * p->d * 4;
   const size_t ws = gram_ws_bytes(p, r, n);
@@ -423,6 +440,7 @@ int grid_gpu_gram(grid_gpu_plan* p, const uint32_t* S, size_t r, size_t n, uint3
 
 int grid_gpu_garbage_h_workspace(const grid_gpu_plan* p, size_t r, size_t n, size_t* bytes) {
   if (!p || !bytes) return GRID_ERR_NULL_POINTER;
+  if (!square_dims_ok(p, r, n)) return GRID_ERR_INVALID_PARAMETERS;
   *bytes = garbage_h_ws_bytes(p, r, n);
   return GRID_OK;
 }
@@ -431,7 +449,7 @@ int grid_gpu_garbage_h_dev(const grid_gpu_plan* p, const uint32_t* S, const uint
                            size_t r, size_t n, uint32_t* H, void* workspace,
                            size_t workspace_bytes, void* stream) {
   if (!p || !S || !Phi || !H) return GRID_ERR_NULL_POINTER;
-  if (!dims_ok(r, n, 1)) return GRID_ERR_INVALID_PARAMETERS;
+  if (!square_dims_ok(p, r, n)) return GRID_ERR_INVALID_PARAMETERS;
   if (!aligned16(S) || !aligned16(Phi) || !aligned16(H) || !aligned16(workspace))
     return GRID_ERR_MISALIGNED;
   cudaStream_t st = (cudaStream_t)stream;
@@ -455,7 +473,7 @@ int grid_gpu_garbage_h_dev(const grid_gpu_plan* p, const uint32_t* S, const uint
 int grid_gpu_garbage_h(grid_gpu_plan* p, const uint32_t* S, const uint32_t* Phi, size_t r,
                        size_t n, uint32_t* H) {
   if (!p || !S || !Phi || !H) return GRID_ERR_NULL_POINTER;
-  if (!dims_ok(r, n, 1)) return GRID_ERR_INVALID_PARAMETERS;
+  if (!square_dims_ok(p, r, n)) return GRID_ERR_INVALID_PARAMETERS;
   std::lock_guard<std::mutex> lk(p->mu);
   const size_t s_bytes = r * n * p->d * 4, h_bytes = r * (r + 1) / 2 * p->d * 4;
   const size_t ws = garbage_h_ws_bytes(p, r, n);
@@ -480,6 +498,7 @@ int grid_gpu_garbage_h(grid_gpu_plan* p, const uint32_t* S, const uint32_t* Phi,
 
 int grid_gpu_amortize_workspace(const grid_gpu_plan* p, size_t r, size_t n, size_t* bytes) {
   if (!p || !bytes) return GRID_ERR_NULL_POINTER;
+  if (!square_dims_ok(p, r, n)) return GRID_ERR_INVALID_PARAMETERS;
   *bytes = amortize_ws_bytes(p, r, n);
   return GRID_OK;
 }
@@ -488,7 +507,7 @@ int grid_gpu_amortize_dev(const grid_gpu_plan* p, const uint32_t* S, const uint3
                           size_t n, uint32_t* z, void* workspace, size_t workspace_bytes,
                           void* stream) {
   if (!p || !S || !c || !z) return GRID_ERR_NULL_POINTER;
-  if (!dims_ok(r, n, 1)) return GRID_ERR_INVALID_PARAMETERS;
+  if (!square_dims_ok(p, r, n)) return GRID_ERR_INVALID_PARAMETERS;
   if (!aligned16(S) || !aligned16(c) || !aligned16(z) || !aligned16(workspace))
     return GRID_ERR_MISALIGNED;
   cudaStream_t st = (cudaStream_t)stream;
@@ -506,7 +525,7 @@ int grid_gpu_amortize_dev(const grid_gpu_plan* p, const uint32_t* S, const uint3
 int grid_gpu_amortize(grid_gpu_plan* p, const uint32_t* S, const uint32_t* c, size_t r, size_t n,
                       uint32_t* z) {
   if (!p || !S || !c || !z) return GRID_ERR_NULL_POINTER;
-  if (!dims_ok(r, n, 1)) return GRID_ERR_INVALID_PARAMETERS;
+  if (!square_dims_ok(p, r, n)) return GRID_ERR_INVALID_PARAMETERS;
   std::lock_guard<std::mutex> lk(p->mu);
   const size_t s_bytes = r * n * p->d * 4, c_bytes = r * p->d * 4, z_bytes = n * p->d * 4;
   const size_t ws = amortize_ws_bytes(p, r, n);
@@ -731,6 +750,8 @@ int grid_gpu_prover_round_workspace(const grid_gpu_matrix* A, size_t r, size_t j
   if (!A || !bytes) return GRID_ERR_NULL_POINTER;
   const grid_gpu_plan* p = A->plan;
   const size_t n = A->cols, kappa = A->rows, d = p->d;
+  if (!dims_ok(r, n, kappa) || !square_dims_ok(p, r, n) || !words_fit(r, kappa, d))
+    return GRID_ERR_INVALID_PARAMETERS;
   const size_t emm = emm_workspace_words(p, (int)r, (int)kappa, (int)n, EMM_DENSE) >
                              emm_workspace_words(p, (int)r, (int)r, (int)n, EMM_UPPER)
                          ? emm_workspace_words(p, (int)r, (int)kappa, (int)n, EMM_DENSE)
@@ -748,7 +769,8 @@ int grid_gpu_prover_round_dev(const grid_gpu_matrix* A, const uint32_t* S, size_
   if (!A || !S || !t_limbs || !g) return GRID_ERR_NULL_POINTER;
   const grid_gpu_plan* p = A->plan;
   const size_t n = A->cols, kappa = A->rows, d = p->d;
-  if (!dims_ok(r, n, kappa)) return GRID_ERR_INVALID_PARAMETERS;
+  if (!dims_ok(r, n, kappa) || !square_dims_ok(p, r, n) || !words_fit(r, kappa, d))
+    return GRID_ERR_INVALID_PARAMETERS;
   if (!aligned16(S) || !aligned16(g) || !aligned16(workspace)) return GRID_ERR_MISALIGNED;
   cudaStream_t st = (cudaStream_t)stream;
   Carver cv(workspace, workspace_bytes);
@@ -760,22 +782,49 @@ int grid_gpu_prover_round_dev(const grid_gpu_matrix* A, const uint32_t* S, size_
   uint32_t* t = cv.take<uint32_t>(r * kappa * d);
   void* jl_ws = cv.take<char>(jl_scratch_bytes(jl_rows ? jl_rows : 1, 0, 0));
   if (!cv.ok) return GRID_ERR_INVALID_PARAMETERS;
-  // Witness to the evaluation domain once; shared by the commitment and the Gram.
-  int rc = launch_ntt(p, MODE_FWD, S, nullptr, s_hat, r * n, st);
-  // 1. inner commitments t_i = A s_i, then balanced limbs (inner_commit_decomposed)
-  if (!rc)
-    rc = launch_emm(p, s_hat, A->d_evals, (int)r, (int)kappa, (int)n, (int)A->ld, EMM_DENSE, t,
-                    work, st);
-  if (!rc) rc = launch_ntt(p, MODE_INV, t, nullptr, t, r * kappa, st);
-  if (!rc) rc = launch_decompose_balanced(p, t, r * kappa, b1, t1, t_limbs, st);
-  // 2. garbage g_ij = <s_i, s_j>, i <= j, then balanced limbs
-  if (!rc) rc = launch_emm(p, s_hat, s_hat, (int)r, (int)r, (int)n, (int)n, EMM_UPPER, g, work, st);
-  if (!rc) rc = launch_ntt(p, MODE_INV, g, nullptr, g, r * (r + 1) / 2, st);
-  if (!rc && g_limbs) rc = launch_decompose_balanced(p, g, r * (r + 1) / 2, b2, t2, g_limbs, st);
-  // 3. JL projection of the coefficient vectors (one part per witness vector)
-  if (!rc && jl_seed && p_out)
-    rc = launch_jl_project(p->f, jl_seed, jl_rows, S, r, n * d, d, p_out, jl_flat, jl_ws,
-                           jl_scratch_bytes(jl_rows, 0, 0), p->num_sms, p->d_err, st);
+  // The JL projection reads only S and shares nothing with the commitment and
+  // Gram chain: fork both off the caller's stream (chain on the high-priority
+  // stream, JL on the low-priority one, so the JL's CTAs fill the SMs the
+  // chain leaves idle) and join them back before returning.
+  const bool jl = jl_seed && p_out;
+  cudaStream_t hi = p->fork_hi, lo = p->fork_lo;
+  cudaEvent_t ev[3] = {};
+  int rc = GRID_OK;
+  for (int i = 0; i < 3 && !rc; ++i)
+    rc = cuda_status(cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming));
+  if (!rc) rc = cuda_status(cudaEventRecord(ev[0], st));
+  if (!rc) rc = cuda_status(cudaStreamWaitEvent(hi, ev[0], 0));
+  if (!rc && jl) rc = cuda_status(cudaStreamWaitEvent(lo, ev[0], 0));
+  int rc_chain = rc, rc_jl = rc;
+  if (!rc) {
+    // 3. JL projection of the coefficient vectors (one part per witness vector)
+    if (jl)
+      rc_jl = launch_jl_project(p->f, jl_seed, jl_rows, S, r, n * d, d, p_out, jl_flat, jl_ws,
+                                jl_scratch_bytes(jl_rows, 0, 0), p->num_sms, p->d_err, lo);
+    // Witness to the evaluation domain once; shared by the commitment and the Gram.
+    rc_chain = launch_ntt(p, MODE_FWD, S, nullptr, s_hat, r * n, hi);
+    // 1. inner commitments t_i = A s_i, then balanced limbs (inner_commit_decomposed)
+    if (!rc_chain)
+      rc_chain = launch_emm(p, s_hat, A->d_evals, (int)r, (int)kappa, (int)n, (int)A->ld,
+                            EMM_DENSE, t, work, hi);
+    if (!rc_chain) rc_chain = launch_ntt(p, MODE_INV, t, nullptr, t, r * kappa, hi);
+    if (!rc_chain) rc_chain = launch_decompose_balanced(p, t, r * kappa, b1, t1, t_limbs, hi);
+    // 2. garbage g_ij = <s_i, s_j>, i <= j, then balanced limbs
+    if (!rc_chain)
+      rc_chain = launch_emm(p, s_hat, s_hat, (int)r, (int)r, (int)n, (int)n, EMM_UPPER, g, work,
+                            hi);
+    if (!rc_chain) rc_chain = launch_ntt(p, MODE_INV, g, nullptr, g, r * (r + 1) / 2, hi);
+    if (!rc_chain && g_limbs)
+      rc_chain = launch_decompose_balanced(p, g, r * (r + 1) / 2, b2, t2, g_limbs, hi);
+    // join: the caller's stream waits for both forks (also after a failed launch)
+    int rj = cuda_status(cudaEventRecord(ev[1], hi));
+    if (!rj) rj = cuda_status(cudaStreamWaitEvent(st, ev[1], 0));
+    if (!rj && jl) rj = cuda_status(cudaEventRecord(ev[2], lo));
+    if (!rj && jl) rj = cuda_status(cudaStreamWaitEvent(st, ev[2], 0));
+    rc = rc_chain ? rc_chain : rc_jl ? rc_jl : rj;
+  }
+  for (cudaEvent_t e : ev)
+    if (e) cudaEventDestroy(e);
   return rc;
 }
 

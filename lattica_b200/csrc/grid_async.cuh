@@ -56,13 +56,19 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 }
 
 // Bounded wait on an mbarrier phase. Returns false (and records a timeout in
-// *err) if the phase did not complete within kMaxSpins polls.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
-  for (uint32_t i = 0; i < kMaxSpins; ++i) {
+// *err) if the phase did not complete within max_spins polls.
+__device__ __forceinline__ bool mbar_wait_budget(uint64_t* bar, uint32_t parity,
+                                                 uint32_t max_spins, int* err) {
+  for (uint32_t i = 0; i < max_spins; ++i) {
     if (mbar_try_wait(bar, parity)) return true;
   }
   atomicExch(err, GRID_DEV_TIMEOUT);
   return false;
+}
+
+// The kernels' wait: kMaxSpins polls.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
+  return mbar_wait_budget(bar, parity, kMaxSpins, err);
 }
 
 // Bounded wait that lets the thread sleep in the barrier between polls

@@ -67,6 +67,10 @@ struct grid_gpu_plan {
   int* d_err = nullptr;
   cudaStream_t stream = nullptr;   // host-buffer entry points: first pipeline stream
   cudaStream_t stream2 = nullptr;  // second pipeline stream
+  // Forked work of *_dev calls (joined back into the caller's stream through
+  // events): the highest-priority stream for the critical path, the lowest for
+  // the independent work that fills the SMs around it.
+  cudaStream_t fork_hi = nullptr, fork_lo = nullptr;
   std::mutex mu;                   // serialises host-buffer calls and scratch growth
   grid::DeviceScratch scratch[16];
   int num_sms = 0;

@@ -28,7 +28,9 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratch
 
 // Device address of the buffer, looked up once per device. In host code the
 // array's name is only a host-side stand-in, so the address must come from
-// cudaGetSymbolAddress with that device current.
+// cudaGetSymbolAddress with that device current. The cached address lives as
+// long as the process's context on that device: like every plan and matrix of
+// this library, it does not survive cudaDeviceReset.
 std::mutex g_setup_mu;
 void* g_scratch_addr[grid::kMaxDevices] = {};
 
@@ -59,10 +61,21 @@ size_t grid_gpu_noalloc_scratch_bytes(void) { return kNoAllocScratchBytes; }
 int grid_gpu_gram_noalloc_dev(const grid_gpu_plan* plan, const uint32_t* S, size_t r, size_t n,
                               uint32_t* G, void* stream) {
   if (!plan || !S || !G) return GRID_ERR_NULL_POINTER;
+  if (r == 0 || n == 0) return GRID_ERR_INVALID_PARAMETERS;
+  // The witness's evaluations alone take r * n * d words of the buffer: reject
+  // sizes beyond it before any product that could wrap is formed.
+  const size_t max_polys = kNoAllocScratchBytes / (4 * (size_t)plan->d);
+  if (r > max_polys || n > max_polys / r) return GRID_ERR_SCRATCH_LIMIT;
   size_t need = 0;
   int st = grid_gpu_gram_workspace(plan, r, n, &need);
   if (st) return st;
   if (need > kNoAllocScratchBytes) return GRID_ERR_SCRATCH_LIMIT;
+  // The buffer's address is per device: the launches go to the current device,
+  // which must be the plan's.
+  int cur = -1;
+  cudaError_t e = cudaGetDevice(&cur);
+  if (e != cudaSuccess) return grid::cuda_status(e);
+  if (cur != plan->device) return GRID_ERR_INVALID_PARAMETERS;
   void* scratch = nullptr;
   st = scratch_for_device(plan->device, &scratch);
   if (st) return st;

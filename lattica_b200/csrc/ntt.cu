@@ -2,7 +2,7 @@
 //
 // Reference path replaced: TwistedNttPlan::{forward,inverse}_in_place_trusted
 // (algebra/src/poly/ntt.rs:75-104) over the bit-reverse + DIT forward and
-// GS + n^-1 + bit-reverse inverse (algebra/src/arith/ntt.rs:620-681), and the
+// GS + n^-1 + bit-reverse inverse (algebra/src/arith/ntt.rs:207-340), and the
 // "NTT -> Montgomery pointwise -> INTT" chain of a negacyclic product.
 //
 // Design (sm_100a):

@@ -6,7 +6,7 @@
 //   Montgomery constants           algebra/src/arith/prime.rs:60-91
 //   find_generator (smallest g)    algebra/src/arith/prime.rs:645-687
 //   root_of_unity / max_ntt_size   algebra/src/arith/prime.rs:566-607
-//   NttPlan::build error order     algebra/src/arith/ntt.rs:469-500
+//   NttPlan::build error order     algebra/src/arith/ntt.rs:124-154
 //   TwistedNttPlan::build (psi)    algebra/src/poly/ntt.rs:139-154
 #include <cuda_runtime.h>
 
@@ -436,6 +436,14 @@ int grid_gpu_plan_create(uint64_t q, uint64_t d, grid_gpu_plan** out) {
     if ((e = cudaMemset(p->d_err, 0, sizeof(int))) != cudaSuccess) break;
     if ((e = cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking)) != cudaSuccess) break;
     if ((e = cudaStreamCreateWithFlags(&p->stream2, cudaStreamNonBlocking)) != cudaSuccess) break;
+    int least = 0, greatest = 0;
+    if ((e = cudaDeviceGetStreamPriorityRange(&least, &greatest)) != cudaSuccess) break;
+    if ((e = cudaStreamCreateWithPriority(&p->fork_hi, cudaStreamNonBlocking, greatest)) !=
+        cudaSuccess)
+      break;
+    if ((e = cudaStreamCreateWithPriority(&p->fork_lo, cudaStreamNonBlocking, least)) !=
+        cudaSuccess)
+      break;
   } while (0);
   if (e != cudaSuccess) status = cuda_status(e);
   if (status) {
@@ -453,6 +461,8 @@ int grid_gpu_plan_destroy(grid_gpu_plan* p) {
   if (prev != p->device) cudaSetDevice(p->device);
   if (p->stream) cudaStreamSynchronize(p->stream);
   if (p->stream2) cudaStreamSynchronize(p->stream2);
+  if (p->fork_hi) cudaStreamSynchronize(p->fork_hi);
+  if (p->fork_lo) cudaStreamSynchronize(p->fork_lo);
   for (auto& s : p->scratch)
     if (s.ptr) cudaFree(s.ptr);
   if (p->d_tw) cudaFree(p->d_tw);
@@ -460,6 +470,8 @@ int grid_gpu_plan_destroy(grid_gpu_plan* p) {
   if (p->d_err) cudaFree(p->d_err);
   if (p->stream) cudaStreamDestroy(p->stream);
   if (p->stream2) cudaStreamDestroy(p->stream2);
+  if (p->fork_hi) cudaStreamDestroy(p->fork_hi);
+  if (p->fork_lo) cudaStreamDestroy(p->fork_lo);
   if (prev >= 0 && prev != p->device) cudaSetDevice(prev);
   delete p;
   return GRID_OK;

@@ -18,7 +18,7 @@ from ._lib import GridGpuError, PlanInfo, check
 
 
 class NttError(ValueError):
-    """Mirror of NttError (algebra/src/arith/ntt.rs:386-395)."""
+    """Mirror of NttError (algebra/src/arith/ntt.rs:40-50)."""
 
     KINDS = {1: "LengthMismatch", 2: "LengthNotPowerOfTwo", 3: "UnsupportedSize",
              4: "UnsupportedTwist"}
@@ -199,6 +199,51 @@ class TwistedNttPlan:
             st = self._lib.grid_gpu_poly_mul(self._h, lhs.ctypes.data, rhs.ctypes.data,
                                              lhs.ctypes.data, n)
         raise_status(st, "grid_gpu_poly_mul")
+
+    # -- slice hooks of Ring for PrimeField (algebra/src/arith/prime.rs:433-491),
+    #    on CUDA tensors of canonical words, in place on the current torch stream
+    def _slice_args(self, dst, src=None):
+        _dev_u32(dst)
+        if src is not None:
+            _dev_u32(src)
+            if src.numel() != dst.numel():
+                raise NttError("LengthMismatch", left=dst.numel(), right=src.numel())
+        return dst.numel(), _stream_ptr(dst)
+
+    def pointwise_mul_assign_slice(self, dst, rhs):
+        n, s = self._slice_args(dst, rhs)
+        raise_status(self._lib.grid_gpu_pointwise_mul_dev(self._h, dst.data_ptr(), rhs.data_ptr(),
+                                                          n, s), "grid_gpu_pointwise_mul_dev")
+
+    def add_assign_slice(self, dst, src):
+        n, s = self._slice_args(dst, src)
+        raise_status(self._lib.grid_gpu_add_assign_dev(self._h, dst.data_ptr(), src.data_ptr(),
+                                                       n, s), "grid_gpu_add_assign_dev")
+
+    def sub_assign_slice(self, dst, src):
+        n, s = self._slice_args(dst, src)
+        raise_status(self._lib.grid_gpu_sub_assign_dev(self._h, dst.data_ptr(), src.data_ptr(),
+                                                       n, s), "grid_gpu_sub_assign_dev")
+
+    def scalar_mul_slice(self, dst, scalar: int):
+        n, s = self._slice_args(dst)
+        raise_status(self._lib.grid_gpu_scalar_mul_dev(self._h, dst.data_ptr(), int(scalar), n, s),
+                     "grid_gpu_scalar_mul_dev")
+
+    def add_assign_scaled_slice(self, dst, src, scalar: int):
+        n, s = self._slice_args(dst, src)
+        raise_status(self._lib.grid_gpu_add_assign_scaled_dev(
+            self._h, dst.data_ptr(), src.data_ptr(), int(scalar), n, s),
+            "grid_gpu_add_assign_scaled_dev")
+
+    def dot_product(self, lhs, rhs) -> int:
+        import torch
+        n, s = self._slice_args(lhs, rhs)
+        out = torch.empty(4, dtype=torch.int32, device=lhs.device)
+        raise_status(self._lib.grid_gpu_dot_product_dev(self._h, lhs.data_ptr(), rhs.data_ptr(),
+                                                        n, out.data_ptr(), s),
+                     "grid_gpu_dot_product_dev")
+        return int(out[0].item()) & 0xFFFFFFFF
 
 
 _PLANS: dict = {}

@@ -200,7 +200,7 @@ int orc_plan_create(orc_plan *p, uint64_t q, uint64_t n) {
     int st = orc_field_init(&p->f, q);
     if (st) return st;
     const orc_field *f = &p->f;
-    /* NttPlan::build, ntt.rs:469-500 */
+    /* NttPlan::build, ntt.rs:124-154 */
     if (n == 0 || (n & (n - 1)) != 0) return ORC_ERR_LENGTH_NOT_POW2;
     uint32_t root = root_of_unity(f, n);
     if (root == 0) return ORC_ERR_UNSUPPORTED_SIZE;
@@ -223,7 +223,7 @@ int orc_plan_create(orc_plan *p, uint64_t q, uint64_t n) {
         orc_plan_destroy(p);
         return ORC_ERR_OOM;
     }
-    /* forward stages: stage_len = 2, 4, ..., n; w_len = root^(n/stage_len); stage_twiddles (ntt.rs:542-550) */
+    /* forward stages: stage_len = 2, 4, ..., n; w_len = root^(n/stage_len); stage_twiddles (ntt.rs:196-205) */
     size_t off = 0;
     for (uint64_t stage_len = 2; stage_len <= n; stage_len <<= 1) {
         uint64_t half = stage_len / 2;
@@ -258,7 +258,7 @@ void orc_plan_destroy(orc_plan *p) {
     p->fwd_tw = p->inv_tw = p->twists = p->untwists = NULL;
 }
 
-/* bit_reverse_permute, ntt.rs:526-540 */
+/* bit_reverse_permute, ntt.rs:180-194 */
 static void bit_reverse_permute(uint32_t *v, uint32_t n) {
     uint32_t j = 0;
     for (uint32_t i = 1; i < n; i++) {
@@ -269,7 +269,7 @@ static void bit_reverse_permute(uint32_t *v, uint32_t n) {
     }
 }
 
-/* scalar_ntt_forward_with_plan + apply_forward_chunk, ntt.rs:552-581,620-640 */
+/* scalar_ntt_forward_with_plan + apply_forward_chunk, ntt.rs:292-312,207-234 */
 void orc_ntt_forward(const orc_plan *p, uint32_t *v) {
     const orc_field *f = &p->f;
     const uint32_t n = p->n;
@@ -290,7 +290,7 @@ void orc_ntt_forward(const orc_plan *p, uint32_t *v) {
     }
 }
 
-/* scalar_ntt_inverse_with_plan + apply_inverse_chunk, ntt.rs:583-618,660-681:
+/* scalar_ntt_inverse_with_plan + apply_inverse_chunk, ntt.rs:314-340,236-280:
  * GS stages from len = n down to 2, n^-1 applied inside the last stage, then
  * bit reversal. */
 void orc_ntt_inverse(const orc_plan *p, uint32_t *v) {
@@ -391,6 +391,183 @@ void orc_naive_negacyclic(const orc_field *f, uint32_t n, const uint32_t *a, con
             if (i + j < n) out[i + j] = orc_add(f, out[i + j], prod);
             else out[i + j - n] = orc_sub(f, out[i + j - n], prod);
         }
+}
+
+/* Slice hooks of Ring for PrimeField (arith/prime.rs:433-491, over
+ * simd/montgomery.rs add_assign / sub_assign / scalar_mul): elementwise field
+ * operations on Montgomery words. dot_product (prime.rs:467-491) sums the
+ * Montgomery products; its CHUNK = 64 split changes no value. */
+void orc_add_assign_slice(const orc_field *f, uint32_t *dst, const uint32_t *src, size_t len) {
+    for (size_t i = 0; i < len; i++) dst[i] = orc_add(f, dst[i], src[i]);
+}
+
+void orc_sub_assign_slice(const orc_field *f, uint32_t *dst, const uint32_t *src, size_t len) {
+    for (size_t i = 0; i < len; i++) dst[i] = orc_sub(f, dst[i], src[i]);
+}
+
+void orc_scalar_mul_slice(const orc_field *f, uint32_t *dst, uint32_t scalar, size_t len) {
+    for (size_t i = 0; i < len; i++) dst[i] = orc_mul(f, dst[i], scalar);
+}
+
+/* add_assign_scaled_slice, prime.rs:449-465: dst += src * scalar */
+void orc_add_assign_scaled_slice(const orc_field *f, uint32_t *dst, const uint32_t *src,
+                                 uint32_t scalar, size_t len) {
+    for (size_t i = 0; i < len; i++) dst[i] = orc_add(f, dst[i], orc_mul(f, src[i], scalar));
+}
+
+uint32_t orc_dot_product(const orc_field *f, const uint32_t *lhs, const uint32_t *rhs, size_t len) {
+    uint32_t acc = 0;
+    for (size_t i = 0; i < len; i++) acc = orc_add(f, acc, orc_mul(f, lhs[i], rhs[i]));
+    return acc;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Ring products by the schoolbook rule, for any odd prime q < 2^32: the    */
+/* path the reference takes when q has no 2d-th root of unity               */
+/* (NegacyclicMulRing::negacyclic_mul_coeffs falls back to                  */
+/* naive_negacyclic_mul_coeffs, poly/ring.rs:60-100).                       */
+/* ------------------------------------------------------------------------ */
+
+/* out = sum_k a_k * b_k in R_q (Ring::dot_product default, arith/ring.rs:167-175,
+ * each term a negacyclic schoolbook product). The exact integer sums of the
+ * word products are kept per output coefficient, positive and negative
+ * (X^d = -1) separately, in 128 bits, and reduced once: sum of Montgomery
+ * products = (sum of word products) * 2^-32 mod q, so the canonical words equal
+ * those of the reference's term-by-term field arithmetic
+ * (tests/test_oracle_ring.py checks this against orc_naive_negacyclic). */
+static void ring_dot_schoolbook(const orc_field *f, uint32_t d, const uint32_t *a, size_t a_stride,
+                                const uint32_t *b, size_t b_stride, size_t len, uint32_t *out,
+                                unsigned __int128 *pos, unsigned __int128 *neg) {
+    for (uint32_t c = 0; c < d; c++) pos[c] = neg[c] = 0;
+    for (size_t k = 0; k < len; k++) {
+        const uint32_t *x = a + k * a_stride, *y = b + k * b_stride;
+        for (uint32_t i = 0; i < d; i++) {
+            const uint64_t xi = x[i];
+            for (uint32_t j = 0; j < d - i; j++) pos[i + j] += xi * y[j];
+            for (uint32_t j = d - i; j < d; j++) neg[i + j - d] += xi * y[j];
+        }
+    }
+    for (uint32_t c = 0; c < d; c++) {
+        const uint32_t pm = (uint32_t)(pos[c] % f->q), nm = (uint32_t)(neg[c] % f->q);
+        out[c] = mont_reduce(f, orc_sub(f, pm, nm));  /* x < q: x * 2^-32 mod q */
+    }
+}
+
+/* RingMat::mul_slice per witness (lattice/types.rs:334-343):
+ * t[b][i] = sum_k A[i][k] * s[b][k]. */
+int orc_ring_matvec(const orc_field *f, uint32_t d, const uint32_t *A, size_t rows, size_t cols,
+                    const uint32_t *s, size_t batch, uint32_t *t, int threads) {
+    if (threads <= 0) threads = 1;
+    int st = ORC_OK;
+#pragma omp parallel num_threads(threads)
+    {
+        unsigned __int128 *pos = (unsigned __int128 *)malloc(sizeof(unsigned __int128) * d);
+        unsigned __int128 *neg = (unsigned __int128 *)malloc(sizeof(unsigned __int128) * d);
+        if (!pos || !neg) {
+#pragma omp atomic write
+            st = ORC_ERR_OOM;
+        } else {
+#pragma omp for schedule(dynamic)
+            for (long long u = 0; u < (long long)(batch * rows); u++) {
+                const size_t b = (size_t)u / rows, i = (size_t)u % rows;
+                ring_dot_schoolbook(f, d, A + i * cols * d, d, s + b * cols * d, d, cols,
+                                    t + u * d, pos, neg);
+            }
+        }
+        free(pos);
+        free(neg);
+    }
+    return st;
+}
+
+/* compute_garbage_g (labrador/src/main_protocol/garbage.rs:76-93) with
+ * schoolbook products: g_ij = <s_i, s_j>, i <= j, garbage_index order. */
+int orc_ring_gram(const orc_field *f, uint32_t d, const uint32_t *S, size_t r, size_t n,
+                  uint32_t *G, int threads) {
+    if (threads <= 0) threads = 1;
+    const size_t cnt = r * (r + 1) / 2;
+    int st = ORC_OK;
+#pragma omp parallel num_threads(threads)
+    {
+        unsigned __int128 *pos = (unsigned __int128 *)malloc(sizeof(unsigned __int128) * d);
+        unsigned __int128 *neg = (unsigned __int128 *)malloc(sizeof(unsigned __int128) * d);
+        if (!pos || !neg) {
+#pragma omp atomic write
+            st = ORC_ERR_OOM;
+        } else {
+#pragma omp for schedule(dynamic)
+            for (long long u = 0; u < (long long)cnt; u++) {
+                size_t i = 0, rem = (size_t)u;
+                while (rem >= r - i) { rem -= r - i; i++; }
+                const size_t j = i + rem;
+                ring_dot_schoolbook(f, d, S + i * n * d, d, S + j * n * d, d, n, G + u * d, pos,
+                                    neg);
+            }
+        }
+        free(pos);
+        free(neg);
+    }
+    return st;
+}
+
+/* compute_garbage_h (garbage.rs:101-133) with schoolbook products:
+ * h_ij = (<phi_i, s_j> + <phi_j, s_i>) * 2^-1, 2^-1 = R::from_u64(q / 2 + 1). */
+int orc_ring_garbage_h(const orc_field *f, uint32_t d, const uint32_t *S, const uint32_t *Phi,
+                       size_t r, size_t n, uint32_t *H, int threads) {
+    if (threads <= 0) threads = 1;
+    const size_t cnt = r * (r + 1) / 2;
+    const uint32_t two_inv = orc_to_mont(f, f->q / 2 + 1);
+    int st = ORC_OK;
+#pragma omp parallel num_threads(threads)
+    {
+        unsigned __int128 *pos = (unsigned __int128 *)malloc(sizeof(unsigned __int128) * d);
+        unsigned __int128 *neg = (unsigned __int128 *)malloc(sizeof(unsigned __int128) * d);
+        uint32_t *t2 = (uint32_t *)malloc(sizeof(uint32_t) * d);
+        if (!pos || !neg || !t2) {
+#pragma omp atomic write
+            st = ORC_ERR_OOM;
+        } else {
+#pragma omp for schedule(dynamic)
+            for (long long u = 0; u < (long long)cnt; u++) {
+                size_t i = 0, rem = (size_t)u;
+                while (rem >= r - i) { rem -= r - i; i++; }
+                const size_t j = i + rem;
+                uint32_t *h = H + u * d;
+                ring_dot_schoolbook(f, d, Phi + i * n * d, d, S + j * n * d, d, n, h, pos, neg);
+                ring_dot_schoolbook(f, d, Phi + j * n * d, d, S + i * n * d, d, n, t2, pos, neg);
+                for (uint32_t c = 0; c < d; c++) h[c] = orc_mul(f, orc_add(f, h[c], t2[c]), two_inv);
+            }
+        }
+        free(pos);
+        free(neg);
+        free(t2);
+    }
+    return st;
+}
+
+/* compute_amortized_witness (labrador/src/main_protocol/amortization.rs:61-84)
+ * without the challenge sampling: z[k] = sum_i c_i * s_i[k], schoolbook products. */
+int orc_ring_amortize(const orc_field *f, uint32_t d, const uint32_t *S, const uint32_t *c,
+                      size_t r, size_t n, uint32_t *Z, int threads) {
+    if (threads <= 0) threads = 1;
+    int st = ORC_OK;
+#pragma omp parallel num_threads(threads)
+    {
+        unsigned __int128 *pos = (unsigned __int128 *)malloc(sizeof(unsigned __int128) * d);
+        unsigned __int128 *neg = (unsigned __int128 *)malloc(sizeof(unsigned __int128) * d);
+        if (!pos || !neg) {
+#pragma omp atomic write
+            st = ORC_ERR_OOM;
+        } else {
+#pragma omp for schedule(dynamic)
+            for (long long k = 0; k < (long long)n; k++)
+                ring_dot_schoolbook(f, d, c, d, S + (size_t)k * d, n * d, r, Z + (size_t)k * d,
+                                    pos, neg);
+        }
+        free(pos);
+        free(neg);
+    }
+    return st;
 }
 
 /* ------------------------------------------------------------------------ */

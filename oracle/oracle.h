@@ -71,7 +71,7 @@ void orc_plan_destroy(orc_plan *p);
 uint64_t orc_max_ntt_size(uint64_t q);
 uint32_t orc_find_generator(const orc_field *f);
 
-/* Cyclic NTT on one length-n vector (arith/ntt.rs:620-681). */
+/* Cyclic NTT on one length-n vector (arith/ntt.rs:207-340). */
 void orc_ntt_forward(const orc_plan *p, uint32_t *v);
 void orc_ntt_inverse(const orc_plan *p, uint32_t *v);
 /* Twisted transforms applied to `count` consecutive polys of length n. */
@@ -98,6 +98,27 @@ void orc_poly_mul_ntt(const orc_plan *p, const uint32_t *a, const uint32_t *b, u
 void orc_naive_negacyclic(const orc_field *f, uint32_t n, const uint32_t *a, const uint32_t *b,
                           uint32_t *out);
 void orc_pointwise_mul(const orc_field *f, uint32_t *dst, const uint32_t *rhs, size_t len);
+
+/* Slice hooks of Ring for PrimeField (arith/prime.rs:433-491). */
+void orc_add_assign_slice(const orc_field *f, uint32_t *dst, const uint32_t *src, size_t len);
+void orc_sub_assign_slice(const orc_field *f, uint32_t *dst, const uint32_t *src, size_t len);
+void orc_scalar_mul_slice(const orc_field *f, uint32_t *dst, uint32_t scalar, size_t len);
+void orc_add_assign_scaled_slice(const orc_field *f, uint32_t *dst, const uint32_t *src,
+                                 uint32_t scalar, size_t len);
+uint32_t orc_dot_product(const orc_field *f, const uint32_t *lhs, const uint32_t *rhs, size_t len);
+
+/* Ring contractions with schoolbook negacyclic products, for any odd prime
+ * q < 2^32 (the reference's path when q has no 2d-th root, poly/ring.rs:60-100):
+ * RingMat::mul_slice per witness, compute_garbage_g / compute_garbage_h, and the
+ * amortized witness z[k] = sum_i c_i s_i[k]. */
+int orc_ring_matvec(const orc_field *f, uint32_t d, const uint32_t *A, size_t rows, size_t cols,
+                    const uint32_t *s, size_t batch, uint32_t *t, int threads);
+int orc_ring_gram(const orc_field *f, uint32_t d, const uint32_t *S, size_t r, size_t n,
+                  uint32_t *G, int threads);
+int orc_ring_garbage_h(const orc_field *f, uint32_t d, const uint32_t *S, const uint32_t *Phi,
+                       size_t r, size_t n, uint32_t *H, int threads);
+int orc_ring_amortize(const orc_field *f, uint32_t d, const uint32_t *S, const uint32_t *c,
+                      size_t r, size_t n, uint32_t *Z, int threads);
 
 /* t[b][row] = sum_k A[row][k] * s[b][k] in R_q (commit/src/linear.rs:459-506,
  * poly/twisted_ntt.rs:378-408). A is coefficient-domain unless a_is_eval. */

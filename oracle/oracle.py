@@ -100,6 +100,19 @@ def lib():
             "orc_chacha20_quarter": (None, [_u32p, _u32p, _u32p, _u32p]),
             "orc_jl_project": (C.c_int, [fp, _u8p, C.c_size_t, C.c_size_t, _u32p, C.c_size_t,
                                          C.c_size_t, _u32p, _i8p, C.c_int]),
+            "orc_add_assign_slice": (None, [fp, _u32p, _u32p, C.c_size_t]),
+            "orc_sub_assign_slice": (None, [fp, _u32p, _u32p, C.c_size_t]),
+            "orc_scalar_mul_slice": (None, [fp, _u32p, C.c_uint32, C.c_size_t]),
+            "orc_add_assign_scaled_slice": (None, [fp, _u32p, _u32p, C.c_uint32, C.c_size_t]),
+            "orc_dot_product": (C.c_uint32, [fp, _u32p, _u32p, C.c_size_t]),
+            "orc_ring_matvec": (C.c_int, [fp, C.c_uint32, _u32p, C.c_size_t, C.c_size_t, _u32p,
+                                          C.c_size_t, _u32p, C.c_int]),
+            "orc_ring_gram": (C.c_int, [fp, C.c_uint32, _u32p, C.c_size_t, C.c_size_t, _u32p,
+                                        C.c_int]),
+            "orc_ring_garbage_h": (C.c_int, [fp, C.c_uint32, _u32p, _u32p, C.c_size_t,
+                                             C.c_size_t, _u32p, C.c_int]),
+            "orc_ring_amortize": (C.c_int, [fp, C.c_uint32, _u32p, _u32p, C.c_size_t, C.c_size_t,
+                                            _u32p, C.c_int]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -149,6 +162,88 @@ class Field:
 
     def one(self) -> int:
         return self.s.r_mod_q
+
+    # -- slice hooks of Ring for PrimeField (arith/prime.rs:433-491); new arrays
+    def add_slice(self, dst, src):
+        d, pd = _u32(np.array(dst, dtype=np.uint32, copy=True))
+        s_, ps = _u32(src)
+        lib().orc_add_assign_slice(C.byref(self.s), pd, ps, d.size)
+        return d
+
+    def sub_slice(self, dst, src):
+        d, pd = _u32(np.array(dst, dtype=np.uint32, copy=True))
+        s_, ps = _u32(src)
+        lib().orc_sub_assign_slice(C.byref(self.s), pd, ps, d.size)
+        return d
+
+    def scalar_mul_slice(self, dst, scalar: int):
+        d, pd = _u32(np.array(dst, dtype=np.uint32, copy=True))
+        lib().orc_scalar_mul_slice(C.byref(self.s), pd, scalar, d.size)
+        return d
+
+    def add_scaled_slice(self, dst, src, scalar: int):
+        d, pd = _u32(np.array(dst, dtype=np.uint32, copy=True))
+        s_, ps = _u32(src)
+        lib().orc_add_assign_scaled_slice(C.byref(self.s), pd, ps, scalar, d.size)
+        return d
+
+    def dot_product(self, lhs, rhs) -> int:
+        a, pa = _u32(lhs)
+        b, pb = _u32(rhs)
+        return lib().orc_dot_product(C.byref(self.s), pa, pb, a.size)
+
+    def pointwise_mul_slice(self, dst, rhs):
+        d, pd = _u32(np.array(dst, dtype=np.uint32, copy=True))
+        r_, pr = _u32(rhs)
+        lib().orc_pointwise_mul(C.byref(self.s), pd, pr, d.size)
+        return d
+
+    # -- ring contractions with schoolbook negacyclic products (any odd prime q)
+    def ring_matvec(self, d: int, A, rows: int, cols: int, s, batch: int, threads: int = 0):
+        A, pA = _u32(A)
+        s, ps = _u32(s)
+        t = np.empty(batch * rows * d, dtype=np.uint32)
+        st = lib().orc_ring_matvec(C.byref(self.s), d, pA, rows, cols, ps, batch,
+                                   t.ctypes.data_as(_u32p), threads or os.cpu_count())
+        if st:
+            raise OracleError(st)
+        return t
+
+    def ring_gram(self, d: int, S, r: int, n: int, threads: int = 0):
+        S, pS = _u32(S)
+        G = np.empty(r * (r + 1) // 2 * d, dtype=np.uint32)
+        st = lib().orc_ring_gram(C.byref(self.s), d, pS, r, n, G.ctypes.data_as(_u32p),
+                                 threads or os.cpu_count())
+        if st:
+            raise OracleError(st)
+        return G
+
+    def ring_garbage_h(self, d: int, S, Phi, r: int, n: int, threads: int = 0):
+        S, pS = _u32(S)
+        Phi, pP = _u32(Phi)
+        H = np.empty(r * (r + 1) // 2 * d, dtype=np.uint32)
+        st = lib().orc_ring_garbage_h(C.byref(self.s), d, pS, pP, r, n, H.ctypes.data_as(_u32p),
+                                      threads or os.cpu_count())
+        if st:
+            raise OracleError(st)
+        return H
+
+    def ring_amortize(self, d: int, S, c, r: int, n: int, threads: int = 0):
+        S, pS = _u32(S)
+        c, pc = _u32(c)
+        Z = np.empty(n * d, dtype=np.uint32)
+        st = lib().orc_ring_amortize(C.byref(self.s), d, pS, pc, r, n, Z.ctypes.data_as(_u32p),
+                                     threads or os.cpu_count())
+        if st:
+            raise OracleError(st)
+        return Z
+
+    def naive_negacyclic(self, a, b):
+        a, pa = _u32(a)
+        b, pb = _u32(b)
+        out = np.empty(a.size, dtype=np.uint32)
+        lib().orc_naive_negacyclic(C.byref(self.s), a.size, pa, pb, out.ctypes.data_as(_u32p))
+        return out
 
 
 class Plan:

@@ -3,9 +3,9 @@
 Reads the reference's Rust test modules as TEXT (the Rust toolchain is not
 available, so the reference cannot be executed) and writes the literal
 known-answer values to tests/golden/reference_kats.json, each with its source
-file:line. Run from this container, where the reference is mounted:
+file:line. The reference checkout's root directory is a required argument:
 
-    python tests/golden/extract_reference_kats.py /root/reference
+    python tests/golden/extract_reference_kats.py <path to the reference checkout>
 """
 from __future__ import annotations
 
@@ -171,4 +171,6 @@ def main(root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2 or not os.path.isdir(sys.argv[1]):
+        sys.exit("usage: extract_reference_kats.py <path to the reference checkout>")
+    main(sys.argv[1])

@@ -61,3 +61,30 @@ def test_reference_arm_line_keeps_the_contract(capsys):
     assert cb["host"]["nproc"] >= 1 and cb["host"]["model"]
     assert line["e2e"] == {"value": line["value"], "unit": "polys/s", "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}
+
+
+def test_secondary_summary_is_short_and_names_the_metric_figures():
+    """The JSON line's `secondary` holds the figures the metric names, flat,
+    and stays short enough for a log tail (the full detail goes to a file)."""
+    sys.path.insert(0, ROOT)
+    import bench
+    rate = {"p99_ms": 1.0, "commits_per_s": 10.0, "req_per_s": 20.0}
+    detail = {
+        "commit": {"commits_per_s": 4e6, "commits_per_s_graph": 8e6, "per_call_commits_per_s": 1e5,
+                   "e2e_commits_per_s": 9e5,
+                   "cpu_oracle_commits_per_s": {"threads_1": 7e3, "threads_all": 9e4}},
+        "round": {"round_ms_p50": 0.7, "round_ms_p99": 0.8, "e2e_round_ms_p50": 1.5,
+                  "cpu_oracle_round_ms": {"threads_1": 18000.0, "threads_all": 2000.0}},
+        "batch": {"batched_commits_per_s": 1.5e6, "per_call_commits_per_s": 2e4,
+                  "batched_ms_p50": 2.7},
+        "ntt256": {"polys_per_s": 7.8e8, "frac": 0.36},
+        "serve": {"commits_per_s_ratio": 8.8, "saturated_req_per_s_ratio": 3.0,
+                  "saturated": {"continuous": rate, "plain": rate},
+                  "rates": {str(k): {"continuous": rate, "plain": rate}
+                            for k in (1000, 5000, 50000)}},
+    }
+    out = bench.secondary_summary(detail)
+    for key in ("round_ms_p50", "round_ms_p99", "served_commits_per_s_ratio",
+                "served_req_per_s_ratio", "config0_commits_per_s", "config3_commits_per_s"):
+        assert out[key] is not None, key
+    assert len(json.dumps(out)) < 2000
