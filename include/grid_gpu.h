@@ -7,7 +7,7 @@
  *     value * 2^32 mod q, canonical in [0, q) (algebra/src/arith/prime.rs:24-29,
  *     repr(transparent) over u32).
  *   - A polynomial is d consecutive words (CyclotomicPolyRing / TwistedNttPoly
- *     are inline [R; N], algebra/src/poly/ring.rs:140-145,
+ *     are inline [R; N], algebra/src/poly/ring.rs:111-118,
  *     algebra/src/poly/twisted_ntt.rs:22-27).
  *   - A ring matrix is row-major rows x cols polynomials (RingMat,
  *     algebra/src/lattice/types.rs:230-265); a batch of vectors is
@@ -92,6 +92,27 @@ uint32_t grid_gpu_max_degree(void);
  * LengthNotPowerOfTwo, UnsupportedSize, UnsupportedTwist in that order. */
 int grid_gpu_plan_create(uint64_t q, uint64_t d, grid_gpu_plan** out);
 int grid_gpu_plan_destroy(grid_gpu_plan* plan);
+/* Ring plan: the plan of CyclotomicPolyRing<PrimeField<q>, d> arithmetic,
+ * mirroring NegacyclicMulRing::negacyclic_mul_coeffs (algebra/src/poly/ring.rs:79-102),
+ * which multiplies through the twisted NTT when q has a primitive 2d-th root of
+ * unity and by the schoolbook rule (naive_negacyclic_mul_coeffs, ring.rs:60-77)
+ * otherwise. For an NTT-friendly (q, d) this is grid_gpu_plan_create. For any
+ * other odd prime q < 2^32 and d in {8, ..., 256} it returns a plan whose ring
+ * products are exact integer sums of the word products, computed through three
+ * auxiliary NTT primes just below 2^32 and reconstructed mod q: the same words as
+ * the schoolbook rule. On such a plan the ring-level calls work (poly_mul,
+ * matrix_create with a_is_evals = 0, commit, linear/BDLOP commits, Gram,
+ * garbage h, amortization, the prover round, JL, decompositions, sampling,
+ * slice hooks); calls that need an evaluation domain mod q (NTT, ntt_mul_inverse,
+ * matrix evaluations, a_is_evals = 1, batch commits) return the error
+ * TwistedNttPlan::build reports for (q, d). Exactness bound: an output
+ * coefficient sums at most terms * d word products (terms = n for a commitment
+ * or Gram row, r for the amortized witness, 1 for poly_mul); calls with
+ * terms * d * (q - 1)^2 >= 2^93 return GRID_ERR_INVALID_PARAMETERS. */
+int grid_gpu_ring_plan_create(uint64_t q, uint64_t d, grid_gpu_plan** out);
+/* kind = 0: NTT plan; 1: ring plan through auxiliary primes (their three
+ * moduli written to aux_moduli when it is not NULL). */
+int grid_gpu_plan_ring_kind(const grid_gpu_plan* plan, int* kind, uint32_t* aux_moduli);
 /* Host-only: validate (q, d) exactly like grid_gpu_plan_create and return the
  * plan's parameters and merged twiddles without touching a device. Any output
  * pointer may be NULL (zeta/izeta: d words each). */
@@ -126,7 +147,10 @@ int grid_gpu_ntt_mul_inverse_dev(const grid_gpu_plan* plan, const uint32_t* a,
                                  const uint32_t* b_evals, uint32_t* out, size_t npolys,
                                  void* stream);
 /* Negacyclic product out = a * b mod (X^d + 1), poly_mul_ntt
- * (algebra/src/poly/ntt.rs:305-319). Uses b_scratch (npolys*d words) for NTT(b). */
+ * (algebra/src/poly/ntt.rs:305-319), or the schoolbook product's words on a
+ * ring plan without an NTT for q. b_scratch holds
+ * grid_gpu_poly_mul_scratch_words(plan, npolys) words (npolys * d on an NTT plan). */
+size_t grid_gpu_poly_mul_scratch_words(const grid_gpu_plan* plan, size_t npolys);
 int grid_gpu_poly_mul_dev(const grid_gpu_plan* plan, const uint32_t* a, const uint32_t* b,
                           uint32_t* out, uint32_t* b_scratch, size_t npolys, void* stream);
 /* Ring::pointwise_mul_assign_slice (algebra/src/arith/prime.rs:433-447): dst *= rhs. */

@@ -47,6 +47,9 @@ SIGNATURES = {
     "grid_gpu_max_degree": (C.c_uint32, []),
     "grid_gpu_plan_create": (C.c_int, [C.c_uint64, C.c_uint64, C.POINTER(_vp)]),
     "grid_gpu_plan_destroy": (C.c_int, [_vp]),
+    "grid_gpu_ring_plan_create": (C.c_int, [C.c_uint64, C.c_uint64, C.POINTER(_vp)]),
+    "grid_gpu_plan_ring_kind": (C.c_int, [_vp, C.POINTER(C.c_int), _vp]),
+    "grid_gpu_poly_mul_scratch_words": (C.c_size_t, [_vp, C.c_size_t]),
     "grid_gpu_plan_describe": (C.c_int, [C.c_uint64, C.c_uint64, C.POINTER(PlanInfo), _vp, _vp]),
     "grid_gpu_plan_get_info": (C.c_int, [_vp, C.POINTER(PlanInfo)]),
     "grid_gpu_plan_get_twiddles": (C.c_int, [_vp, _vp, _vp]),

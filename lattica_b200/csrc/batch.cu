@@ -201,8 +201,6 @@ __global__ void fold_kernel(const unsigned long long* __restrict__ acc, uint32_t
     out[i] = (uint32_t)(acc[i] % q);
 }
 
-size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
-
 }  // namespace
 }  // namespace grid
 
@@ -337,6 +335,9 @@ int build_tables(const grid_gpu_plan* plan, grid_gpu_matrix* const* mats, size_t
                  const grid_gpu_batch_item* items, size_t nitems, uint32_t k_split,
                  Tables& tb) {
   if (!plan || (!mats && nmats) || (!items && nitems)) return GRID_ERR_NULL_POINTER;
+  // the grouped kernel contracts evaluations mod q: a ring plan without an NTT
+  // for q commits through grid_gpu_commit_dev instead
+  if (is_crt(plan)) return plan->ntt_status;
   if (nmats == 0 || nitems == 0 || nitems > (1u << 30)) return GRID_ERR_INVALID_PARAMETERS;
   if (k_split != 0 && (k_split < (uint32_t)KC || k_split % KC)) return GRID_ERR_INVALID_PARAMETERS;
   for (size_t i = 0; i < nmats; ++i) {

@@ -13,51 +13,54 @@ namespace {
 
 bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
 
-size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
-
-// Bump allocator over a caller workspace (256-byte aligned sub-buffers).
-struct Carver {
-  char* base;
-  size_t cap, used = 0;
-  bool ok = true;
-  Carver(void* b, size_t c) : base(static_cast<char*>(b)), cap(c) {}
-  template <typename T>
-  T* take(size_t count) {
-    if (count > (cap + 1) / sizeof(T)) {  // also keeps count * sizeof(T) from wrapping
-      ok = false;
-      return nullptr;
-    }
-    const size_t bytes = round_up(count * sizeof(T), 256);
-    if (used + bytes > cap || !base) {
-      ok = false;
-      used += bytes;
-      return nullptr;
-    }
-    T* p = reinterpret_cast<T*>(base + used);
-    used += bytes;
-    return p;
-  }
-};
-
-size_t words_bytes(size_t words) { return round_up(words * 4, 256); }
-
+// Workspace layouts. On a ring plan without an NTT for q (is_crt) a call
+// lifts its inputs into one residue buffer per auxiliary prime in turn (reused),
+// keeps the three residue results, and runs the prime's own call in the rest of
+// the workspace (reused across the primes); the reconstruction writes the output.
 size_t commit_ws_bytes(const grid_gpu_plan* p, size_t rows, size_t cols, size_t batch) {
+  if (is_crt(p))
+    return words_bytes(batch * cols * p->d) + 3 * words_bytes(batch * rows * p->d) +
+           commit_ws_bytes(p->crt[0], rows, cols, batch);
   return words_bytes(batch * cols * p->d) +
          words_bytes(emm_workspace_words(p, (int)batch, (int)rows, (int)cols, EMM_DENSE));
 }
 
 size_t gram_ws_bytes(const grid_gpu_plan* p, size_t r, size_t n) {
-  return words_bytes(r * n * p->d) + words_bytes(emm_workspace_words(p, (int)r, (int)r, (int)n,
-                                                                       EMM_UPPER));
+  const grid_gpu_plan* e = is_crt(p) ? p->crt[0] : p;
+  const size_t base = words_bytes(r * n * p->d) +
+                      words_bytes(emm_workspace_words(e, (int)r, (int)r, (int)n, EMM_UPPER));
+  return is_crt(p) ? base + 3 * words_bytes(r * (r + 1) / 2 * p->d) : base;
 }
 
 size_t garbage_h_ws_bytes(const grid_gpu_plan* p, size_t r, size_t n) {
-  return 2 * words_bytes(r * n * p->d) + words_bytes(r * r * p->d) +
-         words_bytes(emm_workspace_words(p, (int)r, (int)r, (int)n, EMM_DENSE));
+  const grid_gpu_plan* e = is_crt(p) ? p->crt[0] : p;
+  const size_t base = 2 * words_bytes(r * n * p->d) + words_bytes(r * r * p->d) +
+                      words_bytes(emm_workspace_words(e, (int)r, (int)r, (int)n, EMM_DENSE));
+  return is_crt(p) ? base + 3 * words_bytes(r * r * p->d) : base;
 }
 
 size_t amortize_ws_bytes(const grid_gpu_plan* p, size_t r, size_t n) {
-  return words_bytes(r * n * p->d) + words_bytes(r * p->d);
+  const size_t base = words_bytes(r * n * p->d) + words_bytes(r * p->d);
+  return is_crt(p) ? base + 3 * words_bytes(n * p->d) : base;
+}
+
+size_t round_ws_bytes(const grid_gpu_plan* p, size_t r, size_t n, size_t kappa, size_t jl_rows) {
+  const grid_gpu_plan* e = is_crt(p) ? p->crt[0] : p;
+  const size_t d = p->d;
+  const size_t e1 = emm_workspace_words(e, (int)r, (int)kappa, (int)n, EMM_DENSE);
+  const size_t e2 = emm_workspace_words(e, (int)r, (int)r, (int)n, EMM_UPPER);
+  const size_t base = words_bytes(r * n * d) + words_bytes(e1 > e2 ? e1 : e2) +
+                      words_bytes(r * kappa * d) +
+                      round_up(jl_scratch_bytes(jl_rows ? jl_rows : 1, 0, 0), 256);
+  return is_crt(p) ? base + 3 * (words_bytes(r * kappa * d) + words_bytes(r * (r + 1) / 2 * d))
+                   : base;
+}
+
+// x mod p_j into dst (the j-th auxiliary prime only)
+int lift_one(const grid_gpu_plan* p, int j, const uint32_t* x, size_t words, uint32_t* dst,
+             cudaStream_t st) {
+  return crt_lift(p, x, words, j == 0 ? dst : nullptr, j == 1 ? dst : nullptr,
+                  j == 2 ? dst : nullptr, st);
 }
 
 bool dims_ok(size_t a, size_t b, size_t c) {
@@ -81,6 +84,21 @@ bool square_dims_ok(const grid_gpu_plan* p, size_t r, size_t n) {
 int commit_core(const grid_gpu_matrix* A, const uint32_t* s, size_t batch, uint32_t* t,
                 Carver& cv, cudaStream_t st) {
   const grid_gpu_plan* p = A->plan;
+  if (is_crt(p)) {
+    if (!crt_bound_ok(p, A->cols)) return GRID_ERR_INVALID_PARAMETERS;
+    const size_t sw = batch * A->cols * p->d, tw = batch * A->rows * p->d;
+    uint32_t* sj = cv.take<uint32_t>(sw);
+    uint32_t* tj[3] = {cv.take<uint32_t>(tw), cv.take<uint32_t>(tw), cv.take<uint32_t>(tw)};
+    if (!cv.ok) return GRID_ERR_INVALID_PARAMETERS;
+    const size_t mark = cv.used;
+    for (int j = 0; j < 3; ++j) {
+      int rc = lift_one(p, j, s, sw, sj, st);
+      if (!rc) rc = commit_core(A->crt[j], sj, batch, tj[j], cv, st);
+      if (rc) return rc;
+      cv.used = mark;  // the next prime reuses the same workspace
+    }
+    return crt_combine(p, tj[0], tj[1], tj[2], tw, t, st);
+  }
   if (commit_small_fits(p, A->rows, A->cols, batch))
     return launch_commit_small(p, A->d_evals, A->rows, A->cols, A->ld, s, batch, t, st);
   uint32_t* s_hat = cv.take<uint32_t>(batch * A->cols * p->d);
@@ -107,6 +125,8 @@ int grid_gpu_matrix_create_dev(grid_gpu_plan* p, const uint32_t* A, size_t rows,
   *out = nullptr;
   if (!dims_ok(rows, cols, 1)) return GRID_ERR_INVALID_PARAMETERS;
   if (!aligned16(A)) return GRID_ERR_MISALIGNED;
+  if (!words_fit(rows, cols, p->d)) return GRID_ERR_INVALID_PARAMETERS;
+  if (is_crt(p) && a_is_evals) return p->ntt_status;  // q has no evaluation domain
   grid_gpu_matrix* m = new (std::nothrow) grid_gpu_matrix();
   if (!m) return GRID_ERR_OUT_OF_MEMORY;
   m->plan = p;
@@ -114,6 +134,33 @@ int grid_gpu_matrix_create_dev(grid_gpu_plan* p, const uint32_t* A, size_t rows,
   m->cols = cols;
   m->ld = cols;
   cudaStream_t st = (cudaStream_t)stream;
+  if (is_crt(p)) {
+    // residues mod each auxiliary prime, prepared (transformed) on its plan
+    const size_t words = rows * cols * p->d;
+    int rc = GRID_OK;
+    for (int j = 0; j < 3 && !rc; ++j) {
+      grid_gpu_matrix* sub = new (std::nothrow) grid_gpu_matrix();
+      if (!sub) {
+        rc = GRID_ERR_OUT_OF_MEMORY;
+        break;
+      }
+      m->crt[j] = sub;
+      sub->plan = p->crt[j];
+      sub->rows = rows;
+      sub->cols = cols;
+      sub->ld = cols;
+      rc = cuda_status(cudaMalloc(&sub->d_evals, words * 4));
+      if (!rc) rc = lift_one(p, j, A, words, sub->d_evals, st);
+      if (!rc) rc = launch_ntt(sub->plan, MODE_FWD, sub->d_evals, nullptr, sub->d_evals,
+                               rows * cols, st);
+    }
+    if (rc) {
+      grid_gpu_matrix_destroy(m);
+      return rc;
+    }
+    *out = m;
+    return GRID_OK;
+  }
   cudaError_t e = cudaMalloc(&m->d_evals, rows * cols * p->d * 4);
   if (e != cudaSuccess) {
     delete m;
@@ -159,6 +206,8 @@ int grid_gpu_matrix_create(grid_gpu_plan* p, const uint32_t* A, size_t rows, siz
 
 int grid_gpu_matrix_destroy(grid_gpu_matrix* m) {
   if (!m) return GRID_ERR_NULL_POINTER;
+  for (grid_gpu_matrix* sub : m->crt)
+    if (sub) grid_gpu_matrix_destroy(sub);
   if (m->owned && m->d_evals) cudaFree(m->d_evals);
   delete m;
   return GRID_OK;
@@ -176,6 +225,14 @@ int grid_gpu_matrix_view(const grid_gpu_matrix* parent, size_t cols, grid_gpu_ma
   m->ld = parent->ld;
   m->d_evals = parent->d_evals;
   m->owned = false;
+  for (int j = 0; j < 3; ++j)
+    if (parent->crt[j]) {
+      const int rc = grid_gpu_matrix_view(parent->crt[j], cols, &m->crt[j]);
+      if (rc) {
+        grid_gpu_matrix_destroy(m);
+        return rc;
+      }
+    }
   *out = m;
   return GRID_OK;
 }
@@ -189,6 +246,7 @@ int grid_gpu_matrix_shape(const grid_gpu_matrix* m, size_t* rows, size_t* cols) 
 
 int grid_gpu_matrix_device_evals(const grid_gpu_matrix* m, const uint32_t** evals) {
   if (!m || !evals) return GRID_ERR_NULL_POINTER;
+  if (is_crt(m->plan)) return m->plan->ntt_status;  // no evaluation domain mod q
   *evals = m->d_evals;
   return GRID_OK;
 }
@@ -403,16 +461,33 @@ int grid_gpu_gram_dev(const grid_gpu_plan* p, const uint32_t* S, size_t r, size_
   if (!square_dims_ok(p, r, n)) return GRID_ERR_INVALID_PARAMETERS;
   if (!aligned16(S) || !aligned16(G) || !aligned16(workspace)) return GRID_ERR_MISALIGNED;
   cudaStream_t st = (cudaStream_t)stream;
+  if (is_crt(p) && !crt_bound_ok(p, n)) return GRID_ERR_INVALID_PARAMETERS;
+  const grid_gpu_plan* e = is_crt(p) ? p->crt[0] : p;
+  const size_t gw = r * (r + 1) / 2 * p->d;
   Carver cv(workspace, workspace_bytes);
   uint32_t* s_hat = cv.take<uint32_t>(r * n * p->d);
-  const size_t ew = emm_workspace_words(p, (int)r, (int)r, (int)n, EMM_UPPER);
+  const size_t ew = emm_workspace_words(e, (int)r, (int)r, (int)n, EMM_UPPER);
   uint32_t* work = ew ? cv.take<uint32_t>(ew) : nullptr;
+  uint32_t* gj[3] = {};
+  if (is_crt(p))
+    for (auto& x : gj) x = cv.take<uint32_t>(gw);
   if (!cv.ok) return GRID_ERR_INVALID_PARAMETERS;
-  int rc = launch_ntt(p, MODE_FWD, S, nullptr, s_hat, r * n, st);
-  if (rc) return rc;
-  rc = launch_emm(p, s_hat, s_hat, (int)r, (int)r, (int)n, (int)n, EMM_UPPER, G, work, st);
-  if (rc) return rc;
-  return launch_ntt(p, MODE_INV, G, nullptr, G, r * (r + 1) / 2, st);
+  int rc = GRID_OK;
+  for (int j = 0; j < (is_crt(p) ? 3 : 1) && !rc; ++j) {
+    const grid_gpu_plan* q = is_crt(p) ? p->crt[j] : p;
+    uint32_t* out = is_crt(p) ? gj[j] : G;
+    if (is_crt(p)) {
+      rc = lift_one(p, j, S, r * n * p->d, s_hat, st);
+      if (!rc) rc = launch_ntt(q, MODE_FWD, s_hat, nullptr, s_hat, r * n, st);
+    } else {
+      rc = launch_ntt(q, MODE_FWD, S, nullptr, s_hat, r * n, st);
+    }
+    if (!rc)
+      rc = launch_emm(q, s_hat, s_hat, (int)r, (int)r, (int)n, (int)n, EMM_UPPER, out, work, st);
+    if (!rc) rc = launch_ntt(q, MODE_INV, out, nullptr, out, r * (r + 1) / 2, st);
+  }
+  if (!rc && is_crt(p)) rc = crt_combine(p, gj[0], gj[1], gj[2], gw, G, st);
+  return rc;
 }
 
 int grid_gpu_gram(grid_gpu_plan* p, const uint32_t* S, size_t r, size_t n, uint32_t* G) {
@@ -457,17 +532,42 @@ int grid_gpu_garbage_h_dev(const grid_gpu_plan* p, const uint32_t* S, const uint
   uint32_t* s_hat = cv.take<uint32_t>(r * n * p->d);
   uint32_t* phi_hat = cv.take<uint32_t>(r * n * p->d);
   uint32_t* cross = cv.take<uint32_t>(r * r * p->d);
-  const size_t ew = emm_workspace_words(p, (int)r, (int)r, (int)n, EMM_DENSE);
+  const grid_gpu_plan* e = is_crt(p) ? p->crt[0] : p;
+  const size_t ew = emm_workspace_words(e, (int)r, (int)r, (int)n, EMM_DENSE);
   uint32_t* work = ew ? cv.take<uint32_t>(ew) : nullptr;
+  if (!is_crt(p)) {
+    if (!cv.ok) return GRID_ERR_INVALID_PARAMETERS;
+    int rc = launch_ntt(p, MODE_FWD, S, nullptr, s_hat, r * n, st);
+    if (!rc) rc = launch_ntt(p, MODE_FWD, Phi, nullptr, phi_hat, r * n, st);
+    // cross[i][j] = <phi_i, s_j>
+    if (!rc)
+      rc = launch_emm(p, phi_hat, s_hat, (int)r, (int)r, (int)n, (int)n, EMM_DENSE, cross, work,
+                      st);
+    if (!rc) rc = launch_symmetrize_half(p, cross, (int)r, H, st);
+    if (rc) return rc;
+    return launch_ntt(p, MODE_INV, H, nullptr, H, r * (r + 1) / 2, st);
+  }
+  // ring plan without an NTT for q: the cross products per auxiliary prime,
+  // back to coefficients, reconstructed mod q; then the (linear) symmetrisation
+  if (!crt_bound_ok(p, n)) return GRID_ERR_INVALID_PARAMETERS;
+  const size_t cw = r * r * p->d;
+  uint32_t* cj[3] = {cv.take<uint32_t>(cw), cv.take<uint32_t>(cw), cv.take<uint32_t>(cw)};
   if (!cv.ok) return GRID_ERR_INVALID_PARAMETERS;
-  int rc = launch_ntt(p, MODE_FWD, S, nullptr, s_hat, r * n, st);
-  if (!rc) rc = launch_ntt(p, MODE_FWD, Phi, nullptr, phi_hat, r * n, st);
-  // cross[i][j] = <phi_i, s_j>
-  if (!rc)
-    rc = launch_emm(p, phi_hat, s_hat, (int)r, (int)r, (int)n, (int)n, EMM_DENSE, cross, work, st);
+  int rc = GRID_OK;
+  for (int j = 0; j < 3 && !rc; ++j) {
+    const grid_gpu_plan* q = p->crt[j];
+    rc = lift_one(p, j, S, r * n * p->d, s_hat, st);
+    if (!rc) rc = lift_one(p, j, Phi, r * n * p->d, phi_hat, st);
+    if (!rc) rc = launch_ntt(q, MODE_FWD, s_hat, nullptr, s_hat, r * n, st);
+    if (!rc) rc = launch_ntt(q, MODE_FWD, phi_hat, nullptr, phi_hat, r * n, st);
+    if (!rc)
+      rc = launch_emm(q, phi_hat, s_hat, (int)r, (int)r, (int)n, (int)n, EMM_DENSE, cj[j], work,
+                      st);
+    if (!rc) rc = launch_ntt(q, MODE_INV, cj[j], nullptr, cj[j], r * r, st);
+  }
+  if (!rc) rc = crt_combine(p, cj[0], cj[1], cj[2], cw, cross, st);
   if (!rc) rc = launch_symmetrize_half(p, cross, (int)r, H, st);
-  if (rc) return rc;
-  return launch_ntt(p, MODE_INV, H, nullptr, H, r * (r + 1) / 2, st);
+  return rc;
 }
 
 int grid_gpu_garbage_h(grid_gpu_plan* p, const uint32_t* S, const uint32_t* Phi, size_t r,
@@ -514,12 +614,31 @@ int grid_gpu_amortize_dev(const grid_gpu_plan* p, const uint32_t* S, const uint3
   Carver cv(workspace, workspace_bytes);
   uint32_t* s_hat = cv.take<uint32_t>(r * n * p->d);
   uint32_t* c_hat = cv.take<uint32_t>(r * p->d);
+  if (!is_crt(p)) {
+    if (!cv.ok) return GRID_ERR_INVALID_PARAMETERS;
+    int rc = launch_ntt(p, MODE_FWD, S, nullptr, s_hat, r * n, st);
+    if (!rc) rc = launch_ntt(p, MODE_FWD, c, nullptr, c_hat, r, st);
+    if (!rc) rc = launch_amortize(p, c_hat, s_hat, (int)r, n, z, st);
+    if (rc) return rc;
+    return launch_ntt(p, MODE_INV, z, nullptr, z, n, st);
+  }
+  // ring plan without an NTT for q: z[k] = sum_i c_i s_i[k] sums r * d products
+  if (!crt_bound_ok(p, r)) return GRID_ERR_INVALID_PARAMETERS;
+  const size_t zw = n * p->d;
+  uint32_t* zj[3] = {cv.take<uint32_t>(zw), cv.take<uint32_t>(zw), cv.take<uint32_t>(zw)};
   if (!cv.ok) return GRID_ERR_INVALID_PARAMETERS;
-  int rc = launch_ntt(p, MODE_FWD, S, nullptr, s_hat, r * n, st);
-  if (!rc) rc = launch_ntt(p, MODE_FWD, c, nullptr, c_hat, r, st);
-  if (!rc) rc = launch_amortize(p, c_hat, s_hat, (int)r, n, z, st);
+  int rc = GRID_OK;
+  for (int j = 0; j < 3 && !rc; ++j) {
+    const grid_gpu_plan* q = p->crt[j];
+    rc = lift_one(p, j, S, r * n * p->d, s_hat, st);
+    if (!rc) rc = lift_one(p, j, c, r * p->d, c_hat, st);
+    if (!rc) rc = launch_ntt(q, MODE_FWD, s_hat, nullptr, s_hat, r * n, st);
+    if (!rc) rc = launch_ntt(q, MODE_FWD, c_hat, nullptr, c_hat, r, st);
+    if (!rc) rc = launch_amortize(q, c_hat, s_hat, (int)r, n, zj[j], st);
+    if (!rc) rc = launch_ntt(q, MODE_INV, zj[j], nullptr, zj[j], n, st);
+  }
   if (rc) return rc;
-  return launch_ntt(p, MODE_INV, z, nullptr, z, n, st);
+  return crt_combine(p, zj[0], zj[1], zj[2], zw, z, st);
 }
 
 int grid_gpu_amortize(grid_gpu_plan* p, const uint32_t* S, const uint32_t* c, size_t r, size_t n,
@@ -752,12 +871,7 @@ int grid_gpu_prover_round_workspace(const grid_gpu_matrix* A, size_t r, size_t j
   const size_t n = A->cols, kappa = A->rows, d = p->d;
   if (!dims_ok(r, n, kappa) || !square_dims_ok(p, r, n) || !words_fit(r, kappa, d))
     return GRID_ERR_INVALID_PARAMETERS;
-  const size_t emm = emm_workspace_words(p, (int)r, (int)kappa, (int)n, EMM_DENSE) >
-                             emm_workspace_words(p, (int)r, (int)r, (int)n, EMM_UPPER)
-                         ? emm_workspace_words(p, (int)r, (int)kappa, (int)n, EMM_DENSE)
-                         : emm_workspace_words(p, (int)r, (int)r, (int)n, EMM_UPPER);
-  *bytes = words_bytes(r * n * d) + words_bytes(emm) + words_bytes(r * kappa * d) +
-           round_up(jl_scratch_bytes(jl_rows ? jl_rows : 1, 0, 0), 256);
+  *bytes = round_ws_bytes(p, r, n, kappa, jl_rows);
   return GRID_OK;
 }
 
@@ -772,16 +886,40 @@ int grid_gpu_prover_round_dev(const grid_gpu_matrix* A, const uint32_t* S, size_
   if (!dims_ok(r, n, kappa) || !square_dims_ok(p, r, n) || !words_fit(r, kappa, d))
     return GRID_ERR_INVALID_PARAMETERS;
   if (!aligned16(S) || !aligned16(g) || !aligned16(workspace)) return GRID_ERR_MISALIGNED;
+  if (is_crt(p) && !crt_bound_ok(p, n)) return GRID_ERR_INVALID_PARAMETERS;
   cudaStream_t st = (cudaStream_t)stream;
+  const grid_gpu_plan* e = is_crt(p) ? p->crt[0] : p;
   Carver cv(workspace, workspace_bytes);
   uint32_t* s_hat = cv.take<uint32_t>(r * n * d);
-  const size_t e1 = emm_workspace_words(p, (int)r, (int)kappa, (int)n, EMM_DENSE);
-  const size_t e2 = emm_workspace_words(p, (int)r, (int)r, (int)n, EMM_UPPER);
+  const size_t e1 = emm_workspace_words(e, (int)r, (int)kappa, (int)n, EMM_DENSE);
+  const size_t e2 = emm_workspace_words(e, (int)r, (int)r, (int)n, EMM_UPPER);
   const size_t ew = e1 > e2 ? e1 : e2;
   uint32_t* work = ew ? cv.take<uint32_t>(ew) : nullptr;
   uint32_t* t = cv.take<uint32_t>(r * kappa * d);
   void* jl_ws = cv.take<char>(jl_scratch_bytes(jl_rows ? jl_rows : 1, 0, 0));
+  // ring plan without an NTT for q: t and g per auxiliary prime
+  const size_t tw = r * kappa * d, gw = r * (r + 1) / 2 * d;
+  uint32_t *tj[3] = {}, *gj[3] = {};
+  if (is_crt(p))
+    for (int j = 0; j < 3; ++j) {
+      tj[j] = cv.take<uint32_t>(tw);
+      gj[j] = cv.take<uint32_t>(gw);
+    }
   if (!cv.ok) return GRID_ERR_INVALID_PARAMETERS;
+  // inner commitments and the Gram over the witness's evaluations (one
+  // transform shared by both) on plan q into tt / gg
+  auto contract = [&](const grid_gpu_plan* q, const grid_gpu_matrix* Aq, const uint32_t* src,
+                      uint32_t* tt, uint32_t* gg, cudaStream_t cs) {
+    int rc = launch_ntt(q, MODE_FWD, src, nullptr, s_hat, r * n, cs);
+    if (!rc)
+      rc = launch_emm(q, s_hat, Aq->d_evals, (int)r, (int)kappa, (int)n, (int)Aq->ld, EMM_DENSE,
+                      tt, work, cs);
+    if (!rc) rc = launch_ntt(q, MODE_INV, tt, nullptr, tt, r * kappa, cs);
+    if (!rc)
+      rc = launch_emm(q, s_hat, s_hat, (int)r, (int)r, (int)n, (int)n, EMM_UPPER, gg, work, cs);
+    if (!rc) rc = launch_ntt(q, MODE_INV, gg, nullptr, gg, r * (r + 1) / 2, cs);
+    return rc;
+  };
   // The JL projection reads only S and shares nothing with the commitment and
   // Gram chain: fork both off the caller's stream (chain on the high-priority
   // stream, JL on the low-priority one, so the JL's CTAs fill the SMs the
@@ -801,19 +939,19 @@ int grid_gpu_prover_round_dev(const grid_gpu_matrix* A, const uint32_t* S, size_
     if (jl)
       rc_jl = launch_jl_project(p->f, jl_seed, jl_rows, S, r, n * d, d, p_out, jl_flat, jl_ws,
                                 jl_scratch_bytes(jl_rows, 0, 0), p->num_sms, p->d_err, lo);
-    // Witness to the evaluation domain once; shared by the commitment and the Gram.
-    rc_chain = launch_ntt(p, MODE_FWD, S, nullptr, s_hat, r * n, hi);
-    // 1. inner commitments t_i = A s_i, then balanced limbs (inner_commit_decomposed)
-    if (!rc_chain)
-      rc_chain = launch_emm(p, s_hat, A->d_evals, (int)r, (int)kappa, (int)n, (int)A->ld,
-                            EMM_DENSE, t, work, hi);
-    if (!rc_chain) rc_chain = launch_ntt(p, MODE_INV, t, nullptr, t, r * kappa, hi);
+    // 1. inner commitments t_i = A s_i and 2. garbage g_ij = <s_i, s_j>, i <= j
+    if (!is_crt(p)) {
+      rc_chain = contract(p, A, S, t, g, hi);
+    } else {
+      for (int j = 0; j < 3 && !rc_chain; ++j) {
+        rc_chain = lift_one(p, j, S, r * n * d, s_hat, hi);
+        if (!rc_chain) rc_chain = contract(p->crt[j], A->crt[j], s_hat, tj[j], gj[j], hi);
+      }
+      if (!rc_chain) rc_chain = crt_combine(p, tj[0], tj[1], tj[2], tw, t, hi);
+      if (!rc_chain) rc_chain = crt_combine(p, gj[0], gj[1], gj[2], gw, g, hi);
+    }
+    // balanced limbs of both (inner_commit_decomposed, decompose_polys)
     if (!rc_chain) rc_chain = launch_decompose_balanced(p, t, r * kappa, b1, t1, t_limbs, hi);
-    // 2. garbage g_ij = <s_i, s_j>, i <= j, then balanced limbs
-    if (!rc_chain)
-      rc_chain = launch_emm(p, s_hat, s_hat, (int)r, (int)r, (int)n, (int)n, EMM_UPPER, g, work,
-                            hi);
-    if (!rc_chain) rc_chain = launch_ntt(p, MODE_INV, g, nullptr, g, r * (r + 1) / 2, hi);
     if (!rc_chain && g_limbs)
       rc_chain = launch_decompose_balanced(p, g, r * (r + 1) / 2, b2, t2, g_limbs, hi);
     // join: the caller's stream waits for both forks (also after a failed launch)

@@ -294,6 +294,7 @@ size_t emm_workspace_words(const grid_gpu_plan* p, int M, int N, int K, int mode
 // out_evals: dense [M][N][d] or packed-upper [M(M+1)/2][d]. work: >= emm_workspace_words.
 int launch_emm(const grid_gpu_plan* p, const uint32_t* X, const uint32_t* Y, int M, int N, int K,
                int ldy, int mode, uint32_t* out_evals, uint32_t* work, cudaStream_t s) {
+  if (is_crt(p)) return p->ntt_status;  // evaluation-domain products need an NTT for q
   if (M <= 0 || N <= 0 || K <= 0) return GRID_OK;
   if (p->d % EG) return GRID_ERR_UNSUPPORTED_DEGREE;
   if (mode == OUT_UPPER && M != N) return GRID_ERR_DIMENSION_MISMATCH;

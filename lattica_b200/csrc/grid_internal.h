@@ -48,6 +48,18 @@ struct DeviceScratch {
   size_t bytes = 0;
 };
 
+// Constants of the exact reconstruction of ring_crt.cu: residues mod the three
+// auxiliary primes -> the Montgomery word mod q.
+struct CrtConsts {
+  uint32_t p[3], pinv[3];   // auxiliary primes, their inverses mod 2^32
+  uint32_t r2_0;            // 2^64 mod p0
+  uint32_t c1a, c1b;        // 2^64 p0^-1, 2^32 p0^-1 (mod p1)
+  uint32_t c2a, c2b, c2c;   // 2^64 (p0 p1)^-1, 2^32 (p0 p1)^-1, 2^32 p1^-1 (mod p2)
+  uint32_t half_p2;         // p2 / 2: the sign threshold of the top mixed-radix digit
+  FieldParams fq;           // the ring's modulus q
+  uint32_t m1, m2, p_rinv;  // p0, p0 p1 (mod q); P 2^-32 (mod q)
+};
+
 }  // namespace grid
 
 struct grid_gpu_plan {
@@ -74,6 +86,11 @@ struct grid_gpu_plan {
   std::mutex mu;                   // serialises host-buffer calls and scratch growth
   grid::DeviceScratch scratch[16];
   int num_sms = 0;
+  // Ring plans for a q without a 2d-th root of unity (ring_crt.cu): ordinary
+  // plans for the three auxiliary primes carry the products; null otherwise.
+  grid_gpu_plan* crt[3] = {nullptr, nullptr, nullptr};
+  grid::CrtConsts crt_c{};
+  int ntt_status = 0;  // what TwistedNttPlan::build reports for (q, d) on a ring plan
 };
 
 struct grid_gpu_matrix {
@@ -82,6 +99,9 @@ struct grid_gpu_matrix {
   size_t ld = 0;                // row stride in polys (cols of the owning matrix)
   uint32_t* d_evals = nullptr;  // rows x ld polys in the twisted evaluation domain
   bool owned = true;            // false for views sharing another matrix's evaluations
+  // On a ring plan without an NTT for q: the matrix's residues mod each
+  // auxiliary prime, prepared on that prime's plan (d_evals stays null).
+  grid_gpu_matrix* crt[3] = {nullptr, nullptr, nullptr};
 };
 
 namespace grid {
@@ -160,6 +180,20 @@ int launch_jl_evals(const FieldParams& f, const uint8_t seed[32], size_t rows,
                     uint32_t* evals, void* scratch, size_t scratch_bytes, int num_sms, int* err,
                     cudaStream_t s);
 
+// ring_crt.cu: exact products for q without a 2d-th root (three auxiliary primes)
+inline bool is_crt(const grid_gpu_plan* p) { return p->crt[0] != nullptr; }
+const uint32_t* crt_moduli();
+void crt_consts(uint32_t q, CrtConsts* c);
+// terms * d * (q - 1)^2 < 2^93: every output coefficient sums at most terms * d
+// word products, within the reconstruction's range
+bool crt_bound_ok(const grid_gpu_plan* p, size_t terms);
+// o_j = x mod p_j (null outputs skipped); words % 4 == 0, 16-byte aligned buffers
+int crt_lift(const grid_gpu_plan* p, const uint32_t* x, size_t words, uint32_t* o0, uint32_t* o1,
+             uint32_t* o2, cudaStream_t s);
+// out = Montgomery word mod q of the integer whose words mod p_j are w_j
+int crt_combine(const grid_gpu_plan* p, const uint32_t* w0, const uint32_t* w1,
+                const uint32_t* w2, size_t words, uint32_t* out, cudaStream_t s);
+
 // plan.cu
 int host_pipeline(grid_gpu_plan* p, const uint32_t* const* ins, int nin, uint32_t* out,
                   size_t nunits, size_t unit_words,
@@ -173,6 +207,33 @@ int cuda_status(cudaError_t e);
 int ensure_scratch(grid_gpu_plan* p, int slot, size_t bytes);
 
 constexpr int kMaxDevices = 64;
+
+inline size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+inline size_t words_bytes(size_t words) { return round_up(words * 4, 256); }
+
+// Bump allocator over a caller workspace (256-byte aligned sub-buffers).
+struct Carver {
+  char* base;
+  size_t cap, used = 0;
+  bool ok = true;
+  Carver(void* b, size_t c) : base(static_cast<char*>(b)), cap(c) {}
+  template <typename T>
+  T* take(size_t count) {
+    if (count > (cap + 1) / sizeof(T)) {  // also keeps count * sizeof(T) from wrapping
+      ok = false;
+      return nullptr;
+    }
+    const size_t bytes = round_up(count * sizeof(T), 256);
+    if (used + bytes > cap || !base) {
+      ok = false;
+      used += bytes;
+      return nullptr;
+    }
+    T* p = reinterpret_cast<T*>(base + used);
+    used += bytes;
+    return p;
+  }
+};
 
 // Sets the dynamic shared-memory limit of `kernel` once per device and caches
 // its resident blocks per SM (idempotent; benign if two threads race).

@@ -690,6 +690,7 @@ int ntt_max_degree() { return (int)kMaxDegree; }
 
 int launch_ntt(const grid_gpu_plan* p, int mode, const uint32_t* a, const uint32_t* b,
                uint32_t* out, size_t npolys, cudaStream_t s) {
+  if (is_crt(p)) return p->ntt_status;  // q has no 2d-th root: no transform exists
   if (npolys == 0) return GRID_OK;
   if (ntt_tc_available(p)) return launch_ntt_tc(p, mode, a, b, out, npolys, s);
   if (mode == MODE_MULINV && ntt256_tc_available(p))
@@ -704,7 +705,7 @@ int launch_ntt(const grid_gpu_plan* p, int mode, const uint32_t* a, const uint32
 
 bool commit_small_fits(const grid_gpu_plan* p, size_t rows, size_t cols, size_t batch) {
   // one CTA per witness re-reads the matrix from L2: keep to small batches
-  return p->d == 64 && rows >= 1 && rows <= (size_t)kSmallMaxRows && cols >= 1 &&
+  return !is_crt(p) && p->d == 64 && rows >= 1 && rows <= (size_t)kSmallMaxRows && cols >= 1 &&
          cols <= (size_t)kSmallMaxCols && batch >= 1 && batch <= 1024;
 }
 

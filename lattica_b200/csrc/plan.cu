@@ -237,18 +237,26 @@ int host_pipeline(grid_gpu_plan* p, const uint32_t* const* ins, int nin, uint32_
   return fin;
 }
 
-// Synchronise `s`, then read and clear the plan's device error word.
+// Synchronise `s`, then read and clear the plan's device error word (and, on
+// a ring plan, those of the auxiliary primes' plans).
 int finish_host_call(grid_gpu_plan* p, cudaStream_t s) {
   cudaError_t e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return cuda_status(e);
   int derr = 0;
   e = cudaMemcpy(&derr, p->d_err, sizeof(int), cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return cuda_status(e);
+  int status = GRID_OK;
   if (derr) {
     cudaMemset(p->d_err, 0, sizeof(int));
-    return derr == GRID_DEV_SAMPLE_SHORT ? GRID_ERR_SAMPLE_EXHAUSTED : GRID_ERR_TIMEOUT;
+    status = derr == GRID_DEV_SAMPLE_SHORT ? GRID_ERR_SAMPLE_EXHAUSTED : GRID_ERR_TIMEOUT;
   }
-  return GRID_OK;
+  // a ring plan's products run on the auxiliary primes' plans: their words too
+  for (grid_gpu_plan* sub : p->crt) {
+    if (!sub) continue;
+    const int sst = grid_gpu_plan_check(sub, s);
+    if (!status) status = sst;
+  }
+  return status;
 }
 
 }  // namespace grid
@@ -277,6 +285,34 @@ int ntt_op_polymul(grid_gpu_plan* p, const uint32_t* const* in, uint32_t* out, s
   int st = launch_ntt(p, MODE_FWD, in[1], nullptr, out, n, s);
   if (st) return st;
   return launch_ntt(p, MODE_MULINV, in[0], out, out, n, s);
+}
+
+size_t crt_poly_words(const grid_gpu_plan* p, size_t npolys) {
+  return round_up(npolys * p->d, 64);  // 256-byte aligned sub-buffers
+}
+
+// Negacyclic products on a ring plan without an NTT for q: per auxiliary
+// prime, lift a and b, transform b, multiply and invert; then reconstruct.
+// scratch: 4 * crt_poly_words words.
+int crt_poly_mul(const grid_gpu_plan* p, const uint32_t* a, const uint32_t* b, uint32_t* out,
+                 uint32_t* scratch, size_t npolys, cudaStream_t s) {
+  if (!crt_bound_ok(p, 1)) return GRID_ERR_INVALID_PARAMETERS;
+  const size_t w = npolys * p->d, stride = crt_poly_words(p, npolys);
+  uint32_t* aj[3] = {scratch, scratch + stride, scratch + 2 * stride};
+  uint32_t* bt = scratch + 3 * stride;
+  int rc = GRID_OK;
+  for (int j = 0; j < 3 && !rc; ++j) {
+    const grid_gpu_plan* sub = p->crt[j];
+    rc = crt_lift(p, a, w, j == 0 ? aj[0] : nullptr, j == 1 ? aj[1] : nullptr,
+                  j == 2 ? aj[2] : nullptr, s);
+    if (!rc)
+      rc = crt_lift(p, b, w, j == 0 ? bt : nullptr, j == 1 ? bt : nullptr, j == 2 ? bt : nullptr,
+                    s);
+    if (!rc) rc = launch_ntt(sub, MODE_FWD, bt, nullptr, bt, npolys, s);
+    if (!rc) rc = launch_ntt(sub, MODE_MULINV, aj[j], bt, aj[j], npolys, s);
+  }
+  if (rc) return rc;
+  return crt_combine(p, aj[0], aj[1], aj[2], w, out, s);
 }
 
 }  // namespace
@@ -319,6 +355,26 @@ namespace {
 bool use_tensor_cores() {
   const char* v = std::getenv("GRID_GPU_NTT_ENGINE");
   return !(v && std::strcmp(v, "cuda_core") == 0);
+}
+
+// Device state every plan owns: SM count, error word, the host-buffer
+// pipeline's streams and the fork streams of *_dev calls (on the current device).
+cudaError_t init_device_state(grid_gpu_plan* p) {
+  cudaError_t e;
+  int sms = 0;
+  if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, p->device)) != cudaSuccess)
+    return e;
+  p->num_sms = sms;
+  if ((e = cudaMalloc(&p->d_err, sizeof(int))) != cudaSuccess) return e;
+  if ((e = cudaMemset(p->d_err, 0, sizeof(int))) != cudaSuccess) return e;
+  if ((e = cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking)) != cudaSuccess) return e;
+  if ((e = cudaStreamCreateWithFlags(&p->stream2, cudaStreamNonBlocking)) != cudaSuccess) return e;
+  int least = 0, greatest = 0;
+  if ((e = cudaDeviceGetStreamPriorityRange(&least, &greatest)) != cudaSuccess) return e;
+  if ((e = cudaStreamCreateWithPriority(&p->fork_hi, cudaStreamNonBlocking, greatest)) !=
+      cudaSuccess)
+    return e;
+  return cudaStreamCreateWithPriority(&p->fork_lo, cudaStreamNonBlocking, least);
 }
 
 // Validation and every host-side table of a plan (no device work).
@@ -414,9 +470,7 @@ int grid_gpu_plan_create(uint64_t q, uint64_t d, grid_gpu_plan** out) {
 
   int status = GRID_OK;
   do {
-    int sms = 0;
-    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) break;
-    p->num_sms = sms;
+    if ((e = init_device_state(p)) != cudaSuccess) break;
     if ((e = cudaMalloc(&p->d_tw, dev_tw.size() * sizeof(uint2))) != cudaSuccess) break;
     if ((e = cudaMemcpy(p->d_tw, dev_tw.data(), dev_tw.size() * sizeof(uint2),
                         cudaMemcpyHostToDevice)) != cudaSuccess) break;
@@ -432,18 +486,6 @@ int grid_gpu_plan_create(uint64_t q, uint64_t d, grid_gpu_plan** out) {
           cudaSuccess)
         break;
     }
-    if ((e = cudaMalloc(&p->d_err, sizeof(int))) != cudaSuccess) break;
-    if ((e = cudaMemset(p->d_err, 0, sizeof(int))) != cudaSuccess) break;
-    if ((e = cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking)) != cudaSuccess) break;
-    if ((e = cudaStreamCreateWithFlags(&p->stream2, cudaStreamNonBlocking)) != cudaSuccess) break;
-    int least = 0, greatest = 0;
-    if ((e = cudaDeviceGetStreamPriorityRange(&least, &greatest)) != cudaSuccess) break;
-    if ((e = cudaStreamCreateWithPriority(&p->fork_hi, cudaStreamNonBlocking, greatest)) !=
-        cudaSuccess)
-      break;
-    if ((e = cudaStreamCreateWithPriority(&p->fork_lo, cudaStreamNonBlocking, least)) !=
-        cudaSuccess)
-      break;
   } while (0);
   if (e != cudaSuccess) status = cuda_status(e);
   if (status) {
@@ -454,8 +496,57 @@ int grid_gpu_plan_create(uint64_t q, uint64_t d, grid_gpu_plan** out) {
   return GRID_OK;
 }
 
+int grid_gpu_ring_plan_create(uint64_t q, uint64_t d, grid_gpu_plan** out) {
+  if (!out) return GRID_ERR_NULL_POINTER;
+  *out = nullptr;
+  int st;
+  {
+    grid_gpu_plan probe;
+    st = fill_plan_host(q, d, &probe);
+  }
+  // An NTT-friendly (q, d) gets the ordinary plan, like the reference's
+  // dispatch in negacyclic_mul_coeffs (algebra/src/poly/ring.rs:79-102).
+  if (st != GRID_ERR_UNSUPPORTED_SIZE && st != GRID_ERR_UNSUPPORTED_TWIST)
+    return st ? st : grid_gpu_plan_create(q, d, out);
+  if (d > kMaxDegree || d < 8) return GRID_ERR_UNSUPPORTED_DEGREE;
+  grid_gpu_plan* p = new (std::nothrow) grid_gpu_plan();
+  if (!p) return GRID_ERR_OUT_OF_MEMORY;
+  HostField hf{q};
+  p->q = (uint32_t)q;
+  p->d = (uint32_t)d;
+  p->log_d = 0;
+  while ((1u << p->log_d) < d) ++p->log_d;
+  crt_consts((uint32_t)q, &p->crt_c);
+  p->f = p->crt_c.fq;
+  p->generator = hf.to_mont(smallest_generator(q));
+  p->ntt_status = st;
+  cudaError_t e = cudaGetDevice(&p->device);
+  if (e == cudaSuccess) e = init_device_state(p);
+  int status = e == cudaSuccess ? GRID_OK : cuda_status(e);
+  for (int j = 0; j < 3 && !status; ++j) status = grid_gpu_plan_create(crt_moduli()[j], d, &p->crt[j]);
+  if (status) {
+    grid_gpu_plan_destroy(p);
+    return status;
+  }
+  *out = p;
+  return GRID_OK;
+}
+
+int grid_gpu_plan_ring_kind(const grid_gpu_plan* p, int* kind, uint32_t* aux_moduli) {
+  if (!p || !kind) return GRID_ERR_NULL_POINTER;
+  *kind = is_crt(p) ? 1 : 0;
+  if (aux_moduli && is_crt(p))
+    for (int j = 0; j < 3; ++j) aux_moduli[j] = p->crt[j]->q;
+  return GRID_OK;
+}
+
 int grid_gpu_plan_destroy(grid_gpu_plan* p) {
   if (!p) return GRID_ERR_NULL_POINTER;
+  for (grid_gpu_plan*& sub : p->crt)
+    if (sub) {
+      grid_gpu_plan_destroy(sub);
+      sub = nullptr;
+    }
   int prev = -1;
   cudaGetDevice(&prev);
   if (prev != p->device) cudaSetDevice(p->device);
@@ -498,6 +589,7 @@ int grid_gpu_plan_get_info(const grid_gpu_plan* p, grid_gpu_plan_info* out) {
 
 int grid_gpu_plan_get_twiddles(const grid_gpu_plan* p, uint32_t* zeta, uint32_t* izeta) {
   if (!p || !zeta || !izeta) return GRID_ERR_NULL_POINTER;
+  if (is_crt(p)) return p->ntt_status;  // no 2d-th root: no twiddles
   std::memcpy(zeta, p->tw.zeta.data(), p->d * sizeof(uint32_t));
   std::memcpy(izeta, p->tw.izeta.data(), p->d * sizeof(uint32_t));
   return GRID_OK;
@@ -510,11 +602,18 @@ int grid_gpu_plan_check(grid_gpu_plan* p, void* stream) {
   int derr = 0;
   e = cudaMemcpy(&derr, p->d_err, sizeof(int), cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return cuda_status(e);
+  int status = GRID_OK;
   if (derr) {
     cudaMemset(p->d_err, 0, sizeof(int));
-    return derr == GRID_DEV_SAMPLE_SHORT ? GRID_ERR_SAMPLE_EXHAUSTED : GRID_ERR_TIMEOUT;
+    status = derr == GRID_DEV_SAMPLE_SHORT ? GRID_ERR_SAMPLE_EXHAUSTED : GRID_ERR_TIMEOUT;
   }
-  return GRID_OK;
+  // a ring plan's products run on the auxiliary primes' plans: their words too
+  for (grid_gpu_plan* sub : p->crt) {
+    if (!sub) continue;
+    const int sst = grid_gpu_plan_check(sub, stream);
+    if (!status) status = sst;
+  }
+  return status;
 }
 
 int grid_gpu_ntt_forward_dev(const grid_gpu_plan* p, uint32_t* polys, size_t npolys,
@@ -539,12 +638,18 @@ int grid_gpu_ntt_mul_inverse_dev(const grid_gpu_plan* p, const uint32_t* a,
   return launch_ntt(p, MODE_MULINV, a, b_evals, out, npolys, (cudaStream_t)stream);
 }
 
+size_t grid_gpu_poly_mul_scratch_words(const grid_gpu_plan* p, size_t npolys) {
+  if (!p) return 0;
+  return is_crt(p) ? 4 * crt_poly_words(p, npolys) : npolys * p->d;
+}
+
 int grid_gpu_poly_mul_dev(const grid_gpu_plan* p, const uint32_t* a, const uint32_t* b,
                           uint32_t* out, uint32_t* b_scratch, size_t npolys, void* stream) {
   if (!p || ((!a || !b || !out || !b_scratch) && npolys)) return GRID_ERR_NULL_POINTER;
   if (!aligned16(a) || !aligned16(b) || !aligned16(out) || !aligned16(b_scratch))
     return GRID_ERR_MISALIGNED;
   cudaStream_t s = (cudaStream_t)stream;
+  if (is_crt(p)) return npolys ? crt_poly_mul(p, a, b, out, b_scratch, npolys, s) : GRID_OK;
   int st = launch_ntt(p, MODE_FWD, b, nullptr, b_scratch, npolys, s);
   if (st) return st;
   return launch_ntt(p, MODE_MULINV, a, b_scratch, out, npolys, s);
@@ -582,6 +687,26 @@ int grid_gpu_poly_mul(grid_gpu_plan* p, const uint32_t* a, const uint32_t* b, ui
                       size_t npolys) {
   if (!p || ((!a || !b || !out) && npolys)) return GRID_ERR_NULL_POINTER;
   std::lock_guard<std::mutex> lk(p->mu);
+  if (is_crt(p)) {
+    if (npolys == 0) return GRID_OK;
+    const size_t bytes = npolys * p->d * 4;
+    const size_t sbytes = grid_gpu_poly_mul_scratch_words(p, npolys) * 4;
+    int rc;
+    if ((rc = ensure_scratch(p, 6, bytes)) || (rc = ensure_scratch(p, 7, bytes)) ||
+        (rc = ensure_scratch(p, 8, bytes)) || (rc = ensure_scratch(p, 9, sbytes)))
+      return rc;
+    cudaStream_t st = p->stream;
+    uint32_t* da = static_cast<uint32_t*>(p->scratch[6].ptr);
+    uint32_t* db = static_cast<uint32_t*>(p->scratch[7].ptr);
+    uint32_t* dout = static_cast<uint32_t*>(p->scratch[8].ptr);
+    rc = cuda_status(cudaMemcpyAsync(da, a, bytes, cudaMemcpyHostToDevice, st));
+    if (!rc) rc = cuda_status(cudaMemcpyAsync(db, b, bytes, cudaMemcpyHostToDevice, st));
+    if (!rc)
+      rc = crt_poly_mul(p, da, db, dout, static_cast<uint32_t*>(p->scratch[9].ptr), npolys, st);
+    if (!rc) rc = cuda_status(cudaMemcpyAsync(out, dout, bytes, cudaMemcpyDeviceToHost, st));
+    const int fin = finish_host_call(p, st);
+    return rc ? rc : fin;
+  }
   const uint32_t* ins[2] = {a, b};
   return host_pipeline(p, ins, 2, out, npolys, p->d, ntt_op_polymul, nullptr);
 }

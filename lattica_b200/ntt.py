@@ -86,11 +86,13 @@ class TwistedNttPlan:
     """Twisted negacyclic NTT of length d over Z_q (TwistedNttPlan::build,
     algebra/src/poly/ntt.rs:139-154); owns device twiddles and scratch."""
 
+    _create = "grid_gpu_plan_create"
+
     def __init__(self, q: int, d: int):
         lib = _lib.load()
         handle = C.c_void_p()
-        st = lib.grid_gpu_plan_create(int(q), int(d), C.byref(handle))
-        raise_status(st, "grid_gpu_plan_create", length=int(d))
+        st = getattr(lib, self._create)(int(q), int(d), C.byref(handle))
+        raise_status(st, self._create, length=int(d))
         self._h = handle
         self._lib = lib
         self.q, self.d = int(q), int(d)
@@ -190,7 +192,8 @@ class TwistedNttPlan:
         n = self._npolys(lhs)
         if _is_torch(lhs):
             import torch
-            scratch = torch.empty_like(rhs)
+            words = self._lib.grid_gpu_poly_mul_scratch_words(self._h, n)
+            scratch = torch.empty(max(4, words), dtype=torch.int32, device=lhs.device)
             st = self._lib.grid_gpu_poly_mul_dev(self._h, lhs.data_ptr(), rhs.data_ptr(),
                                                  lhs.data_ptr(), scratch.data_ptr(), n,
                                                  _stream_ptr(lhs))
@@ -244,6 +247,25 @@ class TwistedNttPlan:
                                                         n, out.data_ptr(), s),
                      "grid_gpu_dot_product_dev")
         return int(out[0].item()) & 0xFFFFFFFF
+
+
+class RingPlan(TwistedNttPlan):
+    """Arithmetic of CyclotomicPolyRing<PrimeField<q>, d>, whatever q: the NTT
+    plan when q has a 2d-th root of unity, else exact products through three
+    auxiliary NTT primes with the schoolbook rule's words
+    (NegacyclicMulRing::negacyclic_mul_coeffs, algebra/src/poly/ring.rs:60-100).
+    Every ring-level call of this package accepts it in place of a
+    TwistedNttPlan; NTT calls on a plan without an NTT for q raise the NttError
+    TwistedNttPlan::build would."""
+
+    _create = "grid_gpu_ring_plan_create"
+
+    @property
+    def uses_aux_primes(self) -> bool:
+        kind = C.c_int()
+        raise_status(self._lib.grid_gpu_plan_ring_kind(self._h, C.byref(kind), None),
+                     "grid_gpu_plan_ring_kind")
+        return kind.value == 1
 
 
 _PLANS: dict = {}

@@ -381,7 +381,7 @@ void orc_poly_mul_ntt(const orc_plan *p, const uint32_t *a, const uint32_t *b, u
     free(tmp);
 }
 
-/* neg_cyclic_mul, poly/ring.rs:88-105 */
+/* neg_cyclic_mul, poly/ring.rs:60-77 */
 void orc_naive_negacyclic(const orc_field *f, uint32_t n, const uint32_t *a, const uint32_t *b,
                           uint32_t *out) {
     for (uint32_t i = 0; i < n; i++) out[i] = 0;

@@ -94,7 +94,7 @@ int orc_matvec_avx2(const orc_plan *p, const uint32_t *A, size_t rows, size_t co
                     int a_is_eval, const uint32_t *s, size_t batch, uint32_t *t, int threads);
 /* Negacyclic product via twisted NTT (poly/ntt.rs:110-126). */
 void orc_poly_mul_ntt(const orc_plan *p, const uint32_t *a, const uint32_t *b, uint32_t *out);
-/* Schoolbook negacyclic product (poly/ring.rs:88-105). */
+/* Schoolbook negacyclic product (poly/ring.rs:60-77). */
 void orc_naive_negacyclic(const orc_field *f, uint32_t n, const uint32_t *a, const uint32_t *b,
                           uint32_t *out);
 void orc_pointwise_mul(const orc_field *f, uint32_t *dst, const uint32_t *rhs, size_t len);
@@ -138,7 +138,7 @@ int orc_garbage_h(const orc_plan *p, const uint32_t *S, const uint32_t *Phi, siz
                   uint32_t *H);
 int orc_amortize(const orc_plan *p, const uint32_t *S, const uint32_t *c, size_t r, size_t n,
                  uint32_t *Z);
-/* Slow faithful path: one full negacyclic product per term (poly/ring.rs:111-129). */
+/* Slow faithful path: one full negacyclic product per term (poly/ring.rs:226-228). */
 int orc_gram_naive(const orc_plan *p, const uint32_t *S, size_t r, size_t n, uint32_t *G);
 size_t orc_garbage_index(size_t r, size_t i, size_t j);
 

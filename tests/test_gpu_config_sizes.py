@@ -31,8 +31,9 @@ def _host(t):
 
 
 def _mont(q, values):
-    v = np.asarray(values, dtype=np.int64) % q
-    return ((v.astype(object) << 32) % q).astype(np.uint64).astype(np.uint32)
+    """Signed integers -> Montgomery words v * 2^32 mod q (two exact 16-bit steps)."""
+    v = (np.asarray(values, dtype=np.int64) % q).astype(np.uint64)
+    return ((v * np.uint64(1 << 16)) % np.uint64(q) * np.uint64(1 << 16) % np.uint64(q)).astype(np.uint32)
 
 
 def test_prover_round_at_round_size_matches_oracle(cuda, oracle):

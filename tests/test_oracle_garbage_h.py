@@ -1,6 +1,6 @@
 """Pin the oracle's garbage h and amortization (CPU only) against the
 reference's definitions restated with one naive negacyclic product per term
-(poly/ring.rs:111-129), and against the reference tests' properties: zero phi
+(poly/ring.rs:226-228), and against the reference tests' properties: zero phi
 gives zero h (garbage.rs test_garbage_h_zero_phi), zero witness gives zero z
 (amortization.rs test_amortization_zero_witness), and x 2^-1 2 = x
 (test_garbage_division_by_2)."""
