@@ -171,6 +171,17 @@ int grid_gpu_add_assign_scaled_dev(const grid_gpu_plan* plan, uint32_t* dst, con
                                    uint32_t scalar, size_t nwords, void* stream);
 int grid_gpu_dot_product_dev(const grid_gpu_plan* plan, const uint32_t* lhs, const uint32_t* rhs,
                              size_t nwords, uint32_t* out, void* stream);
+/* The reference's default limb: PrimeField<Q> = PrimeField<Q, u64> stores
+ * value * 2^64 mod q in a u64 (algebra/src/arith/prime.rs:24-29); this library
+ * computes on u32 words value * 2^32 mod q. A u64 caller converts at the
+ * boundary (HBM-bound, 12 bytes per word): from_u64 maps each canonical u64 word
+ * to its u32 word and sets *noncanonical (device int, optional) to 1 if a word
+ * was >= q; to_u64 maps u32 words back. Outputs equal the u64 words the
+ * reference's arithmetic produces. */
+int grid_gpu_words_from_u64_dev(const grid_gpu_plan* plan, const uint64_t* in, size_t nwords,
+                                uint32_t* out, int* noncanonical, void* stream);
+int grid_gpu_words_to_u64_dev(const grid_gpu_plan* plan, const uint32_t* in, size_t nwords,
+                              uint64_t* out, void* stream);
 
 int grid_gpu_ntt_forward(grid_gpu_plan* plan, uint32_t* polys, size_t npolys);
 int grid_gpu_ntt_inverse(grid_gpu_plan* plan, uint32_t* polys, size_t npolys);

@@ -65,6 +65,8 @@ SIGNATURES = {
     "grid_gpu_scalar_mul_dev": (C.c_int, [_vp, _vp, C.c_uint32, C.c_size_t, _vp]),
     "grid_gpu_add_assign_scaled_dev": (C.c_int, [_vp, _vp, _vp, C.c_uint32, C.c_size_t, _vp]),
     "grid_gpu_dot_product_dev": (C.c_int, [_vp, _vp, _vp, C.c_size_t, _vp, _vp]),
+    "grid_gpu_words_from_u64_dev": (C.c_int, [_vp, _vp, C.c_size_t, _vp, _vp, _vp]),
+    "grid_gpu_words_to_u64_dev": (C.c_int, [_vp, _vp, C.c_size_t, _vp, _vp]),
     "grid_gpu_ntt_forward": (C.c_int, [_vp, _vp, C.c_size_t]),
     "grid_gpu_ntt_inverse": (C.c_int, [_vp, _vp, C.c_size_t]),
     "grid_gpu_ntt_mul_inverse": (C.c_int, [_vp, _vp, _vp, _vp, C.c_size_t]),

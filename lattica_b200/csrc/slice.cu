@@ -74,6 +74,26 @@ __global__ void __launch_bounds__(kDotThreads)
   if (threadIdx.x == 0) *out = part[0];
 }
 
+// PrimeField<Q, u64> words (value * 2^64 mod q, the reference's default limb,
+// algebra/src/arith/prime.rs:24-29) <-> the u32 words of this library
+// (value * 2^32 mod q): one Montgomery product by 1, or by 2^64 mod q.
+__global__ void from_u64_kernel(const uint64_t* __restrict__ in, size_t n,
+                                uint32_t* __restrict__ out, int* __restrict__ bad, FieldParams f) {
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const uint64_t w = in[i];
+    if (bad && w >= f.q) atomicExch(bad, 1);  // not a canonical word: its output is meaningless
+    out[i] = mont_mul((uint32_t)w, 1u, f.q, f.qinv);
+  }
+}
+
+__global__ void to_u64_kernel(const uint32_t* __restrict__ in, size_t n,
+                              uint64_t* __restrict__ out, FieldParams f) {
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+    out[i] = mont_mul(in[i], f.r2, f.q, f.qinv);
+}
+
 template <int OP>
 int launch_slice(const grid_gpu_plan* p, uint32_t* dst, const uint32_t* src, uint32_t c,
                  size_t n, cudaStream_t s) {
@@ -128,6 +148,35 @@ int grid_gpu_dot_product_dev(const grid_gpu_plan* p, const uint32_t* lhs, const 
   // each thread's 96-bit accumulator holds at most 2^32 products
   if (nwords > (size_t)kDotThreads << 32) return GRID_ERR_INVALID_PARAMETERS;
   dot_kernel<<<1, kDotThreads, 0, (cudaStream_t)stream>>>(lhs, rhs, nwords, out, p->f);
+  return cuda_status(cudaGetLastError());
+}
+
+int grid_gpu_words_from_u64_dev(const grid_gpu_plan* p, const uint64_t* in, size_t nwords,
+                                uint32_t* out, int* noncanonical, void* stream) {
+  if (!p || ((!in || !out) && nwords)) return GRID_ERR_NULL_POINTER;
+  if (!words_ok(nwords)) return GRID_ERR_INVALID_PARAMETERS;
+  if (nwords == 0) return GRID_OK;
+  if (noncanonical) {
+    const cudaError_t e = cudaMemsetAsync(noncanonical, 0, sizeof(int), (cudaStream_t)stream);
+    if (e != cudaSuccess) return cuda_status(e);
+  }
+  size_t blocks = (nwords + 255) / 256;
+  const size_t cap = (size_t)p->num_sms * 8;
+  if (blocks > cap) blocks = cap;
+  from_u64_kernel<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(
+      in, nwords, out, noncanonical, p->f);
+  return cuda_status(cudaGetLastError());
+}
+
+int grid_gpu_words_to_u64_dev(const grid_gpu_plan* p, const uint32_t* in, size_t nwords,
+                              uint64_t* out, void* stream) {
+  if (!p || ((!in || !out) && nwords)) return GRID_ERR_NULL_POINTER;
+  if (!words_ok(nwords)) return GRID_ERR_INVALID_PARAMETERS;
+  if (nwords == 0) return GRID_OK;
+  size_t blocks = (nwords + 255) / 256;
+  const size_t cap = (size_t)p->num_sms * 8;
+  if (blocks > cap) blocks = cap;
+  to_u64_kernel<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(in, nwords, out, p->f);
   return cuda_status(cudaGetLastError());
 }
 

@@ -239,6 +239,33 @@ class TwistedNttPlan:
             self._h, dst.data_ptr(), src.data_ptr(), int(scalar), n, s),
             "grid_gpu_add_assign_scaled_dev")
 
+    # -- PrimeField<Q, u64> words (value * 2^64 mod q, the reference's default
+    #    limb) to and from this library's u32 words, on CUDA tensors
+    def words_from_u64(self, w64):
+        """int64 tensor of u64 Montgomery words -> int32 tensor of u32 words;
+        raises ValueError if a word is not canonical (>= q)."""
+        import torch
+        if w64.dtype not in (torch.int64, torch.uint64) or not w64.is_cuda or not w64.is_contiguous():
+            raise TypeError("expected a contiguous CUDA tensor of 64-bit words")
+        out = torch.empty(w64.shape, dtype=torch.int32, device=w64.device)
+        flag = torch.zeros(4, dtype=torch.int32, device=w64.device)
+        raise_status(self._lib.grid_gpu_words_from_u64_dev(
+            self._h, w64.data_ptr(), w64.numel(), out.data_ptr(), flag.data_ptr(),
+            _stream_ptr(w64)), "grid_gpu_words_from_u64_dev")
+        if int(flag[0].item()):
+            raise ValueError("a u64 word is not canonical (>= q)")
+        return out
+
+    def words_to_u64(self, w32):
+        """int32 tensor of u32 words -> int64 tensor of u64 Montgomery words."""
+        import torch
+        _dev_u32(w32)
+        out = torch.empty(w32.shape, dtype=torch.int64, device=w32.device)
+        raise_status(self._lib.grid_gpu_words_to_u64_dev(
+            self._h, w32.data_ptr(), w32.numel(), out.data_ptr(), _stream_ptr(w32)),
+            "grid_gpu_words_to_u64_dev")
+        return out
+
     def dot_product(self, lhs, rhs) -> int:
         import torch
         n, s = self._slice_args(lhs, rhs)
