@@ -333,7 +333,8 @@ int grid_gpu_gadget_decompose(grid_gpu_plan* plan, const uint32_t* x, size_t len
 
 /* ---- uneven batched commitments: many AjtaiCommitmentScheme::commit calls
  *      (commit/src/ajtai/mod.rs:429-441) of different lengths in one launch
- *      sequence (NTT of all witnesses, one persistent grouped matmul, INTT) --
+ *      sequence (NTT of all witnesses, the persistent grouped product on the
+ *      tensor cores, one launch per tile class, then fold and INTT) --
  * Instance i commits s_i (n polys starting at poly s_offset of the packed
  * witness buffer) with the first n columns of matrix `matrix` (rows <= 32)
  * and writes rows polys starting at poly t_offset of the packed output. */
@@ -344,10 +345,18 @@ typedef struct grid_gpu_batch_item {
   uint32_t n;
   uint32_t matrix;
 } grid_gpu_batch_item;
+/* Engines of the grouped product: AUTO = the tensor cores where the plan
+ * allows (d % 4 == 0, tensor-core plan), else the CUDA cores; TENSOR requires
+ * them (else GRID_ERR_UNSUPPORTED_DEGREE); CUDA_CORE never uses them. Both give
+ * the same words. */
+enum { GRID_GPU_ENGINE_AUTO = 0, GRID_GPU_ENGINE_TENSOR = 1, GRID_GPU_ENGINE_CUDA_CORE = 2 };
 typedef struct grid_gpu_batch_config {
-  uint32_t k_split;     /* K range of one work item (multiple of 16); set by the autotuner */
-  uint32_t work_items;  /* output of get_config */
-  uint32_t tiles;       /* output of get_config */
+  uint32_t k_split;        /* K range of one work item (multiple of 16, <= 8192) */
+  uint32_t work_items;     /* output of get_config */
+  uint32_t tiles;          /* output of get_config */
+  uint32_t tile_instances; /* instances per tile (multiple of 4, <= 128); 0: the engine's */
+  uint32_t engine;         /* GRID_GPU_ENGINE_* */
+  uint32_t tensor_cores;   /* output of get_config: 1 if the grouped product runs on them */
 } grid_gpu_batch_config;
 int grid_gpu_batch_create(grid_gpu_plan* plan, grid_gpu_matrix* const* mats, size_t nmats,
                           const grid_gpu_batch_item* items, size_t nitems, grid_gpu_batch** out);
@@ -375,6 +384,26 @@ int grid_gpu_batch_commit_oneshot_dev(grid_gpu_plan* plan, grid_gpu_matrix* cons
                                       size_t nitems, uint32_t k_split, const uint32_t* s,
                                       uint32_t* t, void* workspace, size_t workspace_bytes,
                                       void* stream);
+
+/* ---- batched Gram matrices: compute_garbage_g (labrador/src/main_protocol/
+ *      garbage.rs:76-93) for many witnesses of different rank r <= 64 and
+ *      length n in one launch sequence (the witnesses' transforms, one
+ *      persistent grouped tensor-core product per tile class, one fold, one
+ *      inverse transform). Item i's witness is r x n polys at poly s_offset of S;
+ *      its r(r+1)/2 Gram polys (garbage_index order) follow item i-1's in G.
+ *      k_split: K words per work item (0: chosen from the batch's size). On a
+ *      plan without tensor-core products the items run one grid_gpu_gram_dev
+ *      after another in the same workspace. ---------------------------------- */
+typedef struct grid_gpu_gram_item {
+  uint64_t s_offset;
+  uint32_t r;
+  uint32_t n;
+} grid_gpu_gram_item;
+int grid_gpu_batch_gram_workspace(const grid_gpu_plan* plan, const grid_gpu_gram_item* items,
+                                  size_t nitems, uint32_t k_split, size_t* bytes);
+int grid_gpu_batch_gram_dev(const grid_gpu_plan* plan, const uint32_t* S,
+                            const grid_gpu_gram_item* items, size_t nitems, uint32_t k_split,
+                            uint32_t* G, void* workspace, size_t workspace_bytes, void* stream);
 
 /* ---- Gram matrix without allocation (no counterpart in the reference) ----
  * Same result as grid_gpu_gram_dev, for callers that cannot allocate device

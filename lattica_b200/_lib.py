@@ -31,7 +31,16 @@ class BatchItem(C.Structure):
 
 
 class BatchConfig(C.Structure):
-    _fields_ = [("k_split", C.c_uint32), ("work_items", C.c_uint32), ("tiles", C.c_uint32)]
+    _fields_ = [("k_split", C.c_uint32), ("work_items", C.c_uint32), ("tiles", C.c_uint32),
+                ("tile_instances", C.c_uint32), ("engine", C.c_uint32),
+                ("tensor_cores", C.c_uint32)]
+
+
+class GramItem(C.Structure):
+    _fields_ = [("s_offset", C.c_uint64), ("r", C.c_uint32), ("n", C.c_uint32)]
+
+
+ENGINE_AUTO, ENGINE_TENSOR, ENGINE_CUDA_CORE = 0, 1, 2
 
 
 class PlanInfo(C.Structure):
@@ -142,6 +151,10 @@ SIGNATURES = {
                                                    C.c_uint32, C.POINTER(C.c_size_t)]),
     "grid_gpu_batch_commit_oneshot_dev": (C.c_int, [_vp, _vp, C.c_size_t, _vp, C.c_size_t,
                                                     C.c_uint32, _vp, _vp, _vp, C.c_size_t, _vp]),
+    "grid_gpu_batch_gram_workspace": (C.c_int, [_vp, _vp, C.c_size_t, C.c_uint32,
+                                                C.POINTER(C.c_size_t)]),
+    "grid_gpu_batch_gram_dev": (C.c_int, [_vp, _vp, _vp, C.c_size_t, C.c_uint32, _vp, _vp,
+                                          C.c_size_t, _vp]),
     "grid_gpu_noalloc_scratch_bytes": (C.c_size_t, []),
     "grid_gpu_gram_noalloc_dev": (C.c_int, [_vp, _vp, C.c_size_t, C.c_size_t, _vp, _vp]),
     "grid_gpu_host_register": (C.c_int, [_vp, C.c_size_t]),

@@ -2,11 +2,13 @@
 
 `UnevenCommitBatch` runs many Ajtai commitments t_i = A_{m_i}[:, :n_i] s_i of
 different lengths n_i and matrices in one launch sequence (one NTT of all
-witnesses, one persistent grouped evaluation-domain matmul, one INTT),
-optionally captured once into a CUDA graph and replayed. Its only schedule
-parameter, the K range of a work item, is picked by `autotune`, which times
-the candidates on the actual batch with CUDA events and persists the winner in
-a JSON file keyed by the batch's shape signature.
+witnesses, the persistent grouped evaluation-domain product on the tensor
+cores, one INTT), optionally captured once into a CUDA graph and replayed. Its
+schedule — the engine (tensor cores or CUDA cores), the instances per tile (the
+tile shape: 32, 64 or 128 rows of the product) and the K range of a work item —
+is picked by `autotune`, which times the candidates on the actual batch with
+CUDA events and persists the winner in a JSON file keyed by the batch's shape
+signature.
 
 The per-call path (`per_call_commit`) issues one C-ABI commit per instance
 through column views of the same prepared matrices; it is the plain GPU path
@@ -26,7 +28,10 @@ from . import _lib
 from .commit import PreparedMatrix
 from .ntt import TwistedNttPlan, _stream_ptr, raise_status
 
-K_SPLIT_CANDIDATES = (256, 512, 1024, 2048, 4096, 8192)
+K_SPLIT_CANDIDATES = (1024, 2048, 4096, 8192)
+TILE_CANDIDATES = (0, 64, 32)  # instances per tile (0: the engine's largest, 128)
+ENGINE_NAMES = {_lib.ENGINE_AUTO: "auto", _lib.ENGINE_TENSOR: "tensor",
+                _lib.ENGINE_CUDA_CORE: "cuda_core"}
 
 
 def default_cache_path() -> str:
@@ -75,11 +80,19 @@ class UnevenCommitBatch:
     def config(self) -> dict:
         c = _lib.BatchConfig()
         raise_status(self._lib.grid_gpu_batch_get_config(self._h, C.byref(c)), "get_config")
-        return {"k_split": c.k_split, "work_items": c.work_items, "tiles": c.tiles}
+        return {"k_split": c.k_split, "work_items": c.work_items, "tiles": c.tiles,
+                "tile_instances": c.tile_instances, "engine": ENGINE_NAMES[c.engine],
+                "tensor_cores": bool(c.tensor_cores)}
+
+    def set_config(self, k_split: int, tile_instances: int = 0,
+                   engine: int = _lib.ENGINE_AUTO) -> None:
+        c = _lib.BatchConfig(int(k_split), 0, 0, int(tile_instances), int(engine), 0)
+        raise_status(self._lib.grid_gpu_batch_set_config(self._h, C.byref(c)), "set_config")
 
     def set_k_split(self, k_split: int) -> None:
-        c = _lib.BatchConfig(int(k_split), 0, 0)
-        raise_status(self._lib.grid_gpu_batch_set_config(self._h, C.byref(c)), "set_config")
+        cur = _lib.BatchConfig()
+        raise_status(self._lib.grid_gpu_batch_get_config(self._h, C.byref(cur)), "get_config")
+        self.set_config(k_split, cur.tile_instances, cur.engine)
 
     def signature(self) -> str:
         """Shape signature: matrix shapes plus a log2 histogram of lengths per matrix."""
@@ -109,9 +122,18 @@ class UnevenCommitBatch:
         raise_status(st, "grid_gpu_batch_commit")
         return t
 
-    def autotune(self, s, t, candidates=K_SPLIT_CANDIDATES, reps: int = 3,
+    def schedules(self, k_splits=K_SPLIT_CANDIDATES):
+        """Candidate schedules (k_split, tile_instances, engine): tile shapes on
+        the tensor cores, and the CUDA-core kernel with its own tiles."""
+        out = [(k, ti, _lib.ENGINE_TENSOR) for ti in TILE_CANDIDATES for k in k_splits]
+        out += [(k, 0, _lib.ENGINE_CUDA_CORE) for k in k_splits]
+        return out
+
+    def autotune(self, s, t, candidates=None, reps: int = 3,
                  cache_path: str | None = None, use_cache: bool = True) -> dict:
-        """Time each k_split candidate on this batch and keep the fastest."""
+        """Time each schedule candidate on this batch and keep the fastest.
+        candidates: schedules (k_split, tile_instances, engine), or plain k_split
+        values (the current tiles and engine); default: schedules()."""
         import torch
         path = cache_path or default_cache_path()
         sig = self.signature()
@@ -122,13 +144,22 @@ class UnevenCommitBatch:
                     cache = json.load(fh)
             except (OSError, ValueError):
                 cache = {}
-        if use_cache and sig in cache:
-            self.set_k_split(cache[sig]["k_split"])
+        if use_cache and sig in cache and "schedule" in cache[sig]:
+            self.set_config(*cache[sig]["schedule"])
             return dict(cache[sig], cached=True)
         stream = torch.cuda.current_stream(s.device)
+        cur = self.config()
+        engine_now = {v: k for k, v in ENGINE_NAMES.items()}[cur["engine"]]
+        if candidates is None:
+            candidates = self.schedules()
+        candidates = [tuple(c) if isinstance(c, (tuple, list))
+                      else (int(c), cur["tile_instances"], engine_now) for c in candidates]
         results = {}
         for k in candidates:
-            self.set_k_split(k)
+            try:
+                self.set_config(*k)
+            except Exception:  # e.g. no tensor-core products on this plan
+                continue
             self.commit_dev(s, t)
             times = []
             for _ in range(reps):
@@ -141,9 +172,11 @@ class UnevenCommitBatch:
                 times.append(e0.elapsed_time(e1))
             results[k] = min(times)
         best = min(results, key=results.get)
-        self.set_k_split(best)
-        entry = {"k_split": best, "ms": results[best],
-                 "candidates_ms": {str(k): v for k, v in results.items()}}
+        self.set_config(*best)
+        entry = {"schedule": list(best), "k_split": best[0], "tile_instances": best[1],
+                 "engine": ENGINE_NAMES[best[2]], "ms": results[best],
+                 "candidates_ms": {"%d/%d/%s" % (k[0], k[1], ENGINE_NAMES[k[2]]): v
+                                   for k, v in results.items()}}
         cache[sig] = entry
         try:
             os.makedirs(os.path.dirname(path), exist_ok=True)

@@ -24,8 +24,10 @@
 #include <mutex>
 #include <new>
 #include <tuple>
+#include <type_traits>
 #include <vector>
 
+#include "batch_tables.cuh"
 #include "grid_async.cuh"
 #include "grid_field.cuh"
 #include "grid_internal.h"
@@ -54,20 +56,6 @@ constexpr size_t kBatchSmem = std::max({BTile<8>::SMEM, BTile<16>::SMEM, BTile<3
 
 __host__ __device__ constexpr int tile_tmg(uint32_t rows) { return rows <= 8 ? 32 : rows <= 16 ? 16 : 8; }
 
-struct MatDev {
-  const uint32_t* evals;
-  uint32_t rows, ld;  // ld: row stride in polys
-};
-struct ItemDev {
-  unsigned long long s_off, t_off;
-  uint32_t n, pad;
-};
-struct TileDev {
-  uint32_t first, count, matrix, kmax;  // count <= 4 * tile_tmg(rows of the matrix)
-};
-struct WorkDev {
-  uint32_t tile, k0, k1, eg;
-};
 
 // One work item (a tile, evaluation points 8 eg .. + 7, K steps k0 .. k1) with
 // tile shape TMG: operands stream through a cp.async ring (instances' witness
@@ -208,11 +196,17 @@ using namespace grid;
 
 struct grid_gpu_batch {
   grid_gpu_plan* plan = nullptr;
+  std::vector<grid_gpu_matrix*> mat_handles;
+  std::vector<grid_gpu_batch_item> items;  // as given (tiles are rebuilt on a new config)
   std::vector<MatDev> mats;
   std::vector<ItemDev> sorted;    // items grouped by matrix, longest first
   std::vector<TileDev> tiles;
   uint64_t s_polys = 0, t_polys = 0;
   uint32_t k_split = 1024;
+  uint32_t tile_instances = 0;    // 0: the engine's default
+  int engine = GRID_GPU_ENGINE_AUTO;
+  bool tc = false;                // the tensor-core kernel runs the grouped product
+  unsigned class_begin[TC_CLASSES + 1] = {};
   // device tables
   MatDev* d_mats = nullptr;
   ItemDev* d_items = nullptr;
@@ -227,84 +221,6 @@ struct grid_gpu_batch {
 
 namespace {
 
-std::vector<WorkDev> make_work(const std::vector<TileDev>& tiles, uint32_t groups,
-                               uint32_t k_split) {
-  std::vector<WorkDev> work;
-  for (uint32_t ti = 0; ti < tiles.size(); ++ti) {
-    const TileDev& tl = tiles[ti];
-    for (uint32_t k0 = 0; k0 < tl.kmax; k0 += k_split) {
-      const uint32_t k1 = std::min(tl.kmax, k0 + k_split);
-      for (uint32_t g = 0; g < groups; ++g) work.push_back(WorkDev{ti, k0, k1, g});
-    }
-  }
-  // Longest K ranges first (every tile shape carries 1024 outputs per K step).
-  std::stable_sort(work.begin(), work.end(), [](const WorkDev& x, const WorkDev& y) {
-    return (x.k1 - x.k0) > (y.k1 - y.k0);
-  });
-  return work;
-}
-
-int rebuild_work(grid_gpu_batch* b) {
-  const std::vector<WorkDev> work = make_work(b->tiles, b->plan->d / EG, b->k_split);
-  if (b->d_work) cudaFree(b->d_work);
-  b->d_work = nullptr;
-  b->nwork = (unsigned)work.size();
-  for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
-  b->graphs.clear();
-  if (work.empty()) return GRID_OK;
-  cudaError_t e = cudaMalloc(&b->d_work, work.size() * sizeof(WorkDev));
-  if (e == cudaSuccess)
-    e = cudaMemcpy(b->d_work, work.data(), work.size() * sizeof(WorkDev), cudaMemcpyHostToDevice);
-  return cuda_status(e);
-}
-
-size_t ws_bytes(const grid_gpu_batch* b) {
-  const size_t d = b->plan->d;
-  return round_up(b->s_polys * d * 4, 256) + round_up(b->t_polys * d * 8, 256) + 256;
-}
-
-// NTT(s) -> grouped matmul -> fold -> INTT(t), with device tables given.
-int run_core(const grid_gpu_plan* p, const MatDev* d_mats, const ItemDev* d_items,
-             const TileDev* d_tiles, const WorkDev* d_work, unsigned nwork, uint64_t s_polys,
-             uint64_t t_polys, const uint32_t* s, uint32_t* t, void* ws, cudaStream_t st) {
-  const size_t d = p->d;
-  char* base = static_cast<char*>(ws);
-  uint32_t* s_hat = reinterpret_cast<uint32_t*>(base);
-  unsigned long long* acc =
-      reinterpret_cast<unsigned long long*>(base + round_up(s_polys * d * 4, 256));
-  unsigned* counter = reinterpret_cast<unsigned*>(base + round_up(s_polys * d * 4, 256) +
-                                                  round_up(t_polys * d * 8, 256));
-  int rc = launch_ntt(p, MODE_FWD, s, nullptr, s_hat, s_polys, st);
-  if (rc) return rc;
-  cudaError_t e = cudaMemsetAsync(acc, 0, t_polys * d * 8, st);
-  if (e == cudaSuccess) e = cudaMemsetAsync(counter, 0, sizeof(unsigned), st);
-  if (e != cudaSuccess) return cuda_status(e);
-  if (nwork) {
-    static int bps_cache[kMaxDevices] = {};
-    int bps = 0;
-    rc = prepare_kernel(batch_emm_kernel, kBatchSmem, kThreads, p->device, bps_cache, &bps);
-    if (rc) return rc;
-    const unsigned grid = std::min<unsigned>(nwork, (unsigned)(p->num_sms * bps));
-    batch_emm_kernel<<<grid, kThreads, kBatchSmem, st>>>(d_work, nwork, d_tiles, d_items, d_mats, s_hat,
-                                                 acc, counter, (int)d, p->f);
-    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(e);
-  }
-  const size_t words = t_polys * d;
-  unsigned blocks = (unsigned)std::min<size_t>((words + 255) / 256, (size_t)p->num_sms * 8);
-  fold_kernel<<<blocks ? blocks : 1, 256, 0, st>>>(acc, t, words, p->f.q);
-  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(e);
-  return launch_ntt(p, MODE_INV, t, nullptr, t, t_polys, st);
-}
-
-int run_sequence(grid_gpu_batch* b, const uint32_t* s, uint32_t* t, void* ws, cudaStream_t st) {
-  return run_core(b->plan, b->d_mats, b->d_items, b->d_tiles, b->d_work, b->nwork, b->s_polys,
-                  b->t_polys, s, t, ws, st);
-}
-
-}  // namespace
-
-namespace {
-
 struct Tables {
   std::vector<MatDev> mats;
   std::vector<ItemDev> sorted;
@@ -312,34 +228,87 @@ struct Tables {
   std::vector<WorkDev> work;
   uint64_t s_polys = 0, t_polys = 0;
   uint32_t k_split = 0;
+  bool tc = false;
+  unsigned class_begin[TC_CLASSES + 1] = {};
 };
+
+// Evaluation groups of a tile: 8 points per CUDA-core work item; 4 or 2 per
+// tensor-core work item (by the tile's Y rows).
+uint32_t tile_groups(const Tables& tb, const TileDev& tl, uint32_t d) {
+  if (!tb.tc) return d / EG;
+  const uint32_t ny = tl.matrix == kUpperTile ? tl.count : tb.mats[tl.matrix].rows;
+  return d / (uint32_t)tc_points(ny);
+}
+
+// Cut every tile into (K range, evaluation group) work items; longest K ranges
+// first (within each tensor-core class, classes in order).
+void make_work(Tables& tb, uint32_t d) {
+  tb.work.clear();
+  std::vector<int> cls;
+  for (uint32_t ti = 0; ti < tb.tiles.size(); ++ti) {
+    const TileDev& tl = tb.tiles[ti];
+    const uint32_t groups = tile_groups(tb, tl, d);
+    for (uint32_t k0 = 0; k0 < tl.kmax; k0 += tb.k_split) {
+      const uint32_t k1 = std::min(tl.kmax, k0 + tb.k_split);
+      for (uint32_t g = 0; g < groups; ++g) {
+        tb.work.push_back(WorkDev{ti, k0, k1, g});
+        cls.push_back(tb.tc ? tc_class(tl, tb.mats.data()) : 0);
+      }
+    }
+  }
+  std::vector<size_t> order(tb.work.size());
+  for (size_t i = 0; i < order.size(); ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) {
+    if (cls[x] != cls[y]) return cls[x] < cls[y];
+    return (tb.work[x].k1 - tb.work[x].k0) > (tb.work[y].k1 - tb.work[y].k0);
+  });
+  std::vector<WorkDev> sorted(order.size());
+  for (size_t i = 0; i < order.size(); ++i) sorted[i] = tb.work[order[i]];
+  tb.work.swap(sorted);
+  for (int c = 0; c <= TC_CLASSES; ++c) tb.class_begin[c] = 0;
+  for (size_t i = 0; i < order.size(); ++i) tb.class_begin[cls[order[i]] + 1]++;
+  for (int c = 0; c < TC_CLASSES; ++c) tb.class_begin[c + 1] += tb.class_begin[c];
+}
 
 // K range per work item when the caller leaves it to the library: about four
 // work items per SM, so a small batch (a few instances, one tile) still
 // spreads over the whole GPU instead of running its K loop on a few CTAs;
 // large batches reach the 8192 cap, where fewer accumulator atomics win.
-uint32_t auto_k_split(const std::vector<TileDev>& tiles, uint32_t groups, int num_sms) {
+uint32_t auto_k_split(const Tables& tb, uint32_t d, int num_sms) {
   uint64_t steps = 0;  // KC-wide K steps over every tile and evaluation group
-  for (const TileDev& tl : tiles) steps += (tl.kmax + KC - 1) / KC;
-  steps *= groups;
+  for (const TileDev& tl : tb.tiles) steps += (uint64_t)((tl.kmax + KC - 1) / KC) * tile_groups(tb, tl, d);
   const uint64_t target = 4ull * (uint64_t)(num_sms > 0 ? num_sms : 148);
   uint64_t per = (steps + target - 1) / target;
-  per = std::max<uint64_t>(1, std::min<uint64_t>(per, 8192 / KC));
+  per = std::max<uint64_t>(tb.tc ? 2 : 1, std::min<uint64_t>(per, 8192 / KC));
+  if (tb.tc) per = (per + 1) / 2 * 2;  // whole 32-word tensor-core chunks
   return (uint32_t)(per * KC);
 }
 
-// Group items by matrix, longest first, into tiles of 32, 64 or 128 instances
-// (by the matrix's rows, tile_tmg); then cut every tile
-// into (K range, evaluation group) work items, longest K ranges first.
+bool engine_uses_tc(const grid_gpu_plan* plan, int engine) {
+  if (engine == GRID_GPU_ENGINE_CUDA_CORE) return false;
+  return plan->tc_emm && plan->d % 4 == 0;
+}
+
+// Group items by matrix, longest first, into tiles; then cut every tile into
+// work items. Tensor-core tiles hold up to 128 instances (the MMA's M); the
+// CUDA-core kernel's tiles 32, 64 or 128 (by the matrix's rows, tile_tmg).
+// tile_instances (when nonzero) caps the instances per tile.
 int build_tables(const grid_gpu_plan* plan, grid_gpu_matrix* const* mats, size_t nmats,
                  const grid_gpu_batch_item* items, size_t nitems, uint32_t k_split,
-                 Tables& tb) {
+                 uint32_t tile_instances, int engine, Tables& tb) {
   if (!plan || (!mats && nmats) || (!items && nitems)) return GRID_ERR_NULL_POINTER;
-  // the grouped kernel contracts evaluations mod q: a ring plan without an NTT
+  // the grouped kernels contract evaluations mod q: a ring plan without an NTT
   // for q commits through grid_gpu_commit_dev instead
   if (is_crt(plan)) return plan->ntt_status;
   if (nmats == 0 || nitems == 0 || nitems > (1u << 30)) return GRID_ERR_INVALID_PARAMETERS;
-  if (k_split != 0 && (k_split < (uint32_t)KC || k_split % KC)) return GRID_ERR_INVALID_PARAMETERS;
+  if (k_split != 0 && (k_split < (uint32_t)KC || k_split % KC || k_split > kTcMaxK))
+    return GRID_ERR_INVALID_PARAMETERS;
+  if (engine < GRID_GPU_ENGINE_AUTO || engine > GRID_GPU_ENGINE_CUDA_CORE)
+    return GRID_ERR_INVALID_PARAMETERS;
+  if (tile_instances != 0 && (tile_instances % 4 || tile_instances > kTcMaxTileRows))
+    return GRID_ERR_INVALID_PARAMETERS;
+  tb.tc = engine_uses_tc(plan, engine);
+  if (engine == GRID_GPU_ENGINE_TENSOR && !tb.tc) return GRID_ERR_UNSUPPORTED_DEGREE;
   for (size_t i = 0; i < nmats; ++i) {
     if (!mats[i]) return GRID_ERR_NULL_POINTER;
     if (mats[i]->plan != plan) return GRID_ERR_INVALID_PARAMETERS;
@@ -364,7 +333,8 @@ int build_tables(const grid_gpu_plan* plan, grid_gpu_matrix* const* mats, size_t
     const uint32_t m = order[i].first;
     size_t j = i;
     TileDev tl{(uint32_t)tb.sorted.size(), 0, m, 0};
-    const size_t cap = 4 * (size_t)tile_tmg(tb.mats[m].rows);  // instances per tile
+    size_t cap = tb.tc ? (size_t)kTcMaxTileRows : 4 * (size_t)tile_tmg(tb.mats[m].rows);
+    if (tile_instances) cap = std::min<size_t>(cap, tile_instances);
     while (j < order.size() && order[j].first == m && j - i < cap) {
       const grid_gpu_batch_item& it = items[order[j].second];
       tb.sorted.push_back(ItemDev{it.s_offset, it.t_offset, it.n, 0});
@@ -375,10 +345,111 @@ int build_tables(const grid_gpu_plan* plan, grid_gpu_matrix* const* mats, size_t
     tb.tiles.push_back(tl);
     i = j;
   }
-  if (k_split == 0) k_split = auto_k_split(tb.tiles, plan->d / EG, plan->num_sms);
-  tb.k_split = k_split;
-  tb.work = make_work(tb.tiles, plan->d / EG, k_split);
+  tb.k_split = k_split ? k_split : auto_k_split(tb, plan->d, plan->num_sms);
+  make_work(tb, plan->d);
   return GRID_OK;
+}
+
+int upload(grid_gpu_batch* b) {
+  for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
+  b->graphs.clear();
+  for (void* ptr : {(void*)b->d_mats, (void*)b->d_items, (void*)b->d_tiles, (void*)b->d_work})
+    if (ptr) cudaFree(ptr);
+  b->d_mats = nullptr;
+  b->d_items = nullptr;
+  b->d_tiles = nullptr;
+  b->d_work = nullptr;
+  Tables tb;
+  int rc = build_tables(b->plan, b->mat_handles.data(), b->mat_handles.size(), b->items.data(),
+                        b->items.size(), b->k_split, b->tile_instances, b->engine, tb);
+  if (rc) return rc;
+  b->mats = std::move(tb.mats);
+  b->sorted = std::move(tb.sorted);
+  b->tiles = std::move(tb.tiles);
+  b->s_polys = tb.s_polys;
+  b->t_polys = tb.t_polys;
+  b->tc = tb.tc;
+  std::copy(tb.class_begin, tb.class_begin + TC_CLASSES + 1, b->class_begin);
+  b->nwork = (unsigned)tb.work.size();
+  auto send = [](auto** dst, const auto& v) {
+    using T = typename std::remove_reference<decltype(v)>::type::value_type;
+    cudaError_t e = cudaMalloc(dst, std::max<size_t>(1, v.size()) * sizeof(T));
+    if (e == cudaSuccess && !v.empty())
+      e = cudaMemcpy(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+    return e;
+  };
+  cudaError_t e = send(&b->d_mats, b->mats);
+  if (e == cudaSuccess) e = send(&b->d_items, b->sorted);
+  if (e == cudaSuccess) e = send(&b->d_tiles, b->tiles);
+  if (e == cudaSuccess) e = send(&b->d_work, tb.work);
+  return cuda_status(e);
+}
+
+// accumulators and one work counter per tensor-core class after the witness
+size_t core_bytes(uint64_t s_polys, uint64_t t_polys, size_t d) {
+  return round_up(s_polys * d * 4, 256) + round_up(t_polys * d * 8, 256) + 256;
+}
+
+size_t ws_bytes(const grid_gpu_batch* b) { return core_bytes(b->s_polys, b->t_polys, b->plan->d); }
+
+// Grouped product -> fold -> INTT over given transformed witnesses and tables:
+// acc (t_polys x d u64) and the counters are cleared here.
+int run_product(const grid_gpu_plan* p, bool tc, const unsigned* class_begin,
+                const MatDev* d_mats, const ItemDev* d_items, const TileDev* d_tiles,
+                const WorkDev* d_work, unsigned nwork, const uint32_t* s_hat,
+                unsigned long long* acc, unsigned* counters, uint64_t t_polys, uint32_t* t,
+                cudaStream_t st) {
+  const size_t d = p->d;
+  cudaError_t e = cudaMemsetAsync(acc, 0, t_polys * d * 8, st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(counters, 0, TC_CLASSES * sizeof(unsigned), st);
+  if (e != cudaSuccess) return cuda_status(e);
+  int rc = GRID_OK;
+  if (tc) {
+    for (int c = 0; c < TC_CLASSES && !rc; ++c) {
+      const unsigned n = class_begin[c + 1] - class_begin[c];
+      if (n)
+        rc = launch_batch_tc(p, c, d_work + class_begin[c], n, d_tiles, d_items, d_mats, s_hat,
+                             acc, counters + c, st);
+    }
+    if (rc) return rc;
+  } else if (nwork) {
+    static int bps_cache[kMaxDevices] = {};
+    int bps = 0;
+    rc = prepare_kernel(batch_emm_kernel, kBatchSmem, kThreads, p->device, bps_cache, &bps);
+    if (rc) return rc;
+    const unsigned grid = std::min<unsigned>(nwork, (unsigned)(p->num_sms * bps));
+    batch_emm_kernel<<<grid, kThreads, kBatchSmem, st>>>(d_work, nwork, d_tiles, d_items, d_mats,
+                                                         s_hat, acc, counters, (int)d, p->f);
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(e);
+  }
+  const size_t words = t_polys * d;
+  unsigned blocks = (unsigned)std::min<size_t>((words + 255) / 256, (size_t)p->num_sms * 8);
+  fold_kernel<<<blocks ? blocks : 1, 256, 0, st>>>(acc, t, words, p->f.q);
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(e);
+  return launch_ntt(p, MODE_INV, t, nullptr, t, t_polys, st);
+}
+
+// NTT(s) -> grouped product -> fold -> INTT(t), with device tables given.
+int run_core(const grid_gpu_plan* p, bool tc, const unsigned* class_begin, const MatDev* d_mats,
+             const ItemDev* d_items, const TileDev* d_tiles, const WorkDev* d_work,
+             unsigned nwork, uint64_t s_polys, uint64_t t_polys, const uint32_t* s, uint32_t* t,
+             void* ws, cudaStream_t st) {
+  const size_t d = p->d;
+  char* base = static_cast<char*>(ws);
+  uint32_t* s_hat = reinterpret_cast<uint32_t*>(base);
+  unsigned long long* acc =
+      reinterpret_cast<unsigned long long*>(base + round_up(s_polys * d * 4, 256));
+  unsigned* counters = reinterpret_cast<unsigned*>(base + round_up(s_polys * d * 4, 256) +
+                                                   round_up(t_polys * d * 8, 256));
+  const int rc = launch_ntt(p, MODE_FWD, s, nullptr, s_hat, s_polys, st);
+  if (rc) return rc;
+  return run_product(p, tc, class_begin, d_mats, d_items, d_tiles, d_work, nwork, s_hat, acc,
+                     counters, t_polys, t, st);
+}
+
+int run_sequence(grid_gpu_batch* b, const uint32_t* s, uint32_t* t, void* ws, cudaStream_t st) {
+  return run_core(b->plan, b->tc, b->class_begin, b->d_mats, b->d_items, b->d_tiles, b->d_work,
+                  b->nwork, b->s_polys, b->t_polys, s, t, ws, st);
 }
 
 size_t tables_bytes(const Tables& tb) {
@@ -388,8 +459,58 @@ size_t tables_bytes(const Tables& tb) {
          round_up(tb.work.size() * sizeof(WorkDev), 256);
 }
 
-size_t core_bytes(uint64_t s_polys, uint64_t t_polys, size_t d) {
-  return round_up(s_polys * d * 4, 256) + round_up(t_polys * d * 8, 256) + 256;
+// Pack the four tables into one host image of the device layout at `dev` and
+// send it with a single copy. The source is pageable: the copy returns once its
+// bytes are staged, so the image may go away when the caller returns.
+int send_tables(const Tables& tb, char* dev, const MatDev** dm, const ItemDev** di,
+                const TileDev** dt, const WorkDev** dw, cudaStream_t st) {
+  std::vector<char> image(tables_bytes(tb));
+  size_t off = 0;
+  auto put = [&](const void* src, size_t n) -> void* {
+    if (n) std::memcpy(image.data() + off, src, n);
+    void* dst = dev + off;
+    off += round_up(n, 256);
+    return dst;
+  };
+  *dm = static_cast<const MatDev*>(put(tb.mats.data(), tb.mats.size() * sizeof(MatDev)));
+  *di = static_cast<const ItemDev*>(put(tb.sorted.data(), tb.sorted.size() * sizeof(ItemDev)));
+  *dt = static_cast<const TileDev*>(put(tb.tiles.data(), tb.tiles.size() * sizeof(TileDev)));
+  *dw = static_cast<const WorkDev*>(put(tb.work.data(), tb.work.size() * sizeof(WorkDev)));
+  if (image.empty()) return GRID_OK;
+  return cuda_status(cudaMemcpyAsync(dev, image.data(), image.size(), cudaMemcpyHostToDevice, st));
+}
+
+// ---- batched Gram matrices (the Gram of many witnesses of different r, n) ----
+
+// Witness evaluations packed in item order; tiles = one instance (r rows).
+int build_gram_tables(const grid_gpu_plan* plan, const grid_gpu_gram_item* items, size_t nitems,
+                      uint32_t k_split, Tables& tb, uint64_t* g_polys) {
+  if (!plan || (!items && nitems)) return GRID_ERR_NULL_POINTER;
+  if (nitems == 0 || nitems > (1u << 24)) return GRID_ERR_INVALID_PARAMETERS;
+  if (k_split != 0 && (k_split < (uint32_t)KC || k_split % KC || k_split > kTcMaxK))
+    return GRID_ERR_INVALID_PARAMETERS;
+  tb.tc = true;
+  uint64_t shat = 0, g = 0;
+  for (size_t i = 0; i < nitems; ++i) {
+    const grid_gpu_gram_item& it = items[i];
+    if (it.r == 0 || it.n == 0 || it.r > (uint32_t)kTcMaxYRows) return GRID_ERR_INVALID_PARAMETERS;
+    TileDev tl{(uint32_t)tb.sorted.size(), it.r, kUpperTile, it.n};
+    for (uint32_t j = 0; j < it.r; ++j)
+      tb.sorted.push_back(ItemDev{shat + (uint64_t)j * it.n, g, it.n, 0});
+    tb.tiles.push_back(tl);
+    shat += (uint64_t)it.r * it.n;
+    g += (uint64_t)it.r * (it.r + 1) / 2;
+  }
+  tb.s_polys = shat;
+  tb.t_polys = g;
+  *g_polys = g;
+  tb.k_split = k_split ? k_split : auto_k_split(tb, plan->d, plan->num_sms);
+  make_work(tb, plan->d);
+  return GRID_OK;
+}
+
+bool gram_uses_tc(const grid_gpu_plan* plan) {
+  return !is_crt(plan) && plan->tc_emm && plan->d % 4 == 0;
 }
 
 }  // namespace
@@ -400,33 +521,17 @@ int grid_gpu_batch_create(grid_gpu_plan* plan, grid_gpu_matrix* const* mats, siz
                           const grid_gpu_batch_item* items, size_t nitems, grid_gpu_batch** out) {
   if (!out) return GRID_ERR_NULL_POINTER;
   *out = nullptr;
-  Tables tb;
-  int rc = build_tables(plan, mats, nmats, items, nitems, 1024, tb);
+  Tables probe;
+  int rc = build_tables(plan, mats, nmats, items, nitems, 1024, 0, GRID_GPU_ENGINE_AUTO, probe);
   if (rc) return rc;
   grid_gpu_batch* b = new (std::nothrow) grid_gpu_batch();
   if (!b) return GRID_ERR_OUT_OF_MEMORY;
   b->plan = plan;
   b->num_sms = plan->num_sms;
   b->k_split = 1024;
-  b->mats = std::move(tb.mats);
-  b->sorted = std::move(tb.sorted);
-  b->tiles = std::move(tb.tiles);
-  b->s_polys = tb.s_polys;
-  b->t_polys = tb.t_polys;
-  cudaError_t e = cudaMalloc(&b->d_mats, b->mats.size() * sizeof(MatDev));
-  if (e == cudaSuccess) e = cudaMalloc(&b->d_items, b->sorted.size() * sizeof(ItemDev));
-  if (e == cudaSuccess) e = cudaMalloc(&b->d_tiles, b->tiles.size() * sizeof(TileDev));
-  if (e == cudaSuccess)
-    e = cudaMemcpy(b->d_mats, b->mats.data(), b->mats.size() * sizeof(MatDev),
-                   cudaMemcpyHostToDevice);
-  if (e == cudaSuccess)
-    e = cudaMemcpy(b->d_items, b->sorted.data(), b->sorted.size() * sizeof(ItemDev),
-                   cudaMemcpyHostToDevice);
-  if (e == cudaSuccess)
-    e = cudaMemcpy(b->d_tiles, b->tiles.data(), b->tiles.size() * sizeof(TileDev),
-                   cudaMemcpyHostToDevice);
-  rc = cuda_status(e);
-  if (!rc) rc = rebuild_work(b);
+  b->mat_handles.assign(mats, mats + nmats);
+  b->items.assign(items, items + nitems);
+  rc = upload(b);
   if (rc) {
     grid_gpu_batch_destroy(b);
     return rc;
@@ -448,10 +553,22 @@ int grid_gpu_batch_destroy(grid_gpu_batch* b) {
 
 int grid_gpu_batch_set_config(grid_gpu_batch* b, const grid_gpu_batch_config* cfg) {
   if (!b || !cfg) return GRID_ERR_NULL_POINTER;
-  if (cfg->k_split < KC || cfg->k_split % KC) return GRID_ERR_INVALID_PARAMETERS;
+  if (cfg->k_split < KC || cfg->k_split % KC || cfg->k_split > kTcMaxK)
+    return GRID_ERR_INVALID_PARAMETERS;
   std::lock_guard<std::mutex> lk(b->mu);
+  const uint32_t old_k = b->k_split, old_ti = b->tile_instances;
+  const int old_engine = b->engine;
   b->k_split = cfg->k_split;
-  return rebuild_work(b);
+  b->tile_instances = cfg->tile_instances;
+  b->engine = (int)cfg->engine;
+  const int rc = upload(b);
+  if (rc) {  // keep the previous (valid) configuration
+    b->k_split = old_k;
+    b->tile_instances = old_ti;
+    b->engine = old_engine;
+    upload(b);
+  }
+  return rc;
 }
 
 int grid_gpu_batch_get_config(const grid_gpu_batch* b, grid_gpu_batch_config* cfg) {
@@ -459,6 +576,9 @@ int grid_gpu_batch_get_config(const grid_gpu_batch* b, grid_gpu_batch_config* cf
   cfg->k_split = b->k_split;
   cfg->work_items = b->nwork;
   cfg->tiles = (uint32_t)b->tiles.size();
+  cfg->tile_instances = b->tile_instances;
+  cfg->engine = (uint32_t)b->engine;
+  cfg->tensor_cores = b->tc ? 1u : 0u;
   return GRID_OK;
 }
 
@@ -519,7 +639,8 @@ int grid_gpu_batch_oneshot_workspace(grid_gpu_plan* plan, grid_gpu_matrix* const
                                      size_t nitems, uint32_t k_split, size_t* bytes) {
   if (!bytes) return GRID_ERR_NULL_POINTER;
   Tables tb;
-  const int rc = build_tables(plan, mats, nmats, items, nitems, k_split, tb);
+  const int rc =
+      build_tables(plan, mats, nmats, items, nitems, k_split, 0, GRID_GPU_ENGINE_AUTO, tb);
   if (rc) return rc;
   *bytes = core_bytes(tb.s_polys, tb.t_polys, plan->d) + tables_bytes(tb);
   return GRID_OK;
@@ -533,31 +654,100 @@ int grid_gpu_batch_commit_oneshot_dev(grid_gpu_plan* plan, grid_gpu_matrix* cons
   if (!s || !t || !workspace) return GRID_ERR_NULL_POINTER;
   if (((uintptr_t)s | (uintptr_t)t | (uintptr_t)workspace) & 15u) return GRID_ERR_MISALIGNED;
   Tables tb;
-  int rc = build_tables(plan, mats, nmats, items, nitems, k_split, tb);
+  int rc = build_tables(plan, mats, nmats, items, nitems, k_split, 0, GRID_GPU_ENGINE_AUTO, tb);
   if (rc) return rc;
   const size_t core = core_bytes(tb.s_polys, tb.t_polys, plan->d);
   if (workspace_bytes < core + tables_bytes(tb)) return GRID_ERR_INVALID_PARAMETERS;
   cudaStream_t st = (cudaStream_t)stream;
-  // Pack the four tables into one host image of the device layout and send
-  // it with a single copy. The source is pageable: the copy returns once its
-  // bytes are staged, so the image may go away when this call returns.
-  std::vector<char> image(tables_bytes(tb));
-  size_t off = 0;
-  char* const dev = static_cast<char*>(workspace) + core;
-  auto put = [&](const void* src, size_t n) -> void* {
-    if (n) std::memcpy(image.data() + off, src, n);
-    void* dst = dev + off;
-    off += round_up(n, 256);
-    return dst;
-  };
-  auto* dm = static_cast<const MatDev*>(put(tb.mats.data(), tb.mats.size() * sizeof(MatDev)));
-  auto* di = static_cast<const ItemDev*>(put(tb.sorted.data(), tb.sorted.size() * sizeof(ItemDev)));
-  auto* dt = static_cast<const TileDev*>(put(tb.tiles.data(), tb.tiles.size() * sizeof(TileDev)));
-  auto* dw = static_cast<const WorkDev*>(put(tb.work.data(), tb.work.size() * sizeof(WorkDev)));
-  rc = cuda_status(cudaMemcpyAsync(dev, image.data(), image.size(), cudaMemcpyHostToDevice, st));
+  const MatDev* dm;
+  const ItemDev* di;
+  const TileDev* dt;
+  const WorkDev* dw;
+  rc = send_tables(tb, static_cast<char*>(workspace) + core, &dm, &di, &dt, &dw, st);
   if (rc) return rc;
-  return run_core(plan, dm, di, dt, dw, (unsigned)tb.work.size(), tb.s_polys, tb.t_polys, s, t,
-                  workspace, st);
+  return run_core(plan, tb.tc, tb.class_begin, dm, di, dt, dw, (unsigned)tb.work.size(),
+                  tb.s_polys, tb.t_polys, s, t, workspace, st);
+}
+
+int grid_gpu_batch_gram_workspace(const grid_gpu_plan* plan, const grid_gpu_gram_item* items,
+                                  size_t nitems, uint32_t k_split, size_t* bytes) {
+  if (!plan || !bytes) return GRID_ERR_NULL_POINTER;
+  if (!gram_uses_tc(plan)) {  // one Gram call after another in a shared workspace
+    if (!items && nitems) return GRID_ERR_NULL_POINTER;
+    size_t need = 16;
+    for (size_t i = 0; i < nitems; ++i) {
+      size_t w = 0;
+      const int rc = grid_gpu_gram_workspace(plan, items[i].r, items[i].n, &w);
+      if (rc) return rc;
+      need = std::max(need, w);
+    }
+    *bytes = need;
+    return GRID_OK;
+  }
+  Tables tb;
+  uint64_t g_polys = 0;
+  const int rc = build_gram_tables(plan, items, nitems, k_split, tb, &g_polys);
+  if (rc) return rc;
+  *bytes = core_bytes(tb.s_polys, tb.t_polys, plan->d) + tables_bytes(tb);
+  return GRID_OK;
+}
+
+int grid_gpu_batch_gram_dev(const grid_gpu_plan* plan, const uint32_t* S,
+                            const grid_gpu_gram_item* items, size_t nitems, uint32_t k_split,
+                            uint32_t* G, void* workspace, size_t workspace_bytes, void* stream) {
+  if (!plan || !S || !G || !workspace || (!items && nitems)) return GRID_ERR_NULL_POINTER;
+  if (((uintptr_t)S | (uintptr_t)G | (uintptr_t)workspace) & 15u) return GRID_ERR_MISALIGNED;
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t d = plan->d;
+  if (!gram_uses_tc(plan)) {
+    uint64_t g = 0;
+    for (size_t i = 0; i < nitems; ++i) {
+      const int rc = grid_gpu_gram_dev(plan, S + items[i].s_offset * d, items[i].r, items[i].n,
+                                       G + g * d, workspace, workspace_bytes, stream);
+      if (rc) return rc;
+      g += (uint64_t)items[i].r * (items[i].r + 1) / 2;
+    }
+    return GRID_OK;
+  }
+  Tables tb;
+  uint64_t g_polys = 0;
+  int rc = build_gram_tables(plan, items, nitems, k_split, tb, &g_polys);
+  if (rc) return rc;
+  const size_t core = core_bytes(tb.s_polys, tb.t_polys, d);
+  if (workspace_bytes < core + tables_bytes(tb)) return GRID_ERR_INVALID_PARAMETERS;
+  char* base = static_cast<char*>(workspace);
+  uint32_t* s_hat = reinterpret_cast<uint32_t*>(base);
+  unsigned long long* acc =
+      reinterpret_cast<unsigned long long*>(base + round_up(tb.s_polys * d * 4, 256));
+  unsigned* counters = reinterpret_cast<unsigned*>(base + round_up(tb.s_polys * d * 4, 256) +
+                                                   round_up(tb.t_polys * d * 8, 256));
+  // every witness to the evaluation domain, packed in item order (one launch
+  // when the witnesses already lie packed in that order)
+  bool packed = true;
+  uint64_t off = 0;
+  for (size_t i = 0; i < nitems && packed; ++i) {
+    packed = items[i].s_offset == off;
+    off += (uint64_t)items[i].r * items[i].n;
+  }
+  if (packed) {
+    rc = launch_ntt(plan, MODE_FWD, S, nullptr, s_hat, tb.s_polys, st);
+  } else {
+    off = 0;
+    for (size_t i = 0; i < nitems && !rc; ++i) {
+      const uint64_t np = (uint64_t)items[i].r * items[i].n;
+      rc = launch_ntt(plan, MODE_FWD, S + items[i].s_offset * d, nullptr, s_hat + off * d, np, st);
+      off += np;
+    }
+  }
+  if (rc) return rc;
+  const MatDev* dm;
+  const ItemDev* di;
+  const TileDev* dt;
+  const WorkDev* dw;
+  rc = send_tables(tb, base + core, &dm, &di, &dt, &dw, st);
+  if (rc) return rc;
+  return run_product(plan, true, tb.class_begin, dm, di, dt, dw, (unsigned)tb.work.size(), s_hat,
+                     acc, counters, g_polys, G, st);
 }
 
 }  // extern "C"

@@ -341,7 +341,7 @@ const char* grid_gpu_status_string(int status) {
   }
 }
 
-uint32_t grid_gpu_abi_version(void) { return (1u << 16) | 0u; }
+uint32_t grid_gpu_abi_version(void) { return (1u << 16) | 1u; }
 
 uint32_t grid_gpu_max_degree(void) { return kMaxDegree; }
 

@@ -72,6 +72,34 @@ def compute_garbage_g(plan: TwistedNttPlan, witness):
     return g
 
 
+def compute_garbage_g_batch(plan: TwistedNttPlan, pool, items, k_split: int = 0,
+                            workspace=None):
+    """compute_garbage_g for many witnesses of different rank r <= 64 and
+    length n in one launch sequence. pool: CUDA tensor (polys, d) of witness
+    words; items: [(s_offset, r, n)], witness i = r x n polys at poly s_offset.
+    Returns a CUDA tensor (sum_i r_i (r_i + 1) / 2, d): item i's Gram polys in
+    garbage_index order after item i-1's. Equals one compute_garbage_g per item."""
+    import torch
+    lib = _lib.load()
+    d = plan.d
+    arr = (_lib.GramItem * len(items))()
+    total = 0
+    for i, (so, r, n) in enumerate(items):
+        arr[i] = _lib.GramItem(int(so), int(r), int(n))
+        total += garbage_count(int(r))
+    G = torch.empty((total, d), dtype=torch.int32, device=pool.device)
+    if workspace is None:
+        nb = C.c_size_t()
+        raise_status(lib.grid_gpu_batch_gram_workspace(plan.handle, arr, len(items), int(k_split),
+                                                       C.byref(nb)), "batch_gram_workspace")
+        workspace = torch.empty(max(256, nb.value), dtype=torch.uint8, device=pool.device)
+    st = lib.grid_gpu_batch_gram_dev(plan.handle, pool.data_ptr(), arr, len(items), int(k_split),
+                                     G.data_ptr(), workspace.data_ptr(), workspace.numel(),
+                                     _stream_ptr(pool))
+    raise_status(st, "grid_gpu_batch_gram_dev")
+    return G
+
+
 def compute_garbage_h(plan: TwistedNttPlan, witness, aggregated_phis):
     """h_ij = (<phi_i, s_j> + <phi_j, s_i>) * 2^-1 for i <= j in garbage_index
     order (garbage.rs:101-133). witness, aggregated_phis: (r, n, d) numpy

@@ -110,3 +110,101 @@ def test_batch_rejects_bad_items(cuda):
         UnevenCommitBatch(plan, [M], [(0, 0, 11, 0)])   # n beyond the matrix
     with pytest.raises(CommitmentError):
         UnevenCommitBatch(plan, [M], [(0, 0, 5, 1)])    # no such matrix
+
+
+@pytest.mark.parametrize("schedule", [(1024, 0, 1), (2048, 64, 1), (8192, 32, 1), (256, 0, 1),
+                                      (4096, 0, 2)])
+def test_batched_commit_schedules_match_oracle(cuda, oracle, schedule):
+    """Every engine and tile shape (tensor cores with 128, 64 or 32 instances per
+    tile; CUDA cores) gives the oracle's words."""
+    import torch
+    from lattica_b200.batch import UnevenCommitBatch
+    ranks = (8, 16, 32)
+    plan, mats, mats_host, items, s_host, s, t_polys = _setup(cuda, oracle, ranks, 700, 150, 11)
+    want = _oracle_expect(oracle, mats_host, items, s_host, t_polys)
+    batch = UnevenCommitBatch(plan, mats, items)
+    batch.set_config(*schedule)
+    cfg = batch.config()
+    assert cfg["tensor_cores"] == (schedule[2] == 1) and cfg["k_split"] == schedule[0]
+    t = torch.zeros((t_polys, 64), dtype=torch.int32, device=cuda)
+    batch.commit_dev(s, t)
+    torch.cuda.synchronize()
+    assert np.array_equal(t.cpu().numpy().view(np.uint32), want), schedule
+    plan.check_device()
+
+
+def test_autotuner_searches_tile_shapes(cuda, oracle, tmp_path):
+    import torch
+    from lattica_b200.batch import UnevenCommitBatch
+    plan, mats, mats_host, items, s_host, s, t_polys = _setup(cuda, oracle, (8, 32), 400, 60, 12)
+    want = _oracle_expect(oracle, mats_host, items, s_host, t_polys)
+    batch = UnevenCommitBatch(plan, mats, items)
+    t = torch.zeros((t_polys, 64), dtype=torch.int32, device=cuda)
+    res = batch.autotune(s, t, reps=1, cache_path=str(tmp_path / "a.json"))
+    assert len(res["candidates_ms"]) == len(batch.schedules())
+    assert res["engine"] in ("tensor", "cuda_core") and not res["cached"]
+    t.zero_()
+    batch.commit_dev(s, t)
+    torch.cuda.synchronize()
+    assert np.array_equal(t.cpu().numpy().view(np.uint32), want)
+    res2 = batch.autotune(s, t, cache_path=str(tmp_path / "a.json"))
+    assert res2["cached"] and res2["schedule"] == res["schedule"]
+
+
+@pytest.mark.parametrize("k_split", [0, 64, 1024])
+def test_batched_gram_of_uneven_rank_matches_oracle(cuda, oracle, k_split):
+    """compute_garbage_g for witnesses of r in {1, 5, 8, 16, 17, 33, 64} and
+    uneven n, at scattered offsets of one pool, in one launch sequence."""
+    import torch
+    from lattica_b200 import TwistedNttPlan
+    from lattica_b200.labrador import compute_garbage_g, compute_garbage_g_batch
+    plan = TwistedNttPlan(Q, 64)
+    P = oracle.Plan(Q, 64)
+    rng = np.random.default_rng(k_split + 5)
+    shapes = [(64, 300), (1, 7), (5, 130), (16, 64), (17, 33), (33, 200), (8, 1), (64, 40),
+              (16, 1100)]
+    items, off = [], 0
+    for r, n in shapes:
+        off += int(rng.integers(0, 50))  # gaps: witnesses not packed
+        items.append((off, r, n))
+        off += r * n
+    pool_h = rng.integers(0, Q, (off, 64), dtype=np.uint64).astype(np.uint32)
+    pool_h[items[0][0]:items[0][0] + 64 * 300][:, :] = Q - 1  # largest words in one witness
+    pool = torch.from_numpy(pool_h.view(np.int32)).to(cuda)
+    G = compute_garbage_g_batch(plan, pool, items, k_split=k_split)
+    torch.cuda.synchronize()
+    got = G.cpu().numpy().view(np.uint32)
+    g0 = 0
+    for so, r, n in items:
+        cnt = r * (r + 1) // 2
+        want = P.gram(pool_h[so:so + r * n], r, n, threads=0).reshape(cnt, 64)
+        assert np.array_equal(got[g0:g0 + cnt], want), (r, n)
+        g0 += cnt
+    # packed witnesses (one transform launch) give the same words
+    packed, items2, o = [], [], 0
+    for so, r, n in items:
+        packed.append(pool_h[so:so + r * n])
+        items2.append((o, r, n))
+        o += r * n
+    pool2 = torch.from_numpy(np.concatenate(packed).view(np.int32)).to(cuda)
+    G2 = compute_garbage_g_batch(plan, pool2, items2, k_split=k_split)
+    assert torch.equal(G2, G)
+    # and one compute_garbage_g per item
+    so, r, n = items[2]
+    assert torch.equal(compute_garbage_g(plan, pool[so:so + r * n].view(r, n, 64)),
+                       G[sum(x[1] * (x[1] + 1) // 2 for x in items[:2]):][:r * (r + 1) // 2])
+    plan.check_device()
+
+
+def test_batched_gram_rejects_bad_items(cuda):
+    import ctypes as C
+    from lattica_b200 import TwistedNttPlan, _lib
+    lib = _lib.load()
+    plan = TwistedNttPlan(Q, 64)
+    nb = C.c_size_t()
+    bad = (_lib.GramItem * 1)(_lib.GramItem(0, 65, 10))  # r > 64
+    assert lib.grid_gpu_batch_gram_workspace(plan.handle, bad, 1, 0, C.byref(nb)) == 5
+    zero = (_lib.GramItem * 1)(_lib.GramItem(0, 3, 0))
+    assert lib.grid_gpu_batch_gram_workspace(plan.handle, zero, 1, 0, C.byref(nb)) == 5
+    ok = (_lib.GramItem * 1)(_lib.GramItem(0, 3, 10))
+    assert lib.grid_gpu_batch_gram_workspace(plan.handle, ok, 1, 100, C.byref(nb)) == 5  # k % 16
