@@ -570,7 +570,9 @@ def measure_batch(dev, reps=10):
             "outputs_identical": same, "mod_macs": macs,
             "parity": f"all outputs equal the per-call path; {len(pick)} instances "
                       "(longest and shortest included) equal the oracle",
-            "autotune": {k: v for k, v in tune.items() if k in ("k_split", "cached", "ms")},
+            "autotune": {k: v for k, v in tune.items()
+                         if k in ("schedule", "engine", "tile_instances", "k_split", "cached",
+                                  "ms")},
             "schedule": batch.config()}
 
 
@@ -658,6 +660,49 @@ def check_serve_parity(plan, mats, key, pool, arena, pool_polys, count=300, rate
         kinds[k] = kinds.get(k, 0) + 1
     return {"checked": f"{count} requests at {int(rate)} req/s: continuous == alone",
             "by_kind": kinds}
+
+
+def measure_ring_round(dev, reps=20):
+    """The LaBRADOR round at r = 64, n = 2048, kappa = 16 over the reference's own
+    LaBRADOR modulus q = 2^32 - 5, which has no 128th root of unity (the
+    reference multiplies by the schoolbook rule there): ring plan through three
+    auxiliary NTT primes. t limbs, g and p are checked against the oracle's
+    schoolbook products."""
+    import torch
+    from lattica_b200.labrador import CommitKey, prover_round_dev
+    from lattica_b200.ntt import RingPlan
+    from oracle import oracle as O
+    q, d, r, n, kappa = 4294967291, 64, 64, 2048, 16
+    plan = RingPlan(q, d)
+    g = torch.Generator(device=dev).manual_seed(6)
+    A = torch.randint(0, q, (kappa, n, d), dtype=torch.int64, device=dev, generator=g)
+    coeffs = torch.randint(-2048, 2049, (r, n, d), dtype=torch.int64, device=dev, generator=g) % q
+    wit = ((coeffs * ((1 << 32) % q)) % q).to(torch.int32)
+    A = A.to(torch.int32)
+    del coeffs
+    key = CommitKey(plan, A, kappa, n)
+    seed = bytes(range(32))
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(3):
+        o = prover_round_dev(key, wit, 256, 4, 256, 4, seed, 256)
+    torch.cuda.synchronize()
+    times = _events_ms(lambda: prover_round_dev(key, wit, 256, 4, 256, 4, seed, 256), reps, stream)
+    F = O.Field(q)
+    S = wit.cpu().numpy().view(np.uint32)
+    t0 = time.perf_counter()
+    t = F.ring_matvec(d, A.cpu().numpy().view(np.uint32), kappa, n, S, r)
+    gram = F.ring_gram(d, S, r, n)
+    p, _ = O.jl_project(F, seed, 256, S.reshape(r, n * d), r, n * d, d, want_flat=False)
+    oracle_s = time.perf_counter() - t0
+    host = lambda x: x.cpu().numpy().view(np.uint32).reshape(-1)
+    if not (np.array_equal(host(o.t_limbs), O.decompose_polys(F, d, t, 256, 4))
+            and np.array_equal(host(o.g), gram) and np.array_equal(host(o.p), p)):
+        raise AssertionError("ring-plan round differs from the oracle's schoolbook products")
+    return {"workload": "LaBRADOR round r=64 n=2048 kappa=16 at q=2^32-5 (no NTT: three "
+                        "auxiliary primes, exact reconstruction)",
+            "round_ms_p50": _pct(times, 50), "round_ms_p99": _pct(times, 99),
+            "oracle_schoolbook_s": round(oracle_s, 2), "oracle_cores": os.cpu_count() or 1,
+            "parity": "t limbs, g, p bit-exact vs the oracle's schoolbook products"}
 
 
 def measure_ntt256(dev, reps=20):
@@ -796,7 +841,8 @@ def run_ours(args, rank, world, local_rank):
         line["cpu_baseline"] = cpu_baseline(q, d, WORKLOADS[args.workload][2])
     if args.secondary:
         detail = {"commit": measure_commit_plain(dev), "round": measure_round(dev),
-                  "batch": measure_batch(dev), "ntt256": measure_ntt256(dev)}
+                  "batch": measure_batch(dev), "ntt256": measure_ntt256(dev),
+                  "ring_round": measure_ring_round(dev)}
         if args.serve:
             detail["serve"] = measure_serve(dev)
         line["secondary"] = secondary_summary(detail)
@@ -836,6 +882,7 @@ def secondary_summary(detail):
         "config3_ms_p50": r(b["batched_ms_p50"]),
         "config3_parity": "all == per-call; 32 sampled == oracle",
         "ntt256_polys_per_s": r(n2["polys_per_s"], 0), "ntt256_frac": r(n2["frac"]),
+        "round_q_2e32m5_ms_p50": r(detail["ring_round"]["round_ms_p50"], 4),
         "host_cores": os.cpu_count() or 1,
     }
     sv = detail.get("serve")

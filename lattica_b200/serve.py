@@ -12,8 +12,10 @@ end), so a run of queued commitments reads one contiguous span.
 Continuous mode: a scheduler thread admits waiting requests whenever a stream
 slot and device-memory budget are free. All waiting commitments (up to
 `max_batch`, within the budget) are packed into one batched launch sequence
-(grid_gpu_batch_commit_oneshot_dev); Gram + JL and round requests each take a
-slot of their own. Slots are separate CUDA streams, so work admitted while
+(grid_gpu_batch_commit_oneshot_dev); all waiting Gram + JL requests (up to
+`max_gram_batch`) share one batched Gram launch sequence
+(grid_gpu_batch_gram_dev) and then run their JL projections on the same slot;
+round requests each take a slot of their own. Slots are separate CUDA streams, so work admitted while
 other work is on the GPU overlaps with it. Plain mode is the per-call
 baseline: one request at a time, in arrival order, through the
 one-call-per-request C-ABI entry points, waiting for each to finish.
@@ -67,7 +69,7 @@ class RingServer:
 
     def __init__(self, plan, commit_mats: dict, round_key, pool, mode: str = "continuous",
                  streams: int = 4, commit_slots: int = 2, hbm_budget: int = 8 << 30,
-                 k_split: int = 0, max_batch: int = 4096,
+                 k_split: int = 0, max_batch: int = 4096, max_gram_batch: int = 32,
                  jl_seed: bytes = bytes(range(32)), round_limbs=(256, 4, 256, 4)):
         import torch
         if mode not in ("continuous", "plain"):
@@ -87,6 +89,7 @@ class RingServer:
         self.device = pool.device
         self.k_split = k_split
         self.max_batch = max_batch
+        self.max_gram_batch = max_gram_batch
         self.jl_seed = bytes(jl_seed)
         self._seed_c = (C.c_uint8 * 32).from_buffer_copy(self.jl_seed)
         self.round_limbs = round_limbs
@@ -236,7 +239,7 @@ class RingServer:
         for kind in KINDS:
             q = self._queues[kind]
             free = self._free["commit" if kind == "commit" else "heavy"]
-            limit = self.max_batch if kind == "commit" else 1
+            limit = {"commit": self.max_batch, "gramjl": self.max_gram_batch}.get(kind, 1)
             while q and free:
                 reqs, fp = [], 0
                 while q and len(reqs) < limit:
@@ -275,6 +278,8 @@ class RingServer:
                     return self._commit_batch(reqs, stream, fp)
                 return self._commit_one(reqs[0], stream)
             if kind == "gramjl":
+                if self.mode == "continuous":
+                    return self._gramjl_batch(reqs, stream, fp)
                 return self._gramjl(reqs[0], stream, fp)
             return self._round(reqs[0], stream, fp)
 
@@ -385,6 +390,34 @@ class RingServer:
             self.plan.handle, self._seed_c, JL_ROWS, s_ptr, r, n * d, d, p.data_ptr(), None,
             jws.data_ptr(), jws.numel(), stream.cuda_stream), "grid_gpu_jl_project_dev")
         return self._finish([req], [[self._pin(g), self._pin(p)]], fp, [ws, jws, g, p], stream)
+
+    def _gramjl_batch(self, reqs, stream, fp):
+        """All queued Gram + JL requests in one job: their Gram matrices in one
+        batched launch sequence (grid_gpu_batch_gram_dev), then one JL
+        projection per request on the same stream."""
+        from .labrador import compute_garbage_g_batch, garbage_count
+        torch = self._torch
+        lib = self._lib
+        d = self.d
+        items = [(r.offset, r.shape[0], r.shape[1]) for r in reqs]
+        G = compute_garbage_g_batch(self.plan, self.pool, items)
+        jw = C.c_size_t()
+        raise_status(lib.grid_gpu_jl_workspace(JL_ROWS, C.byref(jw)), "grid_gpu_jl_workspace")
+        jws = torch.empty(max(256, jw.value), dtype=torch.uint8, device=self.device)
+        p = torch.empty((len(reqs), JL_ROWS), dtype=torch.int32, device=self.device)
+        for i, req in enumerate(reqs):
+            r, n = req.shape
+            s_ptr = self.pool.data_ptr() + req.offset * d * 4
+            raise_status(lib.grid_gpu_jl_project_dev(
+                self.plan.handle, self._seed_c, JL_ROWS, s_ptr, r, n * d, d, p[i].data_ptr(), None,
+                jws.data_ptr(), jws.numel(), stream.cuda_stream), "grid_gpu_jl_project_dev")
+        g_host, p_host = self._pin(G), self._pin(p)
+        outs, g0 = [], 0
+        for i, req in enumerate(reqs):
+            cnt = garbage_count(req.shape[0])
+            outs.append([g_host[g0:g0 + cnt], p_host[i]])
+            g0 += cnt
+        return self._finish(reqs, outs, fp, [G, jws, p], stream)
 
     def _round(self, req, stream, fp):
         from .labrador import prover_round_dev
