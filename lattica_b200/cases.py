@@ -12,6 +12,9 @@ the median CUDA-event time.
     python -m lattica_b200.cases ntt256 --reps 4     # d = 256 products, 2^20 polys at q'
     python -m lattica_b200.cases commit_plain --reps 5  # A 8 x 64 from a seed, 64 ternary witnesses
     python -m lattica_b200.cases jl_extract --reps 3 --parts 16  # JL p + int8 entries
+    python -m lattica_b200.cases batch --parts 4096 --engine tensor  # uneven batched commits
+    python -m lattica_b200.cases gram_batch --parts 16  # Gram of 16 witnesses, r in 8..64, n = 1024
+    python -m lattica_b200.cases ring_round --reps 5    # the round at q = 2^32 - 5 (no NTT)
 
 Sizes: r = 64 witness vectors of n = 2048 polys (d = 64, coefficients in
 [-2^11, 2^11], as Montgomery words), kappa = 16, JL 256 rows, base 2^8 x 4
@@ -81,9 +84,41 @@ def _jl_extract(torch, dev, g, plan, parts, n):
     return run
 
 
-def build(case: str, parts: int = 64):
+def _batch(torch, dev, g, plan, num, engine):
+    """Uneven batched commits: num instances, n log-uniform in [64, 8192], rank
+    in {8, 16, 32}, one m x 8192 matrix per rank; engine: tensor or cuda_core."""
+    from lattica_b200 import _lib
+    from lattica_b200.batch import UnevenCommitBatch, sample_uneven_instances
+    from lattica_b200.commit import PreparedMatrix
+    mats = [PreparedMatrix(plan, _uniform(torch, dev, g, Q, (m, 8192, 64)), m, 8192)
+            for m in (8, 16, 32)]
+    items, s_polys, t_polys = sample_uneven_instances(num, 7)
+    tern = torch.randint(-1, 2, (s_polys, 64), dtype=torch.int64, device=dev, generator=g)
+    s = ((tern % Q) * ((1 << 32) % Q) % Q).to(torch.int32)
+    t = torch.empty((t_polys, 64), dtype=torch.int32, device=dev)
+    batch = UnevenCommitBatch(plan, mats, items)
+    batch.set_config(4096, 0, _lib.ENGINE_TENSOR if engine == "tensor" else _lib.ENGINE_CUDA_CORE)
+    run = lambda: batch.commit_dev(s, t)
+    run.keep = (mats, batch)
+    return run
+
+
+def _gram_batch(torch, dev, g, plan, count):
+    """Gram matrices of `count` witnesses, r cycling over 8, 16, 32, 64, n = 1024,
+    through grid_gpu_batch_gram_dev."""
+    from lattica_b200.labrador import compute_garbage_g_batch
+    items, off = [], 0
+    for i in range(count):
+        r = (8, 16, 32, 64)[i % 4]
+        items.append((off, r, 1024))
+        off += r * 1024
+    pool = _witness(torch, dev, g, Q, (off, 64))
+    return lambda: compute_garbage_g_batch(plan, pool, items)
+
+
+def build(case: str, parts: int = 64, engine: str = "tensor"):
     """Returns a zero-argument callable that runs one instance of `case`
-    (`parts`: witness vectors of the jl_extract case)."""
+    (`parts`: witness vectors of jl_extract, instances of batch and gram_batch)."""
     import torch
     from lattica_b200 import TwistedNttPlan
     from lattica_b200.labrador import (CommitKey, JLMatrix, amortize_witness, compute_garbage_g,
@@ -96,11 +131,23 @@ def build(case: str, parts: int = 64):
         a = _uniform(torch, dev, g, Q256, (1 << 20, 256))
         b = _uniform(torch, dev, g, Q256, (1 << 20, 256))
         return lambda: plan.ntt_mul_inverse(a, b)
+    if case == "ring_round":
+        from lattica_b200.ntt import RingPlan
+        q = 4294967291  # 2^32 - 5: three auxiliary NTT primes, exact reconstruction
+        plan = RingPlan(q, 64)
+        wit = _witness(torch, dev, g, q, (r, n, 64))
+        key = CommitKey(plan, _uniform(torch, dev, g, q, (kappa, n, 64)), kappa, n)
+        seed = bytes(range(32))
+        return lambda: prover_round_dev(key, wit, 256, 4, 256, 4, seed, 256)
     plan = TwistedNttPlan(Q, 64)
     if case == "commit_plain":
         return _commit_plain(torch, dev, g, plan)
     if case == "jl_extract":
         return _jl_extract(torch, dev, g, plan, parts, n)
+    if case == "batch":
+        return _batch(torch, dev, g, plan, parts, engine)
+    if case == "gram_batch":
+        return _gram_batch(torch, dev, g, plan, parts)
     wit = _witness(torch, dev, g, Q, (r, n, 64))
     if case == "gram":
         return lambda: compute_garbage_g(plan, wit)
@@ -126,12 +173,16 @@ def build(case: str, parts: int = 64):
 def main(argv=None) -> None:
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("case", choices=["round", "gram", "garbage_h", "amortize", "jl_evals", "commit",
-                                       "ntt256", "commit_plain", "jl_extract"])
+                                       "ntt256", "commit_plain", "jl_extract", "batch",
+                                       "gram_batch", "ring_round"])
     ap.add_argument("--reps", type=int, default=4)
-    ap.add_argument("--parts", type=int, default=64, help="witness vectors (jl_extract)")
+    ap.add_argument("--parts", type=int, default=64,
+                    help="witness vectors (jl_extract), instances (batch, gram_batch)")
+    ap.add_argument("--engine", choices=["tensor", "cuda_core"], default="tensor",
+                    help="grouped-product engine of the batch case")
     args = ap.parse_args(argv)
     import torch
-    fn = build(args.case, args.parts)
+    fn = build(args.case, args.parts, args.engine)
     fn()
     torch.cuda.synchronize()
     times = []

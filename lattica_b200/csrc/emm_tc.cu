@@ -15,7 +15,7 @@
 //    sum_l 2^(8l) D_l = sum_k x_k y_k (mod q); one Montgomery reduction of that
 //    sum gives the canonical word. D < 4 K 255^2 stays below 2^31 for K <= 8192
 //    per CTA (the K range is split beyond that and the partials are summed).
-// A CTA takes EPC consecutive evaluation points and a K range; its 256 threads
+// A CTA takes EPC consecutive evaluation points and a K range; its 512 threads
 // gather the operands of each 32-word K chunk from global memory (the words of
 // one (row, k) for the CTA's evaluation points are contiguous: one vector
 // load), into one of two register buffers sized for the shape (X rows <= MX,
@@ -39,7 +39,7 @@ namespace {
 
 using namespace tcx;
 
-constexpr int kEtThreads = 256;
+constexpr int kEtThreads = 512;
 constexpr int KCH = 32;                // K words per chunk: one 128-byte swizzled row
 constexpr uint32_t ABOX = 128u * 128;  // A tile of one evaluation point: 128 rows x 128 bytes
 constexpr int kEtMaxK = 8192;          // K words per CTA: 4 * 8192 * 255^2 < 2^31
@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(kEtThreads, 1)
   if (ok) {
     const int m = 32 * (warp & 3) + lane;
     uint32_t* o = out + (size_t)split * split_stride;
-    for (int el = warp >> 2; el < EPC; el += 2) {
+    for (int el = warp >> 2; el < EPC; el += kEtThreads / 128) {
       const uint32_t taddr = tc::tmem_addr(tbase, 32 * (warp & 3), el * NMMA);
       const int e = e0 + el;
 #pragma unroll 1

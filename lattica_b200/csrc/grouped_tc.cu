@@ -7,7 +7,7 @@
 // upper triangle only).
 //
 // Each work item (tile, K range, group of EPC evaluation points) runs the
-// byte-plane product of emm_tc.cu: per 32-word K chunk the 256 threads gather
+// byte-plane product of emm_tc.cu: per 32-word K chunk the 512 threads gather
 // the tile's X rows (per-row base and length; zero past a row's length) and Y
 // rows for the item's points into registers (one vector load per (row, k)),
 // write them as 128-byte-swizzled A and B tiles (B scaled by 2^(8i) mod q and
@@ -33,7 +33,7 @@ namespace {
 
 using namespace tcx;
 
-constexpr int kGtThreads = 256;
+constexpr int kGtThreads = 512;
 constexpr int KCH = 32;                // K words per chunk: one 128-byte swizzled row
 constexpr uint32_t ABOX = 128u * 128;  // A tile of one evaluation point: 128 rows x 128 bytes
 
@@ -204,7 +204,7 @@ __device__ bool gt_item(const WorkDev& wk, const TileDev& tile, const MatDev& ma
   tc::fence_after_sync();
   if (ok && nch > 0) {
     const int m = 32 * (warp & 3) + lane;
-    for (int el = warp >> 2; el < EPC; el += 2) {
+    for (int el = warp >> 2; el < EPC; el += kGtThreads / 128) {
       const uint32_t taddr = tc::tmem_addr(cx.tbase, 32 * (warp & 3), el * NMMA);
       const int e = e0 + el;
 #pragma unroll 1
