@@ -58,23 +58,44 @@ __device__ __forceinline__ uint32_t redc64(uint64_t v, uint32_t q, uint32_t qinv
   return sub_lazy((uint32_t)(v >> 32), __umulhi(m, q), q);
 }
 
+// Whole warp: lane l receives 16 consecutive columns of tensor-memory lane
+// (taddr.lane + l).
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+      "%12, %13, %14, %15}, [%16];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+                 "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
+                 "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+               : "r"(taddr) : "memory");
+}
+
 // 16 reduced results of this thread's row: columns col0 .. col0 + 15 of the
-// four E_l blocks (64 columns apart) starting at taddr; two tensor-memory
-// round trips of 8 columns x 4 blocks.
+// four E_l blocks (64 columns apart) starting at taddr; one tensor-memory
+// round trip of 16 columns x 4 blocks, with every loaded register named in
+// the wait so that no use is scheduled above it.
 __device__ __forceinline__ void reduce16(uint32_t taddr, const TcConsts& k, uint32_t* out) {
+  uint32_t e[4][16];
 #pragma unroll
-  for (int c = 0; c < 2; ++c) {
-    uint32_t e[4][8];
+  for (int l = 0; l < 4; ++l) tmem_ld16(taddr + 64 * l, e[l]);
+  asm volatile("tcgen05.wait::ld.sync.aligned;"
+               :
+                 "+r"(e[0][0]), "+r"(e[0][1]), "+r"(e[0][2]), "+r"(e[0][3]), "+r"(e[0][4]), "+r"(e[0][5]), "+r"(e[0][6]), "+r"(e[0][7]),
+                 "+r"(e[0][8]), "+r"(e[0][9]), "+r"(e[0][10]), "+r"(e[0][11]), "+r"(e[0][12]), "+r"(e[0][13]), "+r"(e[0][14]), "+r"(e[0][15]),
+                 "+r"(e[1][0]), "+r"(e[1][1]), "+r"(e[1][2]), "+r"(e[1][3]), "+r"(e[1][4]), "+r"(e[1][5]), "+r"(e[1][6]), "+r"(e[1][7]),
+                 "+r"(e[1][8]), "+r"(e[1][9]), "+r"(e[1][10]), "+r"(e[1][11]), "+r"(e[1][12]), "+r"(e[1][13]), "+r"(e[1][14]), "+r"(e[1][15]),
+                 "+r"(e[2][0]), "+r"(e[2][1]), "+r"(e[2][2]), "+r"(e[2][3]), "+r"(e[2][4]), "+r"(e[2][5]), "+r"(e[2][6]), "+r"(e[2][7]),
+                 "+r"(e[2][8]), "+r"(e[2][9]), "+r"(e[2][10]), "+r"(e[2][11]), "+r"(e[2][12]), "+r"(e[2][13]), "+r"(e[2][14]), "+r"(e[2][15]),
+                 "+r"(e[3][0]), "+r"(e[3][1]), "+r"(e[3][2]), "+r"(e[3][3]), "+r"(e[3][4]), "+r"(e[3][5]), "+r"(e[3][6]), "+r"(e[3][7]),
+                 "+r"(e[3][8]), "+r"(e[3][9]), "+r"(e[3][10]), "+r"(e[3][11]), "+r"(e[3][12]), "+r"(e[3][13]), "+r"(e[3][14]), "+r"(e[3][15])
+               :
+               : "memory");
 #pragma unroll
-    for (int l = 0; l < 4; ++l) tc::tmem_ld8(taddr + 64 * l + 8 * c, e[l]);
-    tc::tmem_ld_wait32(e);
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      uint64_t v = mad_wide(e[1][j], 256u, (uint64_t)e[0][j]);
-      v = mad_wide(e[2][j], 65536u, v);
-      v = mad_wide(e[3][j], 16777216u, v);
-      out[8 * c + j] = redc64(v, k.q, k.qinv);
-    }
+  for (int j = 0; j < 16; ++j) {
+    uint64_t v = mad_wide(e[1][j], 256u, (uint64_t)e[0][j]);
+    v = mad_wide(e[2][j], 65536u, v);
+    v = mad_wide(e[3][j], 16777216u, v);
+    out[j] = redc64(v, k.q, k.qinv);
   }
 }
 
