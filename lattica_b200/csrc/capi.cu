@@ -13,6 +13,14 @@ namespace {
 
 bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
 
+// The forward transform stores the evaluations of M x K witness polys
+// point-major and the product with Y (N rows of row stride ldy) runs on the
+// TMA-fed tensor-core kernel (emm_pm.cu).
+bool pm_fits(const grid_gpu_plan* p, size_t M, size_t N, size_t K, size_t ldy, int mode) {
+  EmmPmGeometry g;
+  return ntt_tc_available(p) && emm_pm_geometry(p, (int)M, (int)N, (int)K, (int)ldy, mode, &g);
+}
+
 // Workspace layouts. On a ring plan without an NTT for q (is_crt) a call
 // lifts its inputs into one residue buffer per auxiliary prime in turn (reused),
 // keeps the three residue results, and runs the prime's own call in the rest of
@@ -105,10 +113,18 @@ int commit_core(const grid_gpu_matrix* A, const uint32_t* s, size_t batch, uint3
   const size_t ew = emm_workspace_words(p, (int)batch, (int)A->rows, (int)A->cols, EMM_DENSE);
   uint32_t* work = ew ? cv.take<uint32_t>(ew) : nullptr;
   if (!cv.ok) return GRID_ERR_INVALID_PARAMETERS;
-  int rc = launch_ntt(p, MODE_FWD, s, nullptr, s_hat, batch * A->cols, st);
-  if (rc) return rc;
-  rc = launch_emm(p, s_hat, A->d_evals, (int)batch, (int)A->rows, (int)A->cols, (int)A->ld,
-                  EMM_DENSE, t, work, st);
+  int rc;
+  if (A->d_evals_pm && pm_fits(p, batch, A->rows, A->cols, A->ld, EMM_DENSE)) {
+    rc = launch_ntt_tc(p, MODE_FWD_PM, s, nullptr, s_hat, batch * A->cols, st);
+    if (!rc)
+      rc = launch_emm_pm(p, s_hat, A->d_evals_pm, (int)batch, (int)A->rows, (int)A->cols,
+                         (int)A->ld, EMM_DENSE, t, work, st);
+  } else {
+    rc = launch_ntt(p, MODE_FWD, s, nullptr, s_hat, batch * A->cols, st);
+    if (!rc)
+      rc = launch_emm(p, s_hat, A->d_evals, (int)batch, (int)A->rows, (int)A->cols, (int)A->ld,
+                      EMM_DENSE, t, work, st);
+  }
   if (rc) return rc;
   return launch_ntt(p, MODE_INV, t, nullptr, t, batch * A->rows, st);
 }
@@ -173,9 +189,15 @@ int grid_gpu_matrix_create_dev(grid_gpu_plan* p, const uint32_t* A, size_t rows,
   } else {
     rc = launch_ntt(p, MODE_FWD, A, nullptr, m->d_evals, rows * cols, st);
   }
+  // a point-major copy for products on the TMA-fed tensor-core kernel
+  EmmPmGeometry pg;
+  if (!rc && ntt_tc_available(p) &&
+      emm_pm_geometry(p, 1, (int)rows, (int)cols, (int)cols, EMM_DENSE, &pg)) {
+    rc = cuda_status(cudaMalloc(&m->d_evals_pm, rows * cols * p->d * 4));
+    if (!rc) rc = launch_to_point_major(m->d_evals, m->d_evals_pm, rows * cols, (int)p->d, st);
+  }
   if (rc) {
-    cudaFree(m->d_evals);
-    delete m;
+    grid_gpu_matrix_destroy(m);
     return rc;
   }
   *out = m;
@@ -209,6 +231,7 @@ int grid_gpu_matrix_destroy(grid_gpu_matrix* m) {
   for (grid_gpu_matrix* sub : m->crt)
     if (sub) grid_gpu_matrix_destroy(sub);
   if (m->owned && m->d_evals) cudaFree(m->d_evals);
+  if (m->owned && m->d_evals_pm) cudaFree(m->d_evals_pm);
   delete m;
   return GRID_OK;
 }
@@ -224,6 +247,7 @@ int grid_gpu_matrix_view(const grid_gpu_matrix* parent, size_t cols, grid_gpu_ma
   m->cols = cols;
   m->ld = parent->ld;
   m->d_evals = parent->d_evals;
+  m->d_evals_pm = parent->d_evals_pm;
   m->owned = false;
   for (int j = 0; j < 3; ++j)
     if (parent->crt[j]) {
@@ -479,6 +503,13 @@ int grid_gpu_gram_dev(const grid_gpu_plan* p, const uint32_t* S, size_t r, size_
     if (is_crt(p)) {
       rc = lift_one(p, j, S, r * n * p->d, s_hat, st);
       if (!rc) rc = launch_ntt(q, MODE_FWD, s_hat, nullptr, s_hat, r * n, st);
+    } else if (pm_fits(q, r, r, n, n, EMM_UPPER)) {
+      rc = launch_ntt_tc(q, MODE_FWD_PM, S, nullptr, s_hat, r * n, st);
+      if (!rc)
+        rc = launch_emm_pm(q, s_hat, s_hat, (int)r, (int)r, (int)n, (int)n, EMM_UPPER, out, work,
+                           st);
+      if (!rc) rc = launch_ntt(q, MODE_INV, out, nullptr, out, r * (r + 1) / 2, st);
+      continue;
     } else {
       rc = launch_ntt(q, MODE_FWD, S, nullptr, s_hat, r * n, st);
     }
@@ -537,12 +568,19 @@ int grid_gpu_garbage_h_dev(const grid_gpu_plan* p, const uint32_t* S, const uint
   uint32_t* work = ew ? cv.take<uint32_t>(ew) : nullptr;
   if (!is_crt(p)) {
     if (!cv.ok) return GRID_ERR_INVALID_PARAMETERS;
-    int rc = launch_ntt(p, MODE_FWD, S, nullptr, s_hat, r * n, st);
-    if (!rc) rc = launch_ntt(p, MODE_FWD, Phi, nullptr, phi_hat, r * n, st);
     // cross[i][j] = <phi_i, s_j>
+    const bool pm = pm_fits(p, r, r, n, n, EMM_DENSE);
+    const int fwd = pm ? MODE_FWD_PM : MODE_FWD;
+    int rc = pm ? launch_ntt_tc(p, fwd, S, nullptr, s_hat, r * n, st)
+                : launch_ntt(p, fwd, S, nullptr, s_hat, r * n, st);
     if (!rc)
-      rc = launch_emm(p, phi_hat, s_hat, (int)r, (int)r, (int)n, (int)n, EMM_DENSE, cross, work,
-                      st);
+      rc = pm ? launch_ntt_tc(p, fwd, Phi, nullptr, phi_hat, r * n, st)
+              : launch_ntt(p, fwd, Phi, nullptr, phi_hat, r * n, st);
+    if (!rc)
+      rc = pm ? launch_emm_pm(p, phi_hat, s_hat, (int)r, (int)r, (int)n, (int)n, EMM_DENSE, cross,
+                              work, st)
+              : launch_emm(p, phi_hat, s_hat, (int)r, (int)r, (int)n, (int)n, EMM_DENSE, cross,
+                           work, st);
     if (!rc) rc = launch_symmetrize_half(p, cross, (int)r, H, st);
     if (rc) return rc;
     return launch_ntt(p, MODE_INV, H, nullptr, H, r * (r + 1) / 2, st);
@@ -910,6 +948,20 @@ int grid_gpu_prover_round_dev(const grid_gpu_matrix* A, const uint32_t* S, size_
   // transform shared by both) on plan q into tt / gg
   auto contract = [&](const grid_gpu_plan* q, const grid_gpu_matrix* Aq, const uint32_t* src,
                       uint32_t* tt, uint32_t* gg, cudaStream_t cs) {
+    if (src != s_hat && Aq->d_evals_pm && pm_fits(q, r, kappa, n, Aq->ld, EMM_DENSE) &&
+        pm_fits(q, r, r, n, n, EMM_UPPER)) {
+      // point-major evaluations: both products load their operands with TMA
+      int rc = launch_ntt_tc(q, MODE_FWD_PM, src, nullptr, s_hat, r * n, cs);
+      if (!rc)
+        rc = launch_emm_pm(q, s_hat, Aq->d_evals_pm, (int)r, (int)kappa, (int)n, (int)Aq->ld,
+                           EMM_DENSE, tt, work, cs);
+      if (!rc) rc = launch_ntt(q, MODE_INV, tt, nullptr, tt, r * kappa, cs);
+      if (!rc)
+        rc = launch_emm_pm(q, s_hat, s_hat, (int)r, (int)r, (int)n, (int)n, EMM_UPPER, gg, work,
+                           cs);
+      if (!rc) rc = launch_ntt(q, MODE_INV, gg, nullptr, gg, r * (r + 1) / 2, cs);
+      return rc;
+    }
     int rc = launch_ntt(q, MODE_FWD, src, nullptr, s_hat, r * n, cs);
     if (!rc)
       rc = launch_emm(q, s_hat, Aq->d_evals, (int)r, (int)kappa, (int)n, (int)Aq->ld, EMM_DENSE,

@@ -288,7 +288,9 @@ size_t emm_workspace_words(const grid_gpu_plan* p, int M, int N, int K, int mode
   EmmTcGeometry tg;
   const int splits = !g.mv && emm_tc_geometry(p, M, N, K, mode, &tg) ? tg.splits : g.splits;
   const size_t outputs = mode == OUT_UPPER ? (size_t)M * (M + 1) / 2 : (size_t)M * N;
-  return splits > 1 ? (size_t)splits * outputs * p->d : 0;
+  const size_t words = splits > 1 ? (size_t)splits * outputs * p->d : 0;
+  const size_t pm = emm_pm_workspace_words(p, M, N, K, mode);  // point-major operands
+  return words > pm ? words : pm;
 }
 
 // out_evals: dense [M][N][d] or packed-upper [M(M+1)/2][d]. work: >= emm_workspace_words.
@@ -320,14 +322,48 @@ int launch_emm(const grid_gpu_plan* p, const uint32_t* X, const uint32_t* Y, int
   if (rc) return rc;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_status(e);
-  if (splits > 1) {
-    size_t blocks = (stride + 255) / 256;
-    if (blocks > (size_t)p->num_sms * 8) blocks = (size_t)p->num_sms * 8;
-    sum_splits_kernel<<<(unsigned)blocks, 256, 0, s>>>(work, out_evals, stride, splits, p->f.q);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return cuda_status(e);
+  return splits > 1 ? launch_sum_splits(p, work, out_evals, stride, splits, s) : GRID_OK;
+}
+
+int launch_sum_splits(const grid_gpu_plan* p, const uint32_t* work, uint32_t* out, size_t stride,
+                      int splits, cudaStream_t s) {
+  size_t blocks = (stride + 255) / 256;
+  if (blocks > (size_t)p->num_sms * 8) blocks = (size_t)p->num_sms * 8;
+  sum_splits_kernel<<<(unsigned)blocks, 256, 0, s>>>(work, out, stride, splits, p->f.q);
+  return cuda_status(cudaGetLastError());
+}
+
+namespace {
+
+// out[e][i] = in[i][e]: 32 x 32 tiles through shared memory.
+__global__ void to_point_major_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
+                                      size_t npolys, int d) {
+  __shared__ uint32_t t[32][33];
+  const size_t i0 = (size_t)blockIdx.x * 32;
+  const int e0 = blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const size_t i = i0 + r;
+    const int e = e0 + threadIdx.x;
+    if (i < npolys && e < d) t[r][threadIdx.x] = in[i * d + e];
   }
-  return GRID_OK;
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int e = e0 + r;
+    const size_t i = i0 + threadIdx.x;
+    if (i < npolys && e < d) out[(size_t)e * npolys + i] = t[threadIdx.x][r];
+  }
+}
+
+}  // namespace
+
+int launch_to_point_major(const uint32_t* in, uint32_t* out, size_t npolys, int d,
+                          cudaStream_t s) {
+  if (npolys == 0) return GRID_OK;
+  const size_t bx = (npolys + 31) / 32;
+  if (bx > 0x7fffffffu) return GRID_ERR_INVALID_PARAMETERS;
+  to_point_major_kernel<<<dim3((unsigned)bx, (d + 31) / 32), dim3(32, 8), 0, s>>>(in, out, npolys,
+                                                                                   d);
+  return cuda_status(cudaGetLastError());
 }
 
 }  // namespace grid

@@ -41,6 +41,7 @@ enum NttMode : int {
   MODE_INV = 1,     // twisted evaluations -> coefficients
   MODE_MULINV = 2,  // out = INTT(NTT(a) (.) b_evals)
   MODE_POLYMUL = 3, // out = INTT(NTT(a) (.) NTT(b))  (negacyclic product)
+  MODE_FWD_PM = 4,  // MODE_FWD stored point-major: out[e * npolys + poly] (d = 64 tensor cores)
 };
 
 struct DeviceScratch {
@@ -76,6 +77,7 @@ struct grid_gpu_plan {
   // twist constants of the products. Null selects the CUDA-core kernels.
   void* d_tcw = nullptr;
   bool tc_emm = false;  // evaluation-domain products on the tensor cores where the shape allows
+  bool pm_emm = false;  // ... over point-major evaluations loaded by TMA (emm_pm.cu)
   int* d_err = nullptr;
   cudaStream_t stream = nullptr;   // host-buffer entry points: first pipeline stream
   cudaStream_t stream2 = nullptr;  // second pipeline stream
@@ -98,6 +100,9 @@ struct grid_gpu_matrix {
   size_t rows = 0, cols = 0;
   size_t ld = 0;                // row stride in polys (cols of the owning matrix)
   uint32_t* d_evals = nullptr;  // rows x ld polys in the twisted evaluation domain
+  // The same evaluations point-major, [d][rows][ld], for the tensor-core
+  // contraction over TMA-loaded operands (null where that path does not apply).
+  uint32_t* d_evals_pm = nullptr;
   bool owned = true;            // false for views sharing another matrix's evaluations
   // On a ring plan without an NTT for q: the matrix's residues mod each
   // auxiliary prime, prepared on that prime's plan (d_evals stays null).
@@ -145,6 +150,24 @@ bool emm_tc_geometry(const grid_gpu_plan* p, int M, int N, int K, int mode, EmmT
 int launch_emm_tc(const grid_gpu_plan* p, const uint32_t* X, const uint32_t* Y, int M, int N,
                   int K, int ldy, int mode, uint32_t* dst, const EmmTcGeometry& g, size_t stride,
                   cudaStream_t s);
+// out[i] = sum over splits s of work[s * stride + i] (mod q)
+int launch_sum_splits(const grid_gpu_plan* p, const uint32_t* work, uint32_t* out, size_t stride,
+                      int splits, cudaStream_t s);
+// emm_pm.cu: the same products over point-major operands, X [d][M][K] and
+// Y [d][N][ldy] (tensor cores, TMA; X rows <= 128, Y rows <= 64, K and ldy
+// multiples of 4, 16-byte aligned bases). Split partials go to `work`.
+struct EmmPmGeometry {
+  int np;  // Y rows padded to 16, 32, 48 or 64
+  int splits, k_per_split;
+};
+bool emm_pm_geometry(const grid_gpu_plan* p, int M, int N, int K, int ldy, int mode,
+                     EmmPmGeometry* g);
+size_t emm_pm_workspace_words(const grid_gpu_plan* p, int M, int N, int K, int mode);
+int launch_emm_pm(const grid_gpu_plan* p, const uint32_t* X, const uint32_t* Y, int M, int N,
+                  int K, int ldy, int mode, uint32_t* out_evals, uint32_t* work, cudaStream_t s);
+// in [npolys][d] -> out [d][npolys] (point-major copy of evaluations)
+int launch_to_point_major(const uint32_t* in, uint32_t* out, size_t npolys, int d,
+                          cudaStream_t s);
 // garbage.cu: (C_ij + C_ji) * 2^-1 on the upper triangle; z_hat = sum_i c_hat_i (.) s_hat_i.
 int launch_symmetrize_half(const grid_gpu_plan* p, const uint32_t* C, int r, uint32_t* H,
                            cudaStream_t s);

@@ -78,6 +78,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                   const uint32_t* __restrict__ b, unsigned long long npolys,
                   const uint4* __restrict__ wtab, const TcConsts k, int* __restrict__ err) {
   constexpr bool kTwo = MODE == MODE_MULINV;
+  constexpr bool kPm = MODE == MODE_FWD_PM;
   extern __shared__ __align__(1024) unsigned char sm_raw[];
   const uint32_t raw = smem_addr(sm_raw);
   unsigned char* sm = sm_raw + (((raw + 1023u) & ~1023u) - raw);
@@ -149,8 +150,12 @@ __global__ void __launch_bounds__(THREADS, 1)
         const uint32_t js = t - lag;
         ok = warp_wait_fast(&bars[STAGED0 + buf], staged_seen[buf]++ & 1, err);
         if (ok && lane == 0) {
-          tma_store_2d(&tmap_out, 0, (int)tile_row0(js), dst);
-          tma_store_2d(&tmap_out, 32, (int)tile_row0(js), dst + BOX);
+          if constexpr (kPm) {  // [64 points][128 polys] -> columns row0.. of the [d][npolys] output
+            tma_store_2d(&tmap_out, (int)tile_row0(js), 0, dst);
+          } else {
+            tma_store_2d(&tmap_out, 0, (int)tile_row0(js), dst);
+            tma_store_2d(&tmap_out, 32, (int)tile_row0(js), dst + BOX);
+          }
           bulk_commit();
           bulk_wait_read_all();  // the buffer may be refilled once the store has read it
         }
@@ -215,12 +220,20 @@ __global__ void __launch_bounds__(THREADS, 1)
     const uint32_t lane_off = ((32 * wl) << 16) + 16 * cq;
     bool ok = true;
 
-    // 16 words (columns 16 cq .. + 15 of this row) into a swizzled tile
+    // 16 words (columns 16 cq .. + 15 of this row) into a swizzled tile; the
+    // point-major mode writes the tile transposed, [point][row] (a warp's 32
+    // rows of one point are 32 consecutive words: no bank conflict)
     auto put_row = [&](unsigned char* tile, const uint32_t* res) {
+      if constexpr (kPm) {
+        uint32_t* t = reinterpret_cast<uint32_t*>(tile);
 #pragma unroll
-      for (int c = 0; c < 4; ++c)
-        *reinterpret_cast<uint4*>(tile + sw128(row, cq >> 1, (cq & 1) * 4 + c, BOX)) =
-            make_uint4(res[4 * c], res[4 * c + 1], res[4 * c + 2], res[4 * c + 3]);
+        for (int c = 0; c < 16; ++c) t[(16 * cq + c) * ROWS + row] = res[c];
+      } else {
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+          *reinterpret_cast<uint4*>(tile + sw128(row, cq >> 1, (cq & 1) * 4 + c, BOX)) =
+              make_uint4(res[4 * c], res[4 * c + 1], res[4 * c + 2], res[4 * c + 3]);
+      }
     };
     // Result tile j -> buffer (j + off) & 1 (a tile whose forward is done)
     auto stage = [&](uint32_t j, const uint32_t* res) {
@@ -296,27 +309,6 @@ __global__ void __launch_bounds__(THREADS, 1)
   }
 }
 
-using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
-                                 const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
-                                 const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
-                                 CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-// The driver's tensor-map encoder, looked up once through the runtime (the
-// library does not link the driver library directly).
-EncodeTiled encoder() {
-  static EncodeTiled fn = nullptr;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
-            cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<EncodeTiled>(p);
-  });
-  return fn;
-}
-
 template <int MODE>
 int run_tc(const grid_gpu_plan* p, const uint32_t* a, const uint32_t* b, uint32_t* out,
            size_t npolys, cudaStream_t s) {
@@ -334,6 +326,16 @@ int run_tc(const grid_gpu_plan* p, const uint32_t* a, const uint32_t* b, uint32_
             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
       return GRID_ERR_CUDA;
+  if (MODE == MODE_FWD_PM) {
+    // output [64 points][npolys], one box of 128 polys x 64 points per tile
+    const cuuint64_t pdims[2] = {(cuuint64_t)npolys, 64};
+    const cuuint64_t pstrides[1] = {(cuuint64_t)npolys * 4};
+    const cuuint32_t pbox[2] = {ROWS, 64};
+    if (enc(&map_out, CU_TENSOR_MAP_DATA_TYPE_UINT32, 2, (void*)out, pdims, pstrides, pbox, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return GRID_ERR_CUDA;
+  }
   static int bps_cache[kMaxDevices] = {};
   int bps = 0;
   const int st =
@@ -353,6 +355,22 @@ int run_tc(const grid_gpu_plan* p, const uint32_t* a, const uint32_t* b, uint32_
 
 }  // namespace
 
+// The driver's tensor-map encoder, looked up once through the runtime (the
+// library does not link the driver library directly).
+tcx::EncodeTiled tcx::encoder() {
+  static EncodeTiled fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiled>(p);
+  });
+  return fn;
+}
+
 bool ntt_tc_available(const grid_gpu_plan* p) { return p->d == 64 && p->d_tcw != nullptr; }
 
 int launch_ntt_tc(const grid_gpu_plan* p, int mode, const uint32_t* a, const uint32_t* b,
@@ -363,6 +381,11 @@ int launch_ntt_tc(const grid_gpu_plan* p, int mode, const uint32_t* a, const uin
     case MODE_FWD: return run_tc<MODE_FWD>(p, a, nullptr, out, npolys, s);
     case MODE_INV: return run_tc<MODE_INV>(p, a, nullptr, out, npolys, s);
     case MODE_MULINV: return run_tc<MODE_MULINV>(p, a, b, out, npolys, s);
+    case MODE_FWD_PM:
+      // the row stride of the [64][npolys] output is a multiple of 16 bytes;
+      // tiles of other CTAs still read the input while a tile's columns land
+      if (npolys % 4 || a == out) return GRID_ERR_INVALID_PARAMETERS;
+      return run_tc<MODE_FWD_PM>(p, a, nullptr, out, npolys, s);
     default: return GRID_ERR_INVALID_PARAMETERS;
   }
 }

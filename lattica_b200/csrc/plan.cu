@@ -357,6 +357,14 @@ bool use_tensor_cores() {
   return !(v && std::strcmp(v, "cuda_core") == 0);
 }
 
+// Contractions over point-major evaluations (TMA-fed) unless
+// GRID_GPU_CONTRACTION=gather selects the poly-major kernels that gather
+// their operands.
+bool use_point_major() {
+  const char* v = std::getenv("GRID_GPU_CONTRACTION");
+  return !(v && std::strcmp(v, "gather") == 0);
+}
+
 // Device state every plan owns: SM count, error word, the host-buffer
 // pipeline's streams and the fork streams of *_dev calls (on the current device).
 cudaError_t init_device_state(grid_gpu_plan* p) {
@@ -475,6 +483,7 @@ int grid_gpu_plan_create(uint64_t q, uint64_t d, grid_gpu_plan** out) {
     if ((e = cudaMemcpy(p->d_tw, dev_tw.data(), dev_tw.size() * sizeof(uint2),
                         cudaMemcpyHostToDevice)) != cudaSuccess) break;
     p->tc_emm = use_tensor_cores();
+    p->pm_emm = p->tc_emm && use_point_major();
     if ((d == 64 || d == 256) && use_tensor_cores()) {
       std::vector<unsigned char> tcw;
       if (d == 64)

@@ -4,11 +4,13 @@
 * The LaBRADOR prover round at r = 64, n = 2048, kappa = 16 (every word of the
   t limbs, g, g limbs and p; sampled rows of the 2 GiB JL entries) and the
   checks verify_step applies to those outputs.
-* The tensor-core contraction's int32 bound: one CTA accumulates at most 8192
+* The tensor-core contractions' int32 bound: one CTA accumulates at most 8192
   K words, D_l = sum_{k,i} byte_i(x_k) byte_l(2^(8i) y_k mod q) < 4 * 8192 *
   255^2 = 2,130,739,200 < 2^31. Words are chosen so that one byte plane comes
-  within 1.2 % of 2^31 at exactly 8192 words per CTA, and one word past it
-  (the split boundary).
+  within 1.2 % of 2^31 at exactly 8192 words per CTA, and past it (the split
+  boundary: one word, which only the gathering kernel takes, K not a multiple
+  of 4; four words, a last range of one partial chunk), on the point-major
+  kernel and on the gathering one.
 * The uneven batch (4096 instances, n log-uniform in [64, 8192]) at full size,
   32 instances against the oracle.
 """
@@ -87,14 +89,29 @@ def _const_polys(word, count, d=64):
 
 def _k_per_cta_8192(cuda, groups):
     """K at which the contraction gives every CTA exactly 8192 words: the
-    geometry splits K over num_sms // groups CTAs per evaluation group."""
+    gathering geometry splits K over num_sms // groups CTAs per evaluation
+    group; the point-major one caps every range at 8192 words, fewer ranges
+    than this K needs (2 num_sms / 64 per point)."""
     import torch
     sms = torch.cuda.get_device_properties(cuda).multi_processor_count
     return max(1, sms // groups) * 8192
 
 
-@pytest.mark.parametrize("extra", [0, 1])
-def test_contraction_bound_commit_at_8192_words_per_cta(cuda, extra):
+def _plan(gather):
+    import os
+    from lattica_b200 import TwistedNttPlan
+    if not gather:
+        return TwistedNttPlan(Q, 64)
+    os.environ["GRID_GPU_CONTRACTION"] = "gather"
+    try:
+        return TwistedNttPlan(Q, 64)
+    finally:
+        del os.environ["GRID_GPU_CONTRACTION"]
+
+
+@pytest.mark.parametrize("gather", [False, True])
+@pytest.mark.parametrize("extra", [0, 1, 4])
+def test_contraction_bound_commit_at_8192_words_per_cta(cuda, extra, gather):
     """t = A s with every evaluation of s equal to x = 0xFEFFFFFF (bytes FF FF FF
     FE) and of A equal to y = 0xFEFEFD82, whose byte-3 plane sums to 99.6 % of
     4 * 255^2 per word: 98.8 % of 2^31 in each CTA."""
@@ -107,7 +124,7 @@ def test_contraction_bound_commit_at_8192_words_per_cta(cuda, extra):
     assert plane3 * 8192 > 0.988 * 2 ** 31 and 4 * 8192 * 255 ** 2 < 2 ** 31
     rows, batch = 16, 8          # Y rows <= 16: 4 evaluation points per CTA, 16 groups
     K = _k_per_cta_8192(cuda, 16) + extra
-    plan = TwistedNttPlan(Q, 64)
+    plan = _plan(gather)
     A = _dev(_const_polys(y, rows * K), cuda).view(rows, K, 64)
     M = PreparedMatrix(plan, A, rows, K)
     del A
@@ -120,8 +137,9 @@ def test_contraction_bound_commit_at_8192_words_per_cta(cuda, extra):
     plan.check_device()
 
 
-@pytest.mark.parametrize("extra", [0, 1])
-def test_contraction_bound_gram_at_8192_words_per_cta(cuda, extra):
+@pytest.mark.parametrize("gather", [False, True])
+@pytest.mark.parametrize("extra", [0, 1, 4])
+def test_contraction_bound_gram_at_8192_words_per_cta(cuda, extra, gather):
     """Gram (X = Y) with every evaluation equal to c = 3488348921, the word whose
     largest byte plane is highest among 4 * 10^7 sampled words (89 % of 2^31 per
     CTA)."""
@@ -131,7 +149,7 @@ def test_contraction_bound_gram_at_8192_words_per_cta(cuda, extra):
     c = 3488348921
     r = 16
     K = _k_per_cta_8192(cuda, 16) + extra
-    plan = TwistedNttPlan(Q, 64)
+    plan = _plan(gather)
     S = _dev(_const_polys(c, r * K), cuda).view(r, K, 64)
     g = compute_garbage_g(plan, S)
     torch.cuda.synchronize()
