@@ -79,14 +79,14 @@ struct PmShape {
   static_assert(NSB * BSLOT >= (UPPER ? 64u * 65 / 2 : (uint32_t)MX * NP) * 4, "staging");
 };
 
-// Bounded wait by lane 0, then one poll by every other lane, which returns at
-// once and acquires the phase's writes for that lane.
+// Bounded wait by lane 0 alone (mbarrier operations of a whole warp on one
+// barrier serialise over its lanes); __syncwarp then orders what lane 0
+// acquired before every lane's later accesses.
 __device__ __forceinline__ bool lane0_wait(uint64_t* bar, uint32_t parity, int lane, int* err) {
   bool ok = true;
   if (lane == 0) ok = mbar_wait(bar, parity, err);
-  ok = __shfl_sync(0xffffffffu, ok, 0);
-  if (ok && lane) mbar_try_wait(bar, parity);
-  return ok;
+  __syncwarp();
+  return __shfl_sync(0xffffffffu, ok, 0);
 }
 
 // The builder warps' own barrier (named barrier 1; the CTA's is 0).
@@ -282,8 +282,14 @@ __global__ void sum_transpose_kernel(const uint32_t* __restrict__ part, uint32_t
     const int e = e0 + r, i = i0 + threadIdx.x;
     if (e < d && i < outputs) {
       const uint32_t* src = part + (size_t)e * outputs + i;
-      uint32_t v = src[0];
-      for (int s = 1; s < splits; ++s) v = add_mod(v, src[(size_t)s * stride], q);
+      uint32_t v = 0;
+      for (int s0 = 0; s0 < splits; s0 += 4) {  // four independent loads in flight
+        uint32_t w[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) w[j] = s0 + j < splits ? src[(size_t)(s0 + j) * stride] : 0u;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) v = add_mod(v, w[j], q);
+      }
       t[r][threadIdx.x] = v;
     }
   }
@@ -398,7 +404,7 @@ int launch_emm_pm(const grid_gpu_plan* p, const uint32_t* X, const uint32_t* Y, 
   // point-major partials [split][e][output] -> out [output][e]
   const int outputs = mode == EMM_UPPER ? M * (M + 1) / 2 : M * N;
   const int d = (int)p->d;
-  sum_transpose_kernel<<<dim3((outputs + 31) / 32, (d + 31) / 32), dim3(32, 8), 0, s>>>(
+  sum_transpose_kernel<<<dim3((outputs + 31) / 32, (d + 31) / 32), dim3(32, 32), 0, s>>>(
       work, out_evals, outputs, d, g.splits, p->f.q);
   return cuda_status(cudaGetLastError());
 }
