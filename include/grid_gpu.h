@@ -347,9 +347,17 @@ typedef struct grid_gpu_batch_item {
 } grid_gpu_batch_item;
 /* Engines of the grouped product: AUTO = the tensor cores where the plan
  * allows (d % 4 == 0, tensor-core plan), else the CUDA cores; TENSOR requires
- * them (else GRID_ERR_UNSUPPORTED_DEGREE); CUDA_CORE never uses them. Both give
- * the same words. */
-enum { GRID_GPU_ENGINE_AUTO = 0, GRID_GPU_ENGINE_TENSOR = 1, GRID_GPU_ENGINE_CUDA_CORE = 2 };
+ * them (else GRID_ERR_UNSUPPORTED_DEGREE); CUDA_CORE never uses them;
+ * POINT_MAJOR runs the tensor cores over point-major evaluations (the
+ * witnesses' transform stores [point][poly]; every matrix needs its
+ * point-major copy: d = 64, rows <= 32, cols a multiple of 4, else
+ * GRID_ERR_UNSUPPORTED_DEGREE). All give the same words. */
+enum {
+  GRID_GPU_ENGINE_AUTO = 0,
+  GRID_GPU_ENGINE_TENSOR = 1,
+  GRID_GPU_ENGINE_CUDA_CORE = 2,
+  GRID_GPU_ENGINE_POINT_MAJOR = 3
+};
 typedef struct grid_gpu_batch_config {
   uint32_t k_split;        /* K range of one work item (multiple of 16, <= 8192) */
   uint32_t work_items;     /* output of get_config */

@@ -40,7 +40,7 @@ class GramItem(C.Structure):
     _fields_ = [("s_offset", C.c_uint64), ("r", C.c_uint32), ("n", C.c_uint32)]
 
 
-ENGINE_AUTO, ENGINE_TENSOR, ENGINE_CUDA_CORE = 0, 1, 2
+ENGINE_AUTO, ENGINE_TENSOR, ENGINE_CUDA_CORE, ENGINE_POINT_MAJOR = 0, 1, 2, 3
 
 
 class PlanInfo(C.Structure):

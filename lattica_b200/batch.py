@@ -31,7 +31,7 @@ from .ntt import TwistedNttPlan, _stream_ptr, raise_status
 K_SPLIT_CANDIDATES = (1024, 2048, 4096, 8192)
 TILE_CANDIDATES = (0, 64, 32)  # instances per tile (0: the engine's largest, 128)
 ENGINE_NAMES = {_lib.ENGINE_AUTO: "auto", _lib.ENGINE_TENSOR: "tensor",
-                _lib.ENGINE_CUDA_CORE: "cuda_core"}
+                _lib.ENGINE_CUDA_CORE: "cuda_core", _lib.ENGINE_POINT_MAJOR: "point_major"}
 
 
 def default_cache_path() -> str:
@@ -127,6 +127,7 @@ class UnevenCommitBatch:
         the tensor cores, and the CUDA-core kernel with its own tiles."""
         out = [(k, ti, _lib.ENGINE_TENSOR) for ti in TILE_CANDIDATES for k in k_splits]
         out += [(k, 0, _lib.ENGINE_CUDA_CORE) for k in k_splits]
+        out += [(k, ti, _lib.ENGINE_POINT_MAJOR) for ti in TILE_CANDIDATES for k in k_splits]
         return out
 
     def autotune(self, s, t, candidates=None, reps: int = 3,

@@ -86,7 +86,8 @@ def _jl_extract(torch, dev, g, plan, parts, n):
 
 def _batch(torch, dev, g, plan, num, engine):
     """Uneven batched commits: num instances, n log-uniform in [64, 8192], rank
-    in {8, 16, 32}, one m x 8192 matrix per rank; engine: tensor or cuda_core."""
+    in {8, 16, 32}, one m x 8192 matrix per rank; engine: tensor, cuda_core or
+    point_major."""
     from lattica_b200 import _lib
     from lattica_b200.batch import UnevenCommitBatch, sample_uneven_instances
     from lattica_b200.commit import PreparedMatrix
@@ -97,7 +98,9 @@ def _batch(torch, dev, g, plan, num, engine):
     s = ((tern % Q) * ((1 << 32) % Q) % Q).to(torch.int32)
     t = torch.empty((t_polys, 64), dtype=torch.int32, device=dev)
     batch = UnevenCommitBatch(plan, mats, items)
-    batch.set_config(4096, 0, _lib.ENGINE_TENSOR if engine == "tensor" else _lib.ENGINE_CUDA_CORE)
+    engines = {"tensor": _lib.ENGINE_TENSOR, "cuda_core": _lib.ENGINE_CUDA_CORE,
+               "point_major": _lib.ENGINE_POINT_MAJOR}
+    batch.set_config(4096, 0, engines[engine])
     run = lambda: batch.commit_dev(s, t)
     run.keep = (mats, batch)
     return run
@@ -178,7 +181,7 @@ def main(argv=None) -> None:
     ap.add_argument("--reps", type=int, default=4)
     ap.add_argument("--parts", type=int, default=64,
                     help="witness vectors (jl_extract), instances (batch, gram_batch)")
-    ap.add_argument("--engine", choices=["tensor", "cuda_core"], default="tensor",
+    ap.add_argument("--engine", choices=["tensor", "cuda_core", "point_major"], default="tensor",
                     help="grouped-product engine of the batch case")
     args = ap.parse_args(argv)
     import torch

@@ -206,6 +206,7 @@ struct grid_gpu_batch {
   uint32_t tile_instances = 0;    // 0: the engine's default
   int engine = GRID_GPU_ENGINE_AUTO;
   bool tc = false;                // the tensor-core kernel runs the grouped product
+  bool pm = false;                // ... over point-major evaluations (grouped_pm.cu)
   unsigned class_begin[TC_CLASSES + 1] = {};
   // device tables
   MatDev* d_mats = nullptr;
@@ -213,6 +214,10 @@ struct grid_gpu_batch {
   TileDev* d_tiles = nullptr;
   WorkDev* d_work = nullptr;
   unsigned nwork = 0;
+  // point-major engine: the witnesses' transform tile list, the padded rows
+  uint4* d_xtiles = nullptr;
+  unsigned long long nxtiles = 0;
+  uint64_t s_region = 0;  // polys per point of the transformed witnesses
   // captured graphs, keyed by (s, t, workspace, stream)
   std::mutex mu;
   std::map<std::tuple<const void*, void*, void*, void*>, cudaGraphExec_t> graphs;
@@ -229,13 +234,19 @@ struct Tables {
   uint64_t s_polys = 0, t_polys = 0;
   uint32_t k_split = 0;
   bool tc = false;
+  bool pm = false;
   unsigned class_begin[TC_CLASSES + 1] = {};
+  // Point-major layout: instance i's polys at a column of a multiple of 128
+  // (ItemDev::s_off of the point-major tables), the transform's tile list.
+  uint64_t pm_polys = 0;
+  std::vector<uint4> xtiles;
 };
 
 // Evaluation groups of a tile: 8 points per CUDA-core work item; 4 or 2 per
-// tensor-core work item (by the tile's Y rows).
+// tensor-core work item (by the tile's Y rows); one per point-major item.
 uint32_t tile_groups(const Tables& tb, const TileDev& tl, uint32_t d) {
   if (!tb.tc) return d / EG;
+  if (tb.pm) return d;
   const uint32_t ny = tl.matrix == kUpperTile ? tl.count : tb.mats[tl.matrix].rows;
   return d / (uint32_t)tc_points(ny);
 }
@@ -303,17 +314,26 @@ int build_tables(const grid_gpu_plan* plan, grid_gpu_matrix* const* mats, size_t
   if (nmats == 0 || nitems == 0 || nitems > (1u << 30)) return GRID_ERR_INVALID_PARAMETERS;
   if (k_split != 0 && (k_split < (uint32_t)KC || k_split % KC || k_split > kTcMaxK))
     return GRID_ERR_INVALID_PARAMETERS;
-  if (engine < GRID_GPU_ENGINE_AUTO || engine > GRID_GPU_ENGINE_CUDA_CORE)
+  // point-major work items cover whole 32-word chunks
+  if (engine == GRID_GPU_ENGINE_POINT_MAJOR && k_split % 32) return GRID_ERR_INVALID_PARAMETERS;
+  if (engine < GRID_GPU_ENGINE_AUTO || engine > GRID_GPU_ENGINE_POINT_MAJOR)
     return GRID_ERR_INVALID_PARAMETERS;
   if (tile_instances != 0 && (tile_instances % 4 || tile_instances > kTcMaxTileRows))
     return GRID_ERR_INVALID_PARAMETERS;
-  tb.tc = engine_uses_tc(plan, engine);
+  tb.pm = engine == GRID_GPU_ENGINE_POINT_MAJOR;
+  tb.tc = tb.pm || engine_uses_tc(plan, engine);
   if (engine == GRID_GPU_ENGINE_TENSOR && !tb.tc) return GRID_ERR_UNSUPPORTED_DEGREE;
+  // the point-major engine needs the point-major forward transform (d = 64,
+  // tensor cores) and every matrix's point-major evaluations
+  if (tb.pm && !(plan->pm_emm && ntt_tc_available(plan))) return GRID_ERR_UNSUPPORTED_DEGREE;
+  for (size_t i = 0; tb.pm && i < nmats; ++i)
+    if (mats[i] && !mats[i]->d_evals_pm) return GRID_ERR_UNSUPPORTED_DEGREE;
   for (size_t i = 0; i < nmats; ++i) {
     if (!mats[i]) return GRID_ERR_NULL_POINTER;
     if (mats[i]->plan != plan) return GRID_ERR_INVALID_PARAMETERS;
     if (mats[i]->rows > (size_t)TN) return GRID_ERR_INVALID_PARAMETERS;  // ranks up to 32
-    tb.mats.push_back(MatDev{mats[i]->d_evals, (uint32_t)mats[i]->rows, (uint32_t)mats[i]->ld});
+    tb.mats.push_back(MatDev{mats[i]->d_evals, mats[i]->d_evals_pm, (uint32_t)mats[i]->rows,
+                             (uint32_t)mats[i]->ld});
   }
   std::vector<std::pair<uint32_t, uint32_t>> order;  // (matrix, index)
   order.reserve(nitems);
@@ -323,12 +343,17 @@ int build_tables(const grid_gpu_plan* plan, grid_gpu_matrix* const* mats, size_t
       return GRID_ERR_DIMENSION_MISMATCH;
     tb.s_polys = std::max<uint64_t>(tb.s_polys, it.s_offset + it.n);
     tb.t_polys = std::max<uint64_t>(tb.t_polys, it.t_offset + mats[it.matrix]->rows);
+    tb.pm_polys += round_up(it.n, 128);  // the workspace does not depend on the engine
     order.emplace_back(it.matrix, (uint32_t)i);
   }
+  // transform tiles read rows s_offset .. and store columns .. below 2^31
+  if (tb.pm && (tb.s_polys > (uint64_t)INT32_MAX - 128 || tb.pm_polys > (uint64_t)INT32_MAX - 128))
+    return GRID_ERR_INVALID_PARAMETERS;
   std::stable_sort(order.begin(), order.end(), [&](const auto& x, const auto& y) {
     if (x.first != y.first) return x.first < y.first;
     return items[x.second].n > items[y.second].n;
   });
+  uint64_t pcol = 0;  // next point-major column
   for (size_t i = 0; i < order.size();) {
     const uint32_t m = order[i].first;
     size_t j = i;
@@ -337,7 +362,15 @@ int build_tables(const grid_gpu_plan* plan, grid_gpu_matrix* const* mats, size_t
     if (tile_instances) cap = std::min<size_t>(cap, tile_instances);
     while (j < order.size() && order[j].first == m && j - i < cap) {
       const grid_gpu_batch_item& it = items[order[j].second];
-      tb.sorted.push_back(ItemDev{it.s_offset, it.t_offset, it.n, 0});
+      uint64_t s_off = it.s_offset;
+      if (tb.pm) {  // the instance's own 128-aligned columns; the rest of its last tile is 0
+        for (uint32_t r = 0; r < it.n; r += 128)
+          tb.xtiles.push_back(make_uint4((uint32_t)(it.s_offset + r), (uint32_t)(pcol + r),
+                                         std::min<uint32_t>(128, it.n - r), 0));
+        s_off = pcol;
+        pcol += round_up(it.n, 128);
+      }
+      tb.sorted.push_back(ItemDev{s_off, it.t_offset, it.n, 0});
       tl.kmax = std::max(tl.kmax, it.n);
       ++j;
     }
@@ -350,15 +383,19 @@ int build_tables(const grid_gpu_plan* plan, grid_gpu_matrix* const* mats, size_t
   return GRID_OK;
 }
 
+uint64_t witness_region(uint64_t s_polys, uint64_t pm_polys);
+
 int upload(grid_gpu_batch* b) {
   for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
   b->graphs.clear();
-  for (void* ptr : {(void*)b->d_mats, (void*)b->d_items, (void*)b->d_tiles, (void*)b->d_work})
+  for (void* ptr : {(void*)b->d_mats, (void*)b->d_items, (void*)b->d_tiles, (void*)b->d_work,
+                    (void*)b->d_xtiles})
     if (ptr) cudaFree(ptr);
   b->d_mats = nullptr;
   b->d_items = nullptr;
   b->d_tiles = nullptr;
   b->d_work = nullptr;
+  b->d_xtiles = nullptr;
   Tables tb;
   int rc = build_tables(b->plan, b->mat_handles.data(), b->mat_handles.size(), b->items.data(),
                         b->items.size(), b->k_split, b->tile_instances, b->engine, tb);
@@ -369,6 +406,9 @@ int upload(grid_gpu_batch* b) {
   b->s_polys = tb.s_polys;
   b->t_polys = tb.t_polys;
   b->tc = tb.tc;
+  b->pm = tb.pm;
+  b->s_region = witness_region(tb.s_polys, tb.pm_polys);
+  b->nxtiles = tb.xtiles.size();
   std::copy(tb.class_begin, tb.class_begin + TC_CLASSES + 1, b->class_begin);
   b->nwork = (unsigned)tb.work.size();
   auto send = [](auto** dst, const auto& v) {
@@ -382,21 +422,28 @@ int upload(grid_gpu_batch* b) {
   if (e == cudaSuccess) e = send(&b->d_items, b->sorted);
   if (e == cudaSuccess) e = send(&b->d_tiles, b->tiles);
   if (e == cudaSuccess) e = send(&b->d_work, tb.work);
+  if (e == cudaSuccess && b->pm) e = send(&b->d_xtiles, tb.xtiles);
   return cuda_status(e);
 }
 
-// accumulators and one work counter per tensor-core class after the witness
-size_t core_bytes(uint64_t s_polys, uint64_t t_polys, size_t d) {
-  return round_up(s_polys * d * 4, 256) + round_up(t_polys * d * 8, 256) + 256;
+// The transformed witnesses, s_region polys per point (at least the packed
+// witness buffer's and the point-major engine's padded layout, a multiple of
+// 4), then the accumulators and one work counter per tensor-core class.
+uint64_t witness_region(uint64_t s_polys, uint64_t pm_polys) {
+  return std::max<uint64_t>((s_polys + 3) / 4 * 4, pm_polys);
+}
+size_t core_bytes(uint64_t s_region_polys, uint64_t t_polys, size_t d) {
+  return round_up(s_region_polys * d * 4, 256) + round_up(t_polys * d * 8, 256) + 256;
 }
 
-size_t ws_bytes(const grid_gpu_batch* b) { return core_bytes(b->s_polys, b->t_polys, b->plan->d); }
+size_t ws_bytes(const grid_gpu_batch* b) { return core_bytes(b->s_region, b->t_polys, b->plan->d); }
 
 // Grouped product -> fold -> INTT over given transformed witnesses and tables:
-// acc (t_polys x d u64) and the counters are cleared here.
-int run_product(const grid_gpu_plan* p, bool tc, const unsigned* class_begin,
+// acc (t_polys x d u64) and the counters are cleared here. pm: s_hat is
+// point-major with rows of ps polys (the point-major engine's tables).
+int run_product(const grid_gpu_plan* p, bool tc, bool pm, const unsigned* class_begin,
                 const MatDev* d_mats, const ItemDev* d_items, const TileDev* d_tiles,
-                const WorkDev* d_work, unsigned nwork, const uint32_t* s_hat,
+                const WorkDev* d_work, unsigned nwork, const uint32_t* s_hat, uint64_t ps,
                 unsigned long long* acc, unsigned* counters, uint64_t t_polys, uint32_t* t,
                 cudaStream_t st) {
   const size_t d = p->d;
@@ -404,7 +451,15 @@ int run_product(const grid_gpu_plan* p, bool tc, const unsigned* class_begin,
   if (e == cudaSuccess) e = cudaMemsetAsync(counters, 0, TC_CLASSES * sizeof(unsigned), st);
   if (e != cudaSuccess) return cuda_status(e);
   int rc = GRID_OK;
-  if (tc) {
+  if (pm) {
+    for (int c = 0; c < TC_CLASSES && !rc; ++c) {
+      const unsigned n = class_begin[c + 1] - class_begin[c];
+      if (n)
+        rc = launch_batch_pm(p, c, d_work + class_begin[c], n, d_tiles, d_items, d_mats, s_hat,
+                             ps, acc, st);
+    }
+    if (rc) return rc;
+  } else if (tc) {
     for (int c = 0; c < TC_CLASSES && !rc; ++c) {
       const unsigned n = class_begin[c + 1] - class_begin[c];
       if (n)
@@ -429,27 +484,32 @@ int run_product(const grid_gpu_plan* p, bool tc, const unsigned* class_begin,
   return launch_ntt(p, MODE_INV, t, nullptr, t, t_polys, st);
 }
 
-// NTT(s) -> grouped product -> fold -> INTT(t), with device tables given.
-int run_core(const grid_gpu_plan* p, bool tc, const unsigned* class_begin, const MatDev* d_mats,
-             const ItemDev* d_items, const TileDev* d_tiles, const WorkDev* d_work,
-             unsigned nwork, uint64_t s_polys, uint64_t t_polys, const uint32_t* s, uint32_t* t,
-             void* ws, cudaStream_t st) {
+// NTT(s) -> grouped product -> fold -> INTT(t), with device tables given
+// (layout of core_bytes).
+int run_core(const grid_gpu_plan* p, bool tc, bool pm, const unsigned* class_begin,
+             const MatDev* d_mats, const ItemDev* d_items, const TileDev* d_tiles,
+             const WorkDev* d_work, unsigned nwork, uint64_t s_polys, uint64_t ps, uint64_t t_polys,
+             const uint32_t* s, uint32_t* t, void* ws, cudaStream_t st,
+             const uint4* xtiles = nullptr, unsigned long long nxtiles = 0) {
   const size_t d = p->d;
   char* base = static_cast<char*>(ws);
   uint32_t* s_hat = reinterpret_cast<uint32_t*>(base);
   unsigned long long* acc =
-      reinterpret_cast<unsigned long long*>(base + round_up(s_polys * d * 4, 256));
-  unsigned* counters = reinterpret_cast<unsigned*>(base + round_up(s_polys * d * 4, 256) +
-                                                   round_up(t_polys * d * 8, 256));
-  const int rc = launch_ntt(p, MODE_FWD, s, nullptr, s_hat, s_polys, st);
+      reinterpret_cast<unsigned long long*>(base + round_up(ps * d * 4, 256));
+  unsigned* counters =
+      reinterpret_cast<unsigned*>(base + round_up(ps * d * 4, 256) + round_up(t_polys * d * 8, 256));
+  // point-major: [point][ps], every instance at its own 128-aligned columns
+  const int rc = pm ? launch_ntt_tc_pm_tiles(p, s, s_polys, s_hat, ps, xtiles, nxtiles, st)
+                    : launch_ntt(p, MODE_FWD, s, nullptr, s_hat, s_polys, st);
   if (rc) return rc;
-  return run_product(p, tc, class_begin, d_mats, d_items, d_tiles, d_work, nwork, s_hat, acc,
-                     counters, t_polys, t, st);
+  return run_product(p, tc, pm, class_begin, d_mats, d_items, d_tiles, d_work, nwork, s_hat, ps,
+                     acc, counters, t_polys, t, st);
 }
 
 int run_sequence(grid_gpu_batch* b, const uint32_t* s, uint32_t* t, void* ws, cudaStream_t st) {
-  return run_core(b->plan, b->tc, b->class_begin, b->d_mats, b->d_items, b->d_tiles, b->d_work,
-                  b->nwork, b->s_polys, b->t_polys, s, t, ws, st);
+  return run_core(b->plan, b->tc, b->pm, b->class_begin, b->d_mats, b->d_items, b->d_tiles,
+                  b->d_work, b->nwork, b->s_polys, b->s_region, b->t_polys, s, t, ws, st,
+                  b->d_xtiles, b->nxtiles);
 }
 
 size_t tables_bytes(const Tables& tb) {
@@ -547,6 +607,7 @@ int grid_gpu_batch_destroy(grid_gpu_batch* b) {
   if (b->d_items) cudaFree(b->d_items);
   if (b->d_tiles) cudaFree(b->d_tiles);
   if (b->d_work) cudaFree(b->d_work);
+  if (b->d_xtiles) cudaFree(b->d_xtiles);
   delete b;
   return GRID_OK;
 }
@@ -642,7 +703,7 @@ int grid_gpu_batch_oneshot_workspace(grid_gpu_plan* plan, grid_gpu_matrix* const
   const int rc =
       build_tables(plan, mats, nmats, items, nitems, k_split, 0, GRID_GPU_ENGINE_AUTO, tb);
   if (rc) return rc;
-  *bytes = core_bytes(tb.s_polys, tb.t_polys, plan->d) + tables_bytes(tb);
+  *bytes = core_bytes(witness_region(tb.s_polys, tb.pm_polys), tb.t_polys, plan->d) + tables_bytes(tb);
   return GRID_OK;
 }
 
@@ -656,7 +717,7 @@ int grid_gpu_batch_commit_oneshot_dev(grid_gpu_plan* plan, grid_gpu_matrix* cons
   Tables tb;
   int rc = build_tables(plan, mats, nmats, items, nitems, k_split, 0, GRID_GPU_ENGINE_AUTO, tb);
   if (rc) return rc;
-  const size_t core = core_bytes(tb.s_polys, tb.t_polys, plan->d);
+  const size_t core = core_bytes(witness_region(tb.s_polys, tb.pm_polys), tb.t_polys, plan->d);
   if (workspace_bytes < core + tables_bytes(tb)) return GRID_ERR_INVALID_PARAMETERS;
   cudaStream_t st = (cudaStream_t)stream;
   const MatDev* dm;
@@ -665,8 +726,8 @@ int grid_gpu_batch_commit_oneshot_dev(grid_gpu_plan* plan, grid_gpu_matrix* cons
   const WorkDev* dw;
   rc = send_tables(tb, static_cast<char*>(workspace) + core, &dm, &di, &dt, &dw, st);
   if (rc) return rc;
-  return run_core(plan, tb.tc, tb.class_begin, dm, di, dt, dw, (unsigned)tb.work.size(),
-                  tb.s_polys, tb.t_polys, s, t, workspace, st);
+  return run_core(plan, tb.tc, tb.pm, tb.class_begin, dm, di, dt, dw, (unsigned)tb.work.size(),
+                  tb.s_polys, witness_region(tb.s_polys, tb.pm_polys), tb.t_polys, s, t, workspace, st);
 }
 
 int grid_gpu_batch_gram_workspace(const grid_gpu_plan* plan, const grid_gpu_gram_item* items,
@@ -688,7 +749,7 @@ int grid_gpu_batch_gram_workspace(const grid_gpu_plan* plan, const grid_gpu_gram
   uint64_t g_polys = 0;
   const int rc = build_gram_tables(plan, items, nitems, k_split, tb, &g_polys);
   if (rc) return rc;
-  *bytes = core_bytes(tb.s_polys, tb.t_polys, plan->d) + tables_bytes(tb);
+  *bytes = core_bytes(witness_region(tb.s_polys, tb.pm_polys), tb.t_polys, plan->d) + tables_bytes(tb);
   return GRID_OK;
 }
 
@@ -713,7 +774,7 @@ int grid_gpu_batch_gram_dev(const grid_gpu_plan* plan, const uint32_t* S,
   uint64_t g_polys = 0;
   int rc = build_gram_tables(plan, items, nitems, k_split, tb, &g_polys);
   if (rc) return rc;
-  const size_t core = core_bytes(tb.s_polys, tb.t_polys, d);
+  const size_t core = core_bytes(witness_region(tb.s_polys, tb.pm_polys), tb.t_polys, d);
   if (workspace_bytes < core + tables_bytes(tb)) return GRID_ERR_INVALID_PARAMETERS;
   char* base = static_cast<char*>(workspace);
   uint32_t* s_hat = reinterpret_cast<uint32_t*>(base);
@@ -746,8 +807,8 @@ int grid_gpu_batch_gram_dev(const grid_gpu_plan* plan, const uint32_t* S,
   const WorkDev* dw;
   rc = send_tables(tb, base + core, &dm, &di, &dt, &dw, st);
   if (rc) return rc;
-  return run_product(plan, true, tb.class_begin, dm, di, dt, dw, (unsigned)tb.work.size(), s_hat,
-                     acc, counters, g_polys, G, st);
+  return run_product(plan, true, false, tb.class_begin, dm, di, dt, dw, (unsigned)tb.work.size(),
+                     s_hat, 0, acc, counters, g_polys, G, st);
 }
 
 }  // extern "C"

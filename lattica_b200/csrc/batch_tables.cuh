@@ -19,7 +19,8 @@ constexpr uint32_t kUpperTile = 0xFFFFFFFFu;  // TileDev::matrix of a Gram tile
 
 struct MatDev {
   const uint32_t* evals;
-  uint32_t rows, ld;  // ld: row stride in polys
+  const uint32_t* evals_pm;  // [point][row][ld] (point-major engine), or null
+  uint32_t rows, ld;         // ld: row stride in polys
 };
 struct ItemDev {
   unsigned long long s_off, t_off;
@@ -50,5 +51,12 @@ int launch_batch_tc(const grid_gpu_plan* p, int cls, const WorkDev* work, unsign
                     const TileDev* tiles, const ItemDev* items, const MatDev* mats,
                     const uint32_t* s_hat, unsigned long long* acc, unsigned* counter,
                     cudaStream_t s);
+
+// grouped_pm.cu: the dense classes (TC_D16, TC_D32) over point-major
+// evaluations s_pm [point][ps] (ps >= the packed witness polys, a multiple of 4),
+// one evaluation point per work item (WorkDev::eg = the point).
+int launch_batch_pm(const grid_gpu_plan* p, int cls, const WorkDev* work, unsigned nwork,
+                    const TileDev* tiles, const ItemDev* items, const MatDev* mats,
+                    const uint32_t* s_pm, uint64_t ps, unsigned long long* acc, cudaStream_t s);
 
 }  // namespace grid

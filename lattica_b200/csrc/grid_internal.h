@@ -41,7 +41,8 @@ enum NttMode : int {
   MODE_INV = 1,     // twisted evaluations -> coefficients
   MODE_MULINV = 2,  // out = INTT(NTT(a) (.) b_evals)
   MODE_POLYMUL = 3, // out = INTT(NTT(a) (.) NTT(b))  (negacyclic product)
-  MODE_FWD_PM = 4,  // MODE_FWD stored point-major: out[e * npolys + poly] (d = 64 tensor cores)
+  MODE_FWD_PM = 4,  // MODE_FWD stored point-major: out[e * ps + poly], ps = npolys rounded
+                    // up to a multiple of 4, pad polys zero (d = 64 tensor cores)
 };
 
 struct DeviceScratch {
@@ -127,6 +128,13 @@ int launch_ntt_tc(const grid_gpu_plan* p, int mode, const uint32_t* a, const uin
                   uint32_t* out, size_t npolys, cudaStream_t s);
 void build_tc_tables(uint32_t q, uint32_t d, uint64_t psi, uint64_t ninv,
                      std::vector<unsigned char>& out);
+// MODE_FWD_PM over a tile list: tile t transforms the 128 polys from source
+// row ptiles[t].x of a (npolys polys) into columns ptiles[t].y .. + 127 of
+// out [64][ps_out], polys from ptiles[t].z of the tile on as zeros. Columns
+// are multiples of 4 and tiles do not overlap.
+int launch_ntt_tc_pm_tiles(const grid_gpu_plan* p, const uint32_t* a, size_t npolys,
+                           uint32_t* out, unsigned long long ps_out, const uint4* ptiles,
+                           unsigned long long nptiles, cudaStream_t s);
 // ntt256_tc.cu (d = 256 products, tcgen05)
 bool ntt256_tc_available(const grid_gpu_plan* p);
 int launch_ntt256_tc(const grid_gpu_plan* p, const uint32_t* a, const uint32_t* b, uint32_t* out,

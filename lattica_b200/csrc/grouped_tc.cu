@@ -275,7 +275,7 @@ __global__ void __launch_bounds__(kGtThreads, 1)
     const WorkDev wk = work[w];
     const TileDev tile = tiles[wk.tile];
     const bool upper = tile.matrix == kUpperTile;
-    const MatDev mat = upper ? MatDev{nullptr, tile.count, 0} : mats[tile.matrix];
+    const MatDev mat = upper ? MatDev{nullptr, nullptr, tile.count, 0} : mats[tile.matrix];
     for (int i = tid; i < kTcMaxTileRows; i += kGtThreads) {
       ItemDev it = {0, 0, 0, 0};
       if ((uint32_t)i < tile.count) it = items[tile.first + i];

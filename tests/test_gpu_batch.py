@@ -113,10 +113,12 @@ def test_batch_rejects_bad_items(cuda):
 
 
 @pytest.mark.parametrize("schedule", [(1024, 0, 1), (2048, 64, 1), (8192, 32, 1), (256, 0, 1),
-                                      (4096, 0, 2)])
+                                      (4096, 0, 2), (1024, 0, 3), (8192, 0, 3), (256, 64, 3),
+                                      (32, 32, 3), (96, 0, 3)])
 def test_batched_commit_schedules_match_oracle(cuda, oracle, schedule):
     """Every engine and tile shape (tensor cores with 128, 64 or 32 instances per
-    tile; CUDA cores) gives the oracle's words."""
+    tile; CUDA cores; tensor cores over point-major evaluations, down to one
+    32-word chunk per K range) gives the oracle's words."""
     import torch
     from lattica_b200.batch import UnevenCommitBatch
     ranks = (8, 16, 32)
@@ -125,11 +127,31 @@ def test_batched_commit_schedules_match_oracle(cuda, oracle, schedule):
     batch = UnevenCommitBatch(plan, mats, items)
     batch.set_config(*schedule)
     cfg = batch.config()
-    assert cfg["tensor_cores"] == (schedule[2] == 1) and cfg["k_split"] == schedule[0]
+    assert cfg["tensor_cores"] == (schedule[2] in (1, 3)) and cfg["k_split"] == schedule[0]
     t = torch.zeros((t_polys, 64), dtype=torch.int32, device=cuda)
     batch.commit_dev(s, t)
     torch.cuda.synchronize()
     assert np.array_equal(t.cpu().numpy().view(np.uint32), want), schedule
+    plan.check_device()
+
+
+def test_point_major_engine_needs_whole_chunks_and_point_major_matrices(cuda):
+    """The point-major engine takes K ranges of whole 32-word chunks, and only
+    matrices that hold point-major evaluations (cols a multiple of 4)."""
+    from lattica_b200 import CommitmentError, TwistedNttPlan, _lib
+    from lattica_b200._lib import GridGpuError
+    from lattica_b200.batch import UnevenCommitBatch
+    from lattica_b200.commit import PreparedMatrix
+    plan = TwistedNttPlan(Q, 64)
+    M = PreparedMatrix(plan, np.zeros((4, 40, 64), np.uint32), 4, 40)
+    batch = UnevenCommitBatch(plan, [M], [(0, 0, 40, 0), (40, 4, 7, 0)])
+    with pytest.raises(CommitmentError):
+        batch.set_config(48, 0, _lib.ENGINE_POINT_MAJOR)
+    batch.set_config(64, 0, _lib.ENGINE_POINT_MAJOR)
+    M2 = PreparedMatrix(plan, np.zeros((4, 41, 64), np.uint32), 4, 41)  # no point-major copy
+    batch2 = UnevenCommitBatch(plan, [M2], [(0, 0, 41, 0)])
+    with pytest.raises(GridGpuError, match="UnsupportedDegree"):  # this engine cannot run it
+        batch2.set_config(64, 0, _lib.ENGINE_POINT_MAJOR)
     plan.check_device()
 
 
@@ -142,7 +164,7 @@ def test_autotuner_searches_tile_shapes(cuda, oracle, tmp_path):
     t = torch.zeros((t_polys, 64), dtype=torch.int32, device=cuda)
     res = batch.autotune(s, t, reps=1, cache_path=str(tmp_path / "a.json"))
     assert len(res["candidates_ms"]) == len(batch.schedules())
-    assert res["engine"] in ("tensor", "cuda_core") and not res["cached"]
+    assert res["engine"] in ("tensor", "cuda_core", "point_major") and not res["cached"]
     t.zero_()
     batch.commit_dev(s, t)
     torch.cuda.synchronize()
