@@ -345,13 +345,15 @@ typedef struct grid_gpu_batch_item {
   uint32_t n;
   uint32_t matrix;
 } grid_gpu_batch_item;
-/* Engines of the grouped product: AUTO = the tensor cores where the plan
- * allows (d % 4 == 0, tensor-core plan), else the CUDA cores; TENSOR requires
- * them (else GRID_ERR_UNSUPPORTED_DEGREE); CUDA_CORE never uses them;
- * POINT_MAJOR runs the tensor cores over point-major evaluations (the
- * witnesses' transform stores [point][poly]; every matrix needs its
- * point-major copy: d = 64, rows <= 32, cols a multiple of 4, else
- * GRID_ERR_UNSUPPORTED_DEGREE). All give the same words. */
+/* Engines of the grouped product: POINT_MAJOR runs the tensor cores over
+ * point-major evaluations (the witnesses' transform stores [point][poly], each
+ * instance at its own 128-aligned columns; every matrix needs its point-major
+ * copy: d = 64, rows <= 32, cols a multiple of 4; k_split a multiple of 32;
+ * else GRID_ERR_UNSUPPORTED_DEGREE / GRID_ERR_INVALID_PARAMETERS); TENSOR runs
+ * them over gathered poly-major evaluations (d % 4 == 0, tensor-core plan,
+ * else GRID_ERR_UNSUPPORTED_DEGREE); CUDA_CORE never uses them; AUTO =
+ * POINT_MAJOR where it applies, else TENSOR where the plan allows, else
+ * CUDA_CORE. All give the same words. */
 enum {
   GRID_GPU_ENGINE_AUTO = 0,
   GRID_GPU_ENGINE_TENSOR = 1,

@@ -320,14 +320,15 @@ int build_tables(const grid_gpu_plan* plan, grid_gpu_matrix* const* mats, size_t
     return GRID_ERR_INVALID_PARAMETERS;
   if (tile_instances != 0 && (tile_instances % 4 || tile_instances > kTcMaxTileRows))
     return GRID_ERR_INVALID_PARAMETERS;
-  tb.pm = engine == GRID_GPU_ENGINE_POINT_MAJOR;
+  // the point-major engine needs the point-major forward transform (d = 64,
+  // tensor cores), every matrix's point-major evaluations and K ranges of
+  // whole chunks; AUTO takes it where those hold
+  bool pm_ok = plan->pm_emm && ntt_tc_available(plan) && k_split % 32 == 0;
+  for (size_t i = 0; pm_ok && i < nmats; ++i) pm_ok = mats[i] && mats[i]->d_evals_pm;
+  if (engine == GRID_GPU_ENGINE_POINT_MAJOR && !pm_ok) return GRID_ERR_UNSUPPORTED_DEGREE;
+  tb.pm = engine == GRID_GPU_ENGINE_POINT_MAJOR || (engine == GRID_GPU_ENGINE_AUTO && pm_ok);
   tb.tc = tb.pm || engine_uses_tc(plan, engine);
   if (engine == GRID_GPU_ENGINE_TENSOR && !tb.tc) return GRID_ERR_UNSUPPORTED_DEGREE;
-  // the point-major engine needs the point-major forward transform (d = 64,
-  // tensor cores) and every matrix's point-major evaluations
-  if (tb.pm && !(plan->pm_emm && ntt_tc_available(plan))) return GRID_ERR_UNSUPPORTED_DEGREE;
-  for (size_t i = 0; tb.pm && i < nmats; ++i)
-    if (mats[i] && !mats[i]->d_evals_pm) return GRID_ERR_UNSUPPORTED_DEGREE;
   for (size_t i = 0; i < nmats; ++i) {
     if (!mats[i]) return GRID_ERR_NULL_POINTER;
     if (mats[i]->plan != plan) return GRID_ERR_INVALID_PARAMETERS;
@@ -516,14 +517,16 @@ size_t tables_bytes(const Tables& tb) {
   return round_up(tb.mats.size() * sizeof(MatDev), 256) +
          round_up(tb.sorted.size() * sizeof(ItemDev), 256) +
          round_up(tb.tiles.size() * sizeof(TileDev), 256) +
-         round_up(tb.work.size() * sizeof(WorkDev), 256);
+         round_up(tb.work.size() * sizeof(WorkDev), 256) +
+         round_up(tb.xtiles.size() * sizeof(uint4), 256);
 }
 
-// Pack the four tables into one host image of the device layout at `dev` and
-// send it with a single copy. The source is pageable: the copy returns once its
-// bytes are staged, so the image may go away when the caller returns.
+// Pack the tables (and the point-major transform's tile list) into one host
+// image of the device layout at `dev` and send it with a single copy. The
+// source is pageable: the copy returns once its bytes are staged, so the image
+// may go away when the caller returns.
 int send_tables(const Tables& tb, char* dev, const MatDev** dm, const ItemDev** di,
-                const TileDev** dt, const WorkDev** dw, cudaStream_t st) {
+                const TileDev** dt, const WorkDev** dw, const uint4** dx, cudaStream_t st) {
   std::vector<char> image(tables_bytes(tb));
   size_t off = 0;
   auto put = [&](const void* src, size_t n) -> void* {
@@ -536,6 +539,7 @@ int send_tables(const Tables& tb, char* dev, const MatDev** dm, const ItemDev** 
   *di = static_cast<const ItemDev*>(put(tb.sorted.data(), tb.sorted.size() * sizeof(ItemDev)));
   *dt = static_cast<const TileDev*>(put(tb.tiles.data(), tb.tiles.size() * sizeof(TileDev)));
   *dw = static_cast<const WorkDev*>(put(tb.work.data(), tb.work.size() * sizeof(WorkDev)));
+  *dx = static_cast<const uint4*>(put(tb.xtiles.data(), tb.xtiles.size() * sizeof(uint4)));
   if (image.empty()) return GRID_OK;
   return cuda_status(cudaMemcpyAsync(dev, image.data(), image.size(), cudaMemcpyHostToDevice, st));
 }
@@ -724,10 +728,12 @@ int grid_gpu_batch_commit_oneshot_dev(grid_gpu_plan* plan, grid_gpu_matrix* cons
   const ItemDev* di;
   const TileDev* dt;
   const WorkDev* dw;
-  rc = send_tables(tb, static_cast<char*>(workspace) + core, &dm, &di, &dt, &dw, st);
+  const uint4* dx;
+  rc = send_tables(tb, static_cast<char*>(workspace) + core, &dm, &di, &dt, &dw, &dx, st);
   if (rc) return rc;
   return run_core(plan, tb.tc, tb.pm, tb.class_begin, dm, di, dt, dw, (unsigned)tb.work.size(),
-                  tb.s_polys, witness_region(tb.s_polys, tb.pm_polys), tb.t_polys, s, t, workspace, st);
+                  tb.s_polys, witness_region(tb.s_polys, tb.pm_polys), tb.t_polys, s, t, workspace,
+                  st, dx, tb.xtiles.size());
 }
 
 int grid_gpu_batch_gram_workspace(const grid_gpu_plan* plan, const grid_gpu_gram_item* items,
@@ -805,7 +811,8 @@ int grid_gpu_batch_gram_dev(const grid_gpu_plan* plan, const uint32_t* S,
   const ItemDev* di;
   const TileDev* dt;
   const WorkDev* dw;
-  rc = send_tables(tb, base + core, &dm, &di, &dt, &dw, st);
+  const uint4* dx;
+  rc = send_tables(tb, base + core, &dm, &di, &dt, &dw, &dx, st);
   if (rc) return rc;
   return run_product(plan, true, false, tb.class_begin, dm, di, dt, dw, (unsigned)tb.work.size(),
                      s_hat, 0, acc, counters, g_polys, G, st);

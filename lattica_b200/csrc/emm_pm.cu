@@ -322,7 +322,7 @@ int launch_pm(const grid_gpu_plan* p, const uint32_t* X, const uint32_t* Y, int 
   static int bps_cache[kMaxDevices] = {};
   int bps = 0;
   const int rc = prepare_kernel(emm_pm_kernel<NP, MX, UPPER>, S::SMEM, kPmThreads, p->device,
-                                bps_cache, &bps);
+                                bps_cache, &bps, true);
   if (rc) return rc;
   // boxes of whole 8-row groups: rows past M (N) read as zero fill
   const int bx = (M + 7) & ~7, by = (N + 7) & ~7;

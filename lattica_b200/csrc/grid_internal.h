@@ -268,12 +268,18 @@ struct Carver {
 
 // Sets the dynamic shared-memory limit of `kernel` once per device and caches
 // its resident blocks per SM (idempotent; benign if two threads race).
+// max_shared: prefer the largest shared-memory carveout, for kernels meant to
+// run two CTAs of about half the SM's shared memory each.
 template <typename K>
-int prepare_kernel(K kernel, size_t smem, int threads, int dev, int* cache, int* bps_out) {
+int prepare_kernel(K kernel, size_t smem, int threads, int dev, int* cache, int* bps_out,
+                   bool max_shared = false) {
   if (dev < 0 || dev >= kMaxDevices) return GRID_ERR_INVALID_PARAMETERS;
   if (cache[dev] == 0) {
     cudaError_t e =
         cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess && max_shared)
+      e = cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                               (int)cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess) return cuda_status(e);
     int bps = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kernel, threads, smem);

@@ -12,17 +12,17 @@
 // instances of one matrix (the MMA's M), sorted longest first. The transform
 // gives every instance its own columns from a multiple of 128, zero past its
 // n_i, so that an instance row's 32-word chunk is 128 aligned bytes. Per chunk:
-//  * warp 8 copies the chunk of every instance row still inside its length
-//    (8 lanes per row, 16-byte cp.async), zero-fills the slot's rows that ran
-//    out since the slot was last filled for this item, and copies the matrix
-//    rows into the slot's Y box; its lanes' copy completions arrive on the
-//    slot's mbarrier (cp.async.mbarrier.arrive.noinc);
-//  * warps 0-7 build the four byte planes of the matrix rows, B row l NP + r,
+//  * warps 4-7 (32 instance rows each) copy the chunk of every instance row
+//    still inside its length (8 lanes per row, 16-byte cp.async), zero-fill
+//    the slot's rows that ran out since the slot was last filled for this
+//    item, and copy the matrix rows into the slot's Y box; their lanes' copy
+//    completions arrive on the slot's mbarrier (cp.async.mbarrier.arrive.noinc);
+//  * warps 0-3 build the four byte planes of the matrix rows, B row l NP + r,
 //    K byte 4k + i = byte l of 2^(8i) A_e[r][k] mod q (emm_tc.cu's method);
-//  * one lane of warp 9 issues four MMAs (M 128, N 4 NP, K 32) into one of two
+//  * one lane of warp 8 issues four MMAs (M 128, N 4 NP, K 32) into one of two
 //    tensor-memory accumulators (alternating per item) and commits them to the
 //    slots' barriers and, after the item's last chunk, to the accumulator's;
-//  * warps 10-13 combine the planes of a finished item, reduce once and add
+//  * warps 9-12 combine the planes of a finished item, reduce once and add
 //    each canonical word into the 64-bit accumulator of its output poly and
 //    point, so K ranges of one instance may run in different items.
 // CTAs take the work list's items with a grid stride (longest first), every
@@ -45,12 +45,12 @@ namespace {
 
 using namespace tcx;
 
-constexpr int kGpBuildWarps = 8;
-constexpr int kGpLoadWarp = 8;
-constexpr int kGpMmaWarp = 9;
-constexpr int kGpEpiWarp0 = 10, kGpEpiWarps = 4;
+constexpr int kGpBuildWarps = 4;
+constexpr int kGpLoadWarp0 = 4, kGpLoadWarps = 4;  // 32 instance rows each
+constexpr int kGpMmaWarp = 8;
+constexpr int kGpEpiWarp0 = 9, kGpEpiWarps = 4;
 constexpr int kGpThreads = (kGpEpiWarp0 + kGpEpiWarps) * 32;
-constexpr int kGpLoaders = 32;
+constexpr int kGpLoaders = kGpLoadWarps * 32;
 constexpr int KCH = 32;  // K words per chunk: one 128-byte swizzled row
 
 template <int NP>
@@ -152,11 +152,13 @@ __global__ void __launch_bounds__(kGpThreads, 2)
   const uint32_t tbase = *taddr_slot;
   bool ok = true;
 
-  if (warp == kGpLoadWarp) {
+  if (warp >= kGpLoadWarp0 && warp < kGpLoadWarp0 + kGpLoadWarps) {
     // ------------------------------------------------------------ copies
-    // Rows of a tile are sorted longest first, so the rows still inside their
-    // length at chunk k form a prefix [0, J); each slot remembers from which
-    // row on it already holds zeros for the current item.
+    // Loader warp lw owns instance rows 32 lw .. + 31 of the tile. Rows are
+    // sorted longest first, so the rows still inside their length at chunk k
+    // form a prefix; each slot remembers from which row on it already holds
+    // zeros for the current item.
+    const int lw = warp - kGpLoadWarp0;
     uint32_t gc = 0;  // chunks of this CTA so far
     uint32_t zeroed[NSA];
     for (unsigned wi = blockIdx.x; ok && wi < nwork; wi += gridDim.x) {
@@ -165,22 +167,18 @@ __global__ void __launch_bounds__(kGpThreads, 2)
       const MatDev mt = mats[tl.matrix];
       const uint32_t* se = s_pm + (unsigned long long)w.eg * ps;
       const uint32_t* ye = mt.evals_pm + (unsigned long long)w.eg * mt.rows * mt.ld;
-      // rows lane + 32 h: point-major column (a multiple of 128) and length
-      unsigned long long off[4];
-      uint32_t len[4];
-#pragma unroll
-      for (int h = 0; h < 4; ++h) {
-        const uint32_t j = lane + 32 * h;
-        off[h] = 0;
-        len[h] = 0;
-        if (j < tl.count) {
-          const ItemDev it = rows[tl.first + j];
-          off[h] = it.s_off;
-          len[h] = it.n;
-        }
+      const uint32_t row0 = 32u * lw;
+      const uint32_t cw = tl.count > row0 ? min(tl.count - row0, 32u) : 0u;  // this warp's rows
+      // this lane's row: point-major column (a multiple of 128) and length
+      unsigned long long off = 0;
+      uint32_t len = 0;
+      if ((uint32_t)lane < cw) {
+        const ItemDev it = rows[tl.first + row0 + lane];
+        off = it.s_off;
+        len = it.n;
       }
 #pragma unroll
-      for (int i = 0; i < NSA; ++i) zeroed[i] = 128;  // the slots' rows hold older data
+      for (int i = 0; i < NSA; ++i) zeroed[i] = 32;  // the slots' rows hold older data
       const uint32_t nch = item_chunks(w);
       for (uint32_t c = 0; c < nch; ++c, ++gc) {
         const uint32_t sl = gc % NSA;
@@ -188,35 +186,29 @@ __global__ void __launch_bounds__(kGpThreads, 2)
           break;
         const uint32_t kc = w.k0 + c * KCH;
         const uint32_t sa = s0 + sl * S::ASLOT;
-        uint32_t J = 0;
-#pragma unroll
-        for (int h = 0; h < 4; ++h) J += __popc(__ballot_sync(0xffffffffu, len[h] > kc));
-        // X: eight lanes per row, 16 bytes each (four rows per instruction)
-        // rows [0, J) from the witness, rows [J, zeroed) as zero fill
+        const uint32_t J = __popc(__ballot_sync(0xffffffffu, len > kc));  // live rows of this warp
         uint32_t zeroed_sl = 0;
 #pragma unroll
         for (int i = 0; i < NSA; ++i) zeroed_sl = i == (int)sl ? zeroed[i] : zeroed_sl;
-        const uint32_t zend = min(max(zeroed_sl, J), tl.count);
+        const uint32_t zend = min(max(zeroed_sl, J), cw);
+        // eight lanes per row, 16 bytes each: rows [0, J) from the witness,
+        // [J, zend) as zero fill (four rows per instruction)
         const uint32_t r = lane >> 3, q4 = lane & 7;
 #pragma unroll
-        for (int h = 0; h < 4; ++h) {
-#pragma unroll
-          for (int s8 = 0; s8 < 8; ++s8) {
-            const uint32_t j = 32 * h + 4 * s8 + r;
-            if (32 * h + 4 * s8 >= zend) break;
-            const unsigned long long o = __shfl_sync(0xffffffffu, off[h], 4 * s8 + r);
-            if (j < zend) {
-              const bool live = j < J;
-              cp_async16s(sa + sw128(j, 0, q4, 0), live ? se + o + kc + 4 * q4 : se,
-                          live ? 16u : 0u);
-            }
+        for (int s8 = 0; s8 < 8; ++s8) {
+          const uint32_t jr = 4 * s8 + r;  // row within this warp's 32
+          const unsigned long long o = __shfl_sync(0xffffffffu, off, jr);
+          if (jr < zend) {
+            const bool live = jr < J;
+            cp_async16s(sa + sw128(row0 + jr, 0, q4, 0), live ? se + o + kc + 4 * q4 : se,
+                        live ? 16u : 0u);
           }
         }
 #pragma unroll
         for (int i = 0; i < NSA; ++i)
-          if (i == (int)sl) zeroed[i] = min(J, tl.count);
-        // Y: rows x eight 16-byte pieces
-        for (uint32_t u = lane; u < mt.rows * 8; u += 32) {
+          if (i == (int)sl) zeroed[i] = min(J, cw);
+        // Y: rows x eight 16-byte pieces, spread over the loader warps
+        for (uint32_t u = lw * 32 + lane; u < mt.rows * 8; u += kGpLoaders) {
           const uint32_t yr = u >> 3, yq = u & 7;
           const uint32_t kw = kc + 4 * yq;
           const bool valid = kw < mt.ld;
@@ -234,7 +226,7 @@ __global__ void __launch_bounds__(kGpThreads, 2)
       uint32_t gc = 0, it = 0;
       for (unsigned wi = blockIdx.x; ok && wi < nwork; wi += gridDim.x, ++it) {
         const uint32_t buf = it & 1;
-        if (it >= 2 && !(ok = mbar_wait(&acc_empty[buf], ((it >> 1) - 1) & 1, err))) break;
+        if (it >= 2 && !(ok = mbar_wait_sleep(&acc_empty[buf], ((it >> 1) - 1) & 1, err))) break;
         tc::fence_after_sync();
         const uint32_t nch = item_chunks(work[wi]);
         for (uint32_t c = 0; c < nch; ++c, ++gc) {
@@ -279,14 +271,14 @@ __global__ void __launch_bounds__(kGpThreads, 2)
         uint32_t y[kWords];
 #pragma unroll
         for (int i = 0; i < kWords; ++i) {
-          const int n = n_base + 8 * i;
+          const int n = n_base + kGpBuildWarps * i;
           y[i] = n < (int)mrows ? *reinterpret_cast<const uint32_t*>(
                                       src + sw128(n, 0, kk >> 2, 0) + 4 * (kk & 3))
                                 : 0u;
         }
 #pragma unroll
         for (int i = 0; i < kWords; ++i) {
-          const int n = n_base + 8 * i;
+          const int n = n_base + kGpBuildWarps * i;
           if (n >= (int)mrows) continue;
           const uint32_t v = y[i];
           const uint32_t y1 = mont_c(v, scale.x, scale_q.x, k.q);  // 2^8 y
@@ -316,7 +308,11 @@ __global__ void __launch_bounds__(kGpThreads, 2)
       const TileDev tl = tiles[w.tile];
       const uint32_t mrows = mats[tl.matrix].rows;
       const unsigned long long toff = j < tl.count ? rows[tl.first + j].t_off : 0ull;
-      if (!(ok = lane0_wait(&acc_full[buf], (it >> 1) & 1, lane, err))) break;
+      // the item's whole K loop: sleep in the barrier rather than poll
+      bool got = true;
+      if (lane == 0) got = mbar_wait_sleep(&acc_full[buf], (it >> 1) & 1, err);
+      __syncwarp();
+      if (!(ok = __shfl_sync(0xffffffffu, got, 0))) break;
       tc::fence_after_sync();
       const uint32_t taddr = tc::tmem_addr(tbase, 32 * quarter, buf * NMMA);
 #pragma unroll 1
@@ -357,8 +353,8 @@ int launch_np(const grid_gpu_plan* p, const WorkDev* work, unsigned nwork, const
   using S = GpShape<NP>;
   static int bps_cache[kMaxDevices] = {};
   int bps = 0;
-  const int rc =
-      prepare_kernel(batch_pm_kernel<NP>, S::SMEM, kGpThreads, p->device, bps_cache, &bps);
+  const int rc = prepare_kernel(batch_pm_kernel<NP>, S::SMEM, kGpThreads, p->device, bps_cache,
+                                &bps, true);
   if (rc) return rc;
   // 2^(8i) R mod q (a Montgomery product with it is 2^(8i) y mod q) and the
   // Shoup companions c qinv mod 2^32
