@@ -103,8 +103,10 @@ __device__ __forceinline__ uint32_t item_chunks(const WorkDev& w) {
   return (w.k1 - w.k0 + KCH - 1) / KCH;
 }
 
+// 64 registers: two CTAs of 13 warps put up to 8 warps on one SM sub-partition,
+// whose 16384 registers hold 8 warps of 64 (not of 72).
 template <int NP>
-__global__ void __launch_bounds__(kGpThreads, 2)
+__global__ void __maxnreg__(64)
     batch_pm_kernel(const WorkDev* __restrict__ work, unsigned nwork,
                     const TileDev* __restrict__ tiles, const ItemDev* __restrict__ rows,
                     const MatDev* __restrict__ mats, const uint32_t* __restrict__ s_pm,
