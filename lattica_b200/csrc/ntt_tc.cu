@@ -166,7 +166,7 @@ __global__ void __launch_bounds__(THREADS, 1)
       // past the awaited one reads as not yet there. The two-transform mode
       // needs fwd(0) before load 2: it waits for it before issuing load 1, when
       // no second phase can complete.
-      if (kTwo && t == 1) ok = warp_wait_fast(&bars[FDONE], 0, err);
+      if (kTwo && t == 1 && n > 0) ok = warp_wait_fast(&bars[FDONE], 0, err);
       if (ok && t >= lag) {
         const uint32_t js = t - lag;
         ok = warp_wait_fast(&bars[STAGED0 + buf], staged_seen[buf]++ & 1, err);
