@@ -705,6 +705,50 @@ def measure_ring_round(dev, reps=20):
             "parity": "t limbs, g, p bit-exact vs the oracle's schoolbook products"}
 
 
+def measure_ntt64_transforms(dev, reps=20):
+    """The batched transforms alone (config 1's 2^22 polys at d = 64, in place):
+    forward and inverse each read and write 256 B per poly, 2 GiB per call
+    (inputs > L2). Checked: the inverse returns the input (every word), and 16
+    sampled polys of the forward equal the oracle's."""
+    import torch
+    from lattica_b200 import TwistedNttPlan, _lib
+    q, d, n = WORKLOADS["ntt64"]
+    plan = TwistedNttPlan(q, d)
+    lib = _lib.load()
+    g = torch.Generator(device=dev).manual_seed(64)
+    x = torch.randint(0, q, (n, d), dtype=torch.int64, device=dev, generator=g).to(torch.int32)
+    x0 = x.clone()
+    stream = torch.cuda.current_stream(dev)
+    fwd = lambda: lib.grid_gpu_ntt_forward_dev(plan.handle, x.data_ptr(), n, stream.cuda_stream)
+    inv = lambda: lib.grid_gpu_ntt_inverse_dev(plan.handle, x.data_ptr(), n, stream.cuda_stream)
+    # parity: one forward against the oracle on sampled polys, then the round trip
+    if fwd() or inv():
+        raise RuntimeError("transform launch failed")
+    torch.cuda.synchronize()
+    if not torch.equal(x, x0):
+        raise AssertionError("forward then inverse does not return the input")
+    from oracle import oracle as O
+    rows = torch.linspace(0, n - 1, 16, dtype=torch.int64, device=dev)
+    want = O.Plan(q, d).forward(x0[rows].cpu().numpy().view(np.uint32))
+    if fwd():
+        raise RuntimeError("transform launch failed")
+    torch.cuda.synchronize()
+    if not np.array_equal(x[rows].cpu().numpy().view(np.uint32), want.reshape(16, d)):
+        raise AssertionError("forward transform differs from the oracle")
+    if inv():
+        raise RuntimeError("transform launch failed")
+    peak, _ = _peaks()
+    out = {}
+    for name, f in (("forward", fwd), ("inverse", inv)):
+        for _ in range(3):
+            f()
+        ms = statistics.median(_events_ms(f, reps, stream))
+        out[name] = {"ms_p50": ms, "polys_per_s": n / (ms / 1e3),
+                     "frac": 2 * 4 * d * n / (ms / 1e3) / 1e9 / peak}
+    torch.cuda.synchronize()
+    return out
+
+
 def measure_ntt256(dev, reps=20):
     """The d = 256 sweep of the batched products: 2^20 polys at q' = 4294962689."""
     import torch
@@ -842,6 +886,7 @@ def run_ours(args, rank, world, local_rank):
     if args.secondary:
         detail = {"commit": measure_commit_plain(dev), "round": measure_round(dev),
                   "batch": measure_batch(dev), "ntt256": measure_ntt256(dev),
+                  "ntt64_transforms": measure_ntt64_transforms(dev),
                   "ring_round": measure_ring_round(dev)}
         if args.serve:
             detail["serve"] = measure_serve(dev)
@@ -882,6 +927,8 @@ def secondary_summary(detail):
         "config3_ms_p50": r(b["batched_ms_p50"]),
         "config3_parity": "all == per-call; 32 sampled == oracle",
         "ntt256_polys_per_s": r(n2["polys_per_s"], 0), "ntt256_frac": r(n2["frac"]),
+        "ntt64_forward_frac": r(detail["ntt64_transforms"]["forward"]["frac"]),
+        "ntt64_inverse_frac": r(detail["ntt64_transforms"]["inverse"]["frac"]),
         "round_q_2e32m5_ms_p50": r(detail["ring_round"]["round_ms_p50"], 4),
         "host_cores": os.cpu_count() or 1,
     }

@@ -78,6 +78,7 @@ def test_secondary_summary_is_short_and_names_the_metric_figures():
         "batch": {"batched_commits_per_s": 1.5e6, "per_call_commits_per_s": 2e4,
                   "batched_ms_p50": 2.7},
         "ntt256": {"polys_per_s": 7.8e8, "frac": 0.36},
+        "ntt64_transforms": {"forward": {"frac": 0.8}, "inverse": {"frac": 0.8}},
         "ring_round": {"round_ms_p50": 2.0},
         "serve": {"commits_per_s_ratio": 8.8, "saturated_req_per_s_ratio": 3.0,
                   "saturated": {"continuous": rate, "plain": rate},
