@@ -320,15 +320,6 @@ int build_tables(const grid_gpu_plan* plan, grid_gpu_matrix* const* mats, size_t
     return GRID_ERR_INVALID_PARAMETERS;
   if (tile_instances != 0 && (tile_instances % 4 || tile_instances > kTcMaxTileRows))
     return GRID_ERR_INVALID_PARAMETERS;
-  // the point-major engine needs the point-major forward transform (d = 64,
-  // tensor cores), every matrix's point-major evaluations and K ranges of
-  // whole chunks; AUTO takes it where those hold
-  bool pm_ok = plan->pm_emm && ntt_tc_available(plan) && k_split % 32 == 0;
-  for (size_t i = 0; pm_ok && i < nmats; ++i) pm_ok = mats[i] && mats[i]->d_evals_pm;
-  if (engine == GRID_GPU_ENGINE_POINT_MAJOR && !pm_ok) return GRID_ERR_UNSUPPORTED_DEGREE;
-  tb.pm = engine == GRID_GPU_ENGINE_POINT_MAJOR || (engine == GRID_GPU_ENGINE_AUTO && pm_ok);
-  tb.tc = tb.pm || engine_uses_tc(plan, engine);
-  if (engine == GRID_GPU_ENGINE_TENSOR && !tb.tc) return GRID_ERR_UNSUPPORTED_DEGREE;
   for (size_t i = 0; i < nmats; ++i) {
     if (!mats[i]) return GRID_ERR_NULL_POINTER;
     if (mats[i]->plan != plan) return GRID_ERR_INVALID_PARAMETERS;
@@ -347,9 +338,17 @@ int build_tables(const grid_gpu_plan* plan, grid_gpu_matrix* const* mats, size_t
     tb.pm_polys += round_up(it.n, 128);  // the workspace does not depend on the engine
     order.emplace_back(it.matrix, (uint32_t)i);
   }
-  // transform tiles read rows s_offset .. and store columns .. below 2^31
-  if (tb.pm && (tb.s_polys > (uint64_t)INT32_MAX - 128 || tb.pm_polys > (uint64_t)INT32_MAX - 128))
-    return GRID_ERR_INVALID_PARAMETERS;
+  // The point-major engine needs the point-major forward transform (d = 64,
+  // tensor cores), every matrix's point-major evaluations, K ranges of whole
+  // chunks, and transform tiles whose source rows and destination columns
+  // stay below 2^31; AUTO takes it where those hold.
+  bool pm_ok = plan->pm_emm && ntt_tc_available(plan) && k_split % 32 == 0 &&
+               tb.s_polys <= (uint64_t)INT32_MAX - 128 && tb.pm_polys <= (uint64_t)INT32_MAX - 128;
+  for (size_t i = 0; pm_ok && i < nmats; ++i) pm_ok = mats[i]->d_evals_pm != nullptr;
+  if (engine == GRID_GPU_ENGINE_POINT_MAJOR && !pm_ok) return GRID_ERR_UNSUPPORTED_DEGREE;
+  tb.pm = engine == GRID_GPU_ENGINE_POINT_MAJOR || (engine == GRID_GPU_ENGINE_AUTO && pm_ok);
+  tb.tc = tb.pm || engine_uses_tc(plan, engine);
+  if (engine == GRID_GPU_ENGINE_TENSOR && !tb.tc) return GRID_ERR_UNSUPPORTED_DEGREE;
   std::stable_sort(order.begin(), order.end(), [&](const auto& x, const auto& y) {
     if (x.first != y.first) return x.first < y.first;
     return items[x.second].n > items[y.second].n;
