@@ -78,14 +78,16 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
                : "r"(taddr) : "memory");
 }
 
-// 16 reduced results of this thread's row: columns col0 .. col0 + 15 of the
-// four E_l blocks (64 columns apart) starting at taddr; one tensor-memory
-// round trip of 16 columns x 4 blocks, with every loaded register named in
-// the wait so that no use is scheduled above it.
-__device__ __forceinline__ void reduce16(uint32_t taddr, const TcConsts& k, uint32_t* out) {
-  uint32_t e[4][16];
+// The four E_l blocks (64 columns apart) of 16 columns from taddr: loads
+// issued, not waited for.
+__device__ __forceinline__ void tmem_ld_planes(uint32_t taddr, uint32_t (&e)[4][16]) {
 #pragma unroll
   for (int l = 0; l < 4; ++l) tmem_ld16(taddr + 64 * l, e[l]);
+}
+
+// Wait for this thread's tensor-memory loads, naming every loaded register so
+// that no use is scheduled above the wait.
+__device__ __forceinline__ void tmem_wait_planes(uint32_t (&e)[4][16]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;"
                :
                  "+r"(e[0][0]), "+r"(e[0][1]), "+r"(e[0][2]), "+r"(e[0][3]), "+r"(e[0][4]), "+r"(e[0][5]), "+r"(e[0][6]), "+r"(e[0][7]),
@@ -98,6 +100,11 @@ __device__ __forceinline__ void reduce16(uint32_t taddr, const TcConsts& k, uint
                  "+r"(e[3][8]), "+r"(e[3][9]), "+r"(e[3][10]), "+r"(e[3][11]), "+r"(e[3][12]), "+r"(e[3][13]), "+r"(e[3][14]), "+r"(e[3][15])
                :
                : "memory");
+}
+
+// 16 canonical words from loaded planes: sum_l 2^(8l) E_l, one reduction.
+__device__ __forceinline__ void combine16(const uint32_t (&e)[4][16], const TcConsts& k,
+                                          uint32_t* out) {
 #pragma unroll
   for (int j = 0; j < 16; ++j) {
     uint64_t v = mad_wide(e[1][j], 256u, (uint64_t)e[0][j]);
@@ -105,6 +112,25 @@ __device__ __forceinline__ void reduce16(uint32_t taddr, const TcConsts& k, uint
     v = mad_wide(e[3][j], 16777216u, v);
     out[j] = redc64(v, k.q, k.qinv);
   }
+}
+
+// 16 reduced results of this thread's row: columns col0 .. col0 + 15 of the
+// four E_l blocks (64 columns apart) starting at taddr; one tensor-memory
+// round trip of 16 columns x 4 blocks. after_load() runs once the loads have
+// landed in registers, before the arithmetic (the columns may be reused from
+// then on).
+template <typename AfterLoad>
+__device__ __forceinline__ void reduce16(uint32_t taddr, const TcConsts& k, uint32_t* out,
+                                         AfterLoad&& after_load) {
+  uint32_t e[4][16];
+  tmem_ld_planes(taddr, e);
+  tmem_wait_planes(e);
+  after_load();
+  combine16(e, k, out);
+}
+
+__device__ __forceinline__ void reduce16(uint32_t taddr, const TcConsts& k, uint32_t* out) {
+  reduce16(taddr, k, out, [] {});
 }
 
 // One transform of a 128-row tile (A at `a`, B at `w`) into 256 columns.
