@@ -12,7 +12,8 @@ the median CUDA-event time.
     python -m lattica_b200.cases ntt256 --reps 4     # d = 256 products, 2^20 polys at q'
     python -m lattica_b200.cases commit_plain --reps 5  # A 8 x 64 from a seed, 64 ternary witnesses
     python -m lattica_b200.cases jl_extract --reps 3 --parts 16  # JL p + int8 entries
-    python -m lattica_b200.cases batch --parts 4096 --engine tensor  # uneven batched commits
+    python -m lattica_b200.cases batch --parts 4096 --engine point_major  # uneven batched commits
+                                                    # (engines: point_major, tensor, cuda_core)
     python -m lattica_b200.cases gram_batch --parts 16  # Gram of 16 witnesses, r in 8..64, n = 1024
     python -m lattica_b200.cases ring_round --reps 5    # the round at q = 2^32 - 5 (no NTT)
 
