@@ -1,11 +1,14 @@
-"""CPU models of two kernel index mappings, checked before the kernels ran on a GPU:
+"""CPU models of kernel index mappings:
 
 * the element placement of the T-threads-per-polynomial transform stages
   (`fwdT_stages` / `invT_stages` in lattica_b200/csrc/ntt.cu) at d = 64,
   T = 8, as the one-launch commitment uses them, against the
   one-thread-per-polynomial stages (`fwd1_stages` / `inv1_stages`);
 * the 4 x 4 byte transpose across a lane quad in the JL projection kernel
-  that writes the int8 entries (`jl_tc_kernel<true, true>` in jl.cu).
+  that writes the int8 entries (`jl_tc_kernel<true, true>` in jl.cu);
+* the instance-row copies of the grouped point-major product
+  (`batch_pm_kernel` in grouped_pm.cu): which rows each chunk copies or
+  zero-fills, over rotating shared-memory slots.
 
 The models restate the kernels' index arithmetic with exact arithmetic mod q
 and arbitrary twiddle values, so they check data movement, not the field."""
@@ -176,3 +179,65 @@ def test_lane_quad_byte_transpose_of_jl_entries():
         for r in range(4):
             for u in range(4):
                 assert (o[r] >> (8 * u)) & 0xFF == (M[u][r] - 1) & 0xFF
+
+
+def _sw128(row, c16):
+    """Byte offset of 16-byte chunk c16 of `row` in a 128-byte-swizzled tile."""
+    return (row >> 3) * 1024 + (row & 7) * 128 + ((c16 ^ (row & 7)) << 4)
+
+
+def test_grouped_point_major_loader_keeps_live_rows_and_zeroes_finished_ones():
+    """The copy bookkeeping of batch_pm_kernel (grouped_pm.cu): four loader
+    warps of 32 instance rows, eight lanes per row and four rows per step; per
+    chunk, rows still inside their length (a prefix: tiles are sorted longest
+    first) are copied, rows that ran out since the slot last held this item are
+    zero-filled, and the rest are left as they are. Slots rotate over chunks and
+    items. Every stored row of every chunk must read its words inside the
+    instance's padded columns, and hold exactly its words there, zero past n."""
+    rng = random.Random(11)
+    NSA, KCH = 4, 32
+    slots = [[rng.randrange(1 << 32) for _ in range(128 * 32)] for _ in range(NSA)]  # old data
+    gc = 0
+    for item in range(40):
+        count = rng.randint(1, 128)
+        ns = sorted((rng.randint(1, 900) for _ in range(count)), reverse=True)
+        kmax = ns[0]
+        k_split = rng.choice([32, 64, 256, 1024])
+        k0 = rng.randrange(0, kmax, 32) if kmax > 32 else 0
+        k0 -= k0 % k_split
+        k1 = min(kmax, k0 + k_split)
+        padded = [(n + 127) // 128 * 128 for n in ns]
+        value = lambda j, k: (j * 100003 + k * 7 + item) % (1 << 32)
+        zeroed = [[32] * NSA for _ in range(4)]  # per loader warp, per slot
+        for c in range((k1 - k0 + KCH - 1) // KCH):
+            sl = gc % NSA
+            kc = k0 + c * KCH
+            tile = slots[sl]
+            for lw in range(4):
+                row0 = 32 * lw
+                cw = max(0, min(count - row0, 32))
+                J = sum(1 for jr in range(cw) if ns[row0 + jr] > kc)
+                assert all(ns[row0 + jr] > kc for jr in range(J))  # a prefix
+                zend = min(max(zeroed[lw][sl], J), cw)
+                for s8 in range(8):
+                    for lane in range(32):
+                        r, q4 = lane >> 3, lane & 7
+                        jr = 4 * s8 + r
+                        if jr >= zend:
+                            continue
+                        j = row0 + jr
+                        off = _sw128(j, q4) // 4
+                        for w in range(4):
+                            k = kc + 4 * q4 + w
+                            if jr < J:  # 16 bytes of the instance's columns
+                                assert k < padded[j]
+                                tile[off + w] = value(j, k) if k < ns[j] else 0
+                            else:
+                                tile[off + w] = 0
+                zeroed[lw][sl] = min(J, cw)
+            for j in range(count):
+                for kk in range(KCH):
+                    k = kc + kk
+                    word = tile[_sw128(j, kk >> 2) // 4 + (kk & 3)]
+                    assert word == (value(j, k) if k < ns[j] else 0), (item, c, j, kk)
+            gc += 1
