@@ -241,3 +241,121 @@ def test_grouped_point_major_loader_keeps_live_rows_and_zeroes_finished_ones():
                     word = tile[_sw128(j, kk >> 2) // 4 + (kk & 3)]
                     assert word == (value(j, k) if k < ns[j] else 0), (item, c, j, kk)
             gc += 1
+
+
+def _transform_roles(n, two, old_loader_wait):
+    """The waits and arrivals of ntt_tc_kernel's loader, MMA and epilogue
+    roles for n tiles (two: the NTT -> product -> INTT mode). Each role is a
+    generator of ('wait', barrier, phase index), ('arrive', barrier) and
+    ('async', barrier) (a copy or MMA completion that lands later)."""
+    lag = 3 if two else 2
+
+    def loader():
+        staged_seen = [0, 0]
+        for t in range(n + lag):
+            if old_loader_wait:
+                if t >= 2 and t - 2 < n:
+                    yield ("wait", "FDONE", t - 2)
+            elif two and t == 1 and n > 0:
+                yield ("wait", "FDONE", 0)
+            if t >= lag:
+                buf = t & 1
+                yield ("wait", f"STAGED{buf}", staged_seen[buf])
+                staged_seen[buf] += 1
+            if t < n:
+                if t >= 2:  # buffer t & 1 held tile t - 2: its forward must be done
+                    yield ("check", "FDONE", t - 1)
+                yield ("async", f"AFULL{t & 1}")
+
+    def mma():
+        def inverse(j):
+            yield ("wait", "PREADY", j)
+            if j >= 1:
+                yield ("wait", "EREAD", j - 1)
+            yield ("async", "IDONE")
+        for j in range(n):
+            yield ("wait", f"AFULL{j & 1}", j >> 1)
+            if j >= 1:
+                yield ("wait", "FREAD", j - 1)
+            yield ("async", "FDONE")
+            if two and j >= 1:
+                yield from inverse(j - 1)
+        if two and n > 0:
+            yield from inverse(n - 1)
+
+    def epilogue():
+        def inverse_out(j):
+            yield ("wait", "IDONE", j)
+            yield ("arrive", "EREAD")
+            yield ("arrive", f"STAGED{(j + 1) & 1}")
+        for j in range(n):
+            yield ("wait", "FDONE", j)
+            yield ("arrive", "FREAD")
+            if two:
+                if j >= 1:
+                    yield ("wait", "IDONE", j - 1)
+                yield ("arrive", "PREADY")
+                if j >= 1:
+                    yield from inverse_out(j - 1)
+            else:
+                yield ("arrive", f"STAGED{j & 1}")
+        if two and n > 0:
+            yield from inverse_out(n - 1)
+
+    return [loader(), mma(), epilogue()]
+
+
+def _run_transform_model(n, two, old_loader_wait, rng):
+    """Random interleaving with mbarrier parity semantics; returns the first
+    wait that met its barrier two or more phases past the awaited one (where a
+    parity test reads a completed phase as pending), or the first load into a
+    buffer whose previous tile's forward transform had not completed, or None."""
+    done = {}
+    roles = _transform_roles(n, two, old_loader_wait)
+    current = [next(r, None) for r in roles]
+    pending = []  # async completions not landed yet
+    while any(c is not None for c in current) or pending:
+        choices = [("role", i) for i, c in enumerate(current) if c is not None]
+        choices += [("land", i) for i in range(len(pending))]
+        kind, i = rng.choice(choices)
+        if kind == "land":
+            bar = pending.pop(i)
+            done[bar] = done.get(bar, 0) + 1
+            continue
+        op = current[i]
+        if op[0] == "wait":
+            completed = done.get(op[1], 0)
+            if completed >= op[2] + 2:
+                return op
+            if completed <= op[2]:
+                # blocked; if nothing else can move the model is stuck
+                if not pending and all(c is None or c[0] == "wait" and done.get(c[1], 0) <= c[2]
+                                       for c in current):
+                    raise AssertionError(f"stuck at {current}")
+                continue
+        elif op[0] == "check":
+            if done.get(op[1], 0) < op[2]:
+                return op
+        elif op[0] == "arrive":
+            done[op[1]] = done.get(op[1], 0) + 1
+        else:
+            pending.append(op[1])
+        current[i] = next(roles[i], None)
+    return None
+
+
+def test_transform_barrier_waits_never_alias_a_phase():
+    """ntt_tc_kernel's waits are parity waits: each is correct only while its
+    barrier is at most one phase past the awaited one. Over random
+    interleavings of the three roles and of copy and MMA completions, no wait
+    of the kernel as written ever meets an older phase, and no load refills a
+    buffer before the forward transform of its previous tile. The loader's earlier
+    wait for fwd(t - 2) did: with load t - 1 issued, fwd(t - 1) could complete
+    before it polled."""
+    rng = random.Random(5)
+    for two in (False, True):
+        for n in (1, 2, 3, 7):
+            for _ in range(300):
+                assert _run_transform_model(n, two, False, rng) is None, (two, n)
+    hits = sum(_run_transform_model(7, False, True, rng) is not None for _ in range(300))
+    assert hits > 0  # the model does find the old race
