@@ -8,7 +8,11 @@
   that writes the int8 entries (`jl_tc_kernel<true, true>` in jl.cu);
 * the instance-row copies of the grouped point-major product
   (`batch_pm_kernel` in grouped_pm.cu): which rows each chunk copies or
-  zero-fills, over rotating shared-memory slots.
+  zero-fills, over rotating shared-memory slots;
+* the mbarrier protocols of the tensor-core transform (`ntt_tc_kernel`) and of
+  the grouped point-major product: parity waits never meet a barrier two
+  phases past the awaited one, and no buffer, slot or accumulator is reused
+  early, over random interleavings of the roles and of copy / MMA completions.
 
 The models restate the kernels' index arithmetic with exact arithmetic mod q
 and arbitrary twiddle values, so they check data movement, not the field."""
@@ -359,3 +363,95 @@ def test_transform_barrier_waits_never_alias_a_phase():
                 assert _run_transform_model(n, two, False, rng) is None, (two, n)
     hits = sum(_run_transform_model(7, False, True, rng) is not None for _ in range(300))
     assert hits > 0  # the model does find the old race
+
+
+def _grouped_pm_roles(items, nsa, nsb):
+    """batch_pm_kernel's roles over one CTA's items (chunks per item): loader
+    (A slots), builders (B slots), MMA issuer (two accumulators) and epilogue,
+    as generators of ('wait', barrier, phase), ('arrive', barrier), ('async',
+    barrier) and ('check', barrier, completions needed) ops."""
+    def loader():
+        gc = 0
+        for nch in items:
+            for _ in range(nch):
+                sl = gc % nsa
+                if gc >= nsa:
+                    yield ("wait", f"afree{sl}", gc // nsa - 1)
+                yield ("check", f"afree{sl}", gc // nsa)  # slot's previous MMAs done
+                yield ("async", f"full{sl}")
+                gc += 1
+
+    def builders():
+        gc = 0
+        for nch in items:
+            for _ in range(nch):
+                sl, bs = gc % nsa, gc % nsb
+                yield ("wait", f"full{sl}", gc // nsa)
+                if gc >= nsb:
+                    yield ("wait", f"bfree{bs}", gc // nsb - 1)
+                yield ("check", f"bfree{bs}", gc // nsb)
+                yield ("arrive", f"built{bs}")
+                gc += 1
+
+    def mma():
+        gc = 0
+        for it, nch in enumerate(items):
+            buf = it & 1
+            if it >= 2:
+                yield ("wait", f"accempty{buf}", (it >> 1) - 1)
+            yield ("check", f"accempty{buf}", it >> 1)  # accumulator read out
+            for _ in range(nch):
+                sl, bs = gc % nsa, gc % nsb
+                yield ("wait", f"full{sl}", gc // nsa)
+                yield ("wait", f"built{bs}", gc // nsb)
+                yield ("async", f"afree{sl}")
+                yield ("async", f"bfree{bs}")
+                gc += 1
+            yield ("async", f"accfull{buf}")
+
+    def epilogue():
+        for it in range(len(items)):
+            buf = it & 1
+            yield ("wait", f"accfull{buf}", it >> 1)
+            yield ("arrive", f"accempty{buf}")
+
+    return [loader(), builders(), mma(), epilogue()]
+
+
+def test_grouped_point_major_barriers_never_alias_and_never_reuse_early():
+    """The same check for the grouped point-major product: over random
+    interleavings, every parity wait meets its barrier at most one phase past
+    the awaited one, no A slot is refilled and no B slot rebuilt before the
+    MMAs of its previous chunk completed, and no item's MMAs start on an
+    accumulator before the epilogue read the item two back."""
+    rng = random.Random(9)
+    for nsa, nsb in ((4, 3), (3, 2), (2, 2), (5, 3)):
+        for _ in range(150):
+            items = [rng.randint(1, 9) for _ in range(rng.randint(1, 6))]
+            roles = _grouped_pm_roles(items, nsa, nsb)
+            done, pending = {}, []
+            current = [next(r, None) for r in roles]
+            while any(c is not None for c in current) or pending:
+                choices = [("role", i) for i, c in enumerate(current) if c is not None]
+                choices += [("land", i) for i in range(len(pending))]
+                kind, i = rng.choice(choices)
+                if kind == "land":
+                    bar = pending.pop(i)
+                    done[bar] = done.get(bar, 0) + 1
+                    continue
+                op = current[i]
+                if op[0] == "wait":
+                    completed = done.get(op[1], 0)
+                    assert completed <= op[2] + 1, (items, nsa, nsb, op)
+                    if completed <= op[2]:
+                        assert pending or any(
+                            c is not None and not (c[0] == "wait" and done.get(c[1], 0) <= c[2])
+                            for c in current), ("stuck", items, current)
+                        continue
+                elif op[0] == "check":
+                    assert done.get(op[1], 0) >= op[2], (items, nsa, nsb, op)
+                elif op[0] == "arrive":
+                    done[op[1]] = done.get(op[1], 0) + 1
+                else:
+                    pending.append(op[1])
+                current[i] = next(roles[i], None)
